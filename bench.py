@@ -1,0 +1,452 @@
+#!/usr/bin/env python
+"""FDK benchmark: backprojection GUPS and recons/s on one or more B200s.
+
+Workload (default ``cone512``): flat-panel cone-beam full scan, 512^3 volume at 0.5 mm, 720 views
+over 360 degrees, 1024 x 768 detector at 0.4 mm, SOD 750 mm, SDD 1200 mm. Input: analytic line
+integrals of 16 seeded random ellipsoids (FP64 on the device, cast to float32) with Poisson noise
+at 1e5 incident photons per ray. A step is one full FDK reconstruction (weighting + ramp filter +
+backprojection) of that input, resident in HBM. Inputs (2.26 GB) and the volume (537 MB) exceed the
+126 MB L2, so no flush is needed between steps.
+
+``value`` is GUPS (voxel x view updates per second, all GPUs) of the mixed-precision path (FP16
+filtered storage with per-view scale, FP32 accumulation); the plain FP32 path is timed in the same
+run (``fp32``). Errors are relative RMS / max against the FP64 CPU oracle on sampled voxels.
+
+``--impl reference`` times the reference's CPU path. The reference (satidev/gct) has no CPU FDK,
+so its stand-in is the FP64 oracle port (oracle/), run on all host cores on a bounded sample of the
+same workload.
+
+Multi-GPU: every rank reconstructs its own copy of the workload (independent reconstructions,
+weak scaling, no collective on the data path); times are max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+CONFIGS = {
+    "cone512": dict(kind="cone_flat", nv=720, nc=1024, nr=768, du=0.4, dv=0.4, sod=750.0, sdd=1200.0,
+                    n=(512, 512, 512), vox=0.5, range=2 * math.pi, n_ell=16, i0=1e5,
+                    label="flat-panel cone-beam full scan, 512^3 at 0.5 mm, 720 views, 1024x768 at 0.4 mm, "
+                          "SOD 750, SDD 1200"),
+    "short384": dict(kind="cone_flat", nv=496, nc=1240, nr=960, du=0.3, dv=0.3, sod=785.0, sdd=1200.0,
+                     n=(512, 512, 384), vox=0.5, range=None, n_ell=16, i0=None,
+                     label="flat-panel cone-beam short scan (pi + fan), 512x512x384, 496 views, 1240x960 at 0.3 mm, "
+                           "SOD 785, SDD 1200"),
+    "fan256": dict(kind="fan_line", nv=360, nc=512, nr=1, du=1.2, dv=1.0, sod=570.0, sdd=1040.0,
+                   n=(256, 256, 1), vox=1.0, range=2 * math.pi, n_ell=10, i0=None,
+                   label="fan-beam line detector full scan, 256^2 at 1 mm, 360 views, 512 cells at 1.2 mm, "
+                         "SOD 570, SDD 1040"),
+}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["gct", "reference"], default="gct")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="cone512")
+    ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--zpt", type=int, default=0, help="backprojection z per thread (0 = default)")
+    ap.add_argument("--no-error", action="store_true", help="skip the FP64 oracle error check")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------------
+# workload
+
+def make_geometry(cfg):
+    import gct_b200 as g
+    nv, nc, nr = cfg["nv"], cfg["nc"], cfg["nr"]
+    rng = cfg["range"]
+    if rng is None:  # short scan: pi + full fan angle
+        rng = math.pi + 2.0 * math.atan(nc * cfg["du"] / 2.0 / cfg["sdd"])
+    rot = g.RotationParams(g.RotDir.CW, 0.0, rng / nv, nv)
+    if cfg["kind"] == "cone_flat":
+        det = (g.DetFanLine(nc, cfg["du"]), g.DetFanLine(nr, cfg["dv"]))
+        params = g.ConeBeamProjGeomParams((nc - 1) / 2.0, rot, cfg["sdd"], cfg["sod"], (nr - 1) / 2.0)
+    else:
+        det = (g.DetFanLine(nc, cfg["du"]),)
+        params = g.FanBeamProjGeomParams((nc - 1) / 2.0, rot, cfg["sdd"], cfg["sod"])
+    cg = g.AxialCTGeom.from_params(det, params)
+    nx, ny, nz = cfg["n"]
+    v = cfg["vox"]
+    if cfg["kind"] == "cone_flat":
+        vg = g.ReconImgGeom(g.EqDistSampler(nx, v), g.EqDistSampler(ny, v), g.EqDistSampler(nz, v), (0.0, 0.0, 0.0))
+    else:
+        vg = g.ReconImgGeom(g.EqDistSampler(nx, v), g.EqDistSampler(ny, v), None, (0.0, 0.0))
+    return cg, vg
+
+
+def make_ellipsoids(cfg, seed):
+    """Seeded phantom: a water-like body plus random inner ellipsoids (mm, 1/mm)."""
+    rs = np.random.RandomState(seed)
+    nx, ny, nz = cfg["n"]
+    half = 0.5 * cfg["vox"] * min(nx, ny)
+    halfz = 0.5 * cfg["vox"] * nz if nz > 1 else half
+    ell = [(0.0, 0.0, 0.0, 0.80 * half, 0.65 * half, 0.75 * halfz, 0.0, 0.019)]
+    for _ in range(cfg["n_ell"] - 1):
+        r = 0.55 * half * math.sqrt(rs.uniform())
+        t = rs.uniform(0, 2 * math.pi)
+        cz = rs.uniform(-0.5, 0.5) * halfz
+        a = rs.uniform(5.0, 0.25 * half, size=3)
+        ell.append((r * math.cos(t), r * math.sin(t), cz, a[0], a[1], min(a[2], 0.4 * halfz), rs.uniform(0, math.pi),
+                    rs.uniform(0.01, 0.05) - 0.03))
+    return ell
+
+
+def make_projections(cg, cfg, seed, device):
+    import torch
+    import gct_b200 as g
+    proj = torch.empty((cg.num_views, cg.num_rows, cg.num_cols), dtype=torch.float32, device=device)
+    g.phantom_project(cg, make_ellipsoids(cfg, seed), proj)
+    if cfg["i0"]:
+        gen = torch.Generator(device=device)
+        gen.manual_seed(seed)
+        lam = cfg["i0"] * torch.exp(-proj.double())
+        counts = torch.poisson(lam, generator=gen).clamp_(min=1.0)
+        proj = (-torch.log(counts / cfg["i0"])).float()
+        del lam, counts
+    torch.cuda.synchronize()
+    return proj.contiguous()
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU oracle leg (reference arm and cpu_baseline)
+
+def sample_rows(nr: int) -> tuple:
+    """Detector rows [lo, hi) that the two central z-slices of a centred grid project onto."""
+    lo = max(0, (nr - 1) // 2 - 7)
+    return lo, min(nr, lo + 16)
+
+
+def oracle_sample(cfg, seed, proj_rows=None):
+    """Bounded CPU sample: FP64 oracle FDK of the two central z-slices (all x, y) over all views.
+
+    The detector is cut to the rows those slices project onto (geometry with a shifted row
+    centre, identical for these voxels). Projections are the given device rows, or generated by
+    the FP64 oracle phantom with numpy Poisson noise when None."""
+    from oracle import oracle as orc
+    import gct_b200 as g
+    cg, _ = make_geometry(cfg)
+    nx, ny, nz = cfg["n"]
+    k0 = nz // 2 - 1
+    r_lo, r_hi = sample_rows(cg.num_rows)
+    views = cg.views.copy()
+    if cg.is_3d:
+        views["det_col_center"] -= r_lo
+    og = orc.Geometry(int(cg.kind), cg.num_cols, cg.det_geom()[0].sampling_width, views,
+                      (r_hi - r_lo) if cg.is_3d else 1, cg.det_geom()[1].sampling_width if cg.is_3d else 1.0)
+    if proj_rows is None:
+        p = orc.phantom(og, np.array(make_ellipsoids(cfg, seed)))
+        if cfg["i0"]:
+            rs = np.random.RandomState(seed)
+            cnt = np.maximum(rs.poisson(cfg["i0"] * np.exp(-p)), 1.0)
+            p = -np.log(cnt / cfg["i0"])
+        proj_rows = p.astype(np.float32)
+    nslab = 2 if nz > 1 else 1
+    ov = orc.Volume(nx, ny, nz, cfg["vox"], cfg["vox"], cfg["vox"], (0.0, 0.0, 0.0))
+    ii, jj = np.meshgrid(np.arange(nx), np.arange(ny), indexing="xy")
+    vox = np.concatenate([np.stack([ii.ravel(), jj.ravel(), np.full(ii.size, k0 + s if nz > 1 else 0)], 1)
+                          for s in range(nslab)]).astype(np.uint32)
+    threads = os.cpu_count() or 1
+    t = time.perf_counter()
+    orc.fdk(og, ov, proj_rows, voxels=vox, use_fft=True, threads=threads)
+    dt = time.perf_counter() - t
+    updates = len(vox) * cg.num_views
+    sample = (f"FP64 oracle FDK of {nslab} central z-slice(s) ({nx}x{ny}x{nslab} voxels) over all {cg.num_views} "
+              f"views, detector rows {r_lo}-{r_hi - 1} (the rows those slices touch), {threads} threads")
+    return updates / dt / 1e9, threads, sample, (r_lo, r_hi)
+
+
+def run_reference(args, cfg, rank):
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        oracle_sample(cfg, args.seed)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        v, threads, sample, _ = oracle_sample(cfg, args.seed)
+        vals.append(v)
+    wall = time.perf_counter() - t0
+    value = float(np.median(vals))
+    nx, ny, nz = cfg["n"]
+    line = {
+        "impl": "reference", "metric": "FDK backprojection GUPS (voxel x view updates / s)", "value": value,
+        "unit": "GUPS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * wall / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.config, "description": cfg["label"], "volume": list(cfg["n"]),
+                   "views": cfg["nv"], "detector": [cfg["nc"], cfg["nr"]]},
+        "cpu_baseline": {"value": value, "unit": "GUPS", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "satidev/gct has no CPU FDK; the FP64 oracle port stands in for its CPU path",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------
+# GPU arm
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(gpu_index)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        self.path.unlink(missing_ok=True)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(name: str):
+    """DRAM bytes per launch recorded from an ncu capture summary under profiles/ (or None)."""
+    p = REPO / "profiles" / name
+    if not p.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+def sample_voxels(cfg, seed):
+    nx, ny, nz = cfg["n"]
+    rs = np.random.RandomState(seed + 7)
+    ks = np.linspace(nz // 8, nz - 1 - nz // 8, 6).astype(int) if nz > 1 else np.zeros(1, int)
+    pts = []
+    for k in ks:
+        ii = rs.randint(0, nx, 700)
+        jj = rs.randint(0, ny, 700)
+        pts.append(np.stack([ii, jj, np.full(700, k)], 1))
+    return np.concatenate(pts).astype(np.uint32)
+
+
+def oracle_errors(cg, cfg, proj_dev, vols, seed):
+    """relRMS / max error of each device volume against the FP64 oracle on sampled voxels."""
+    from oracle import oracle as orc
+    vox = sample_voxels(cfg, seed)
+    proj = proj_dev.cpu().numpy()
+    og = orc.Geometry(int(cg.kind), cg.num_cols, cg.det_geom()[0].sampling_width, cg.views,
+                      cg.num_rows, cg.det_geom()[1].sampling_width if cg.is_3d else 1.0)
+    nx, ny, nz = cfg["n"]
+    ov = orc.Volume(nx, ny, nz, cfg["vox"], cfg["vox"], cfg["vox"], (0.0, 0.0, 0.0))
+    ref = orc.fdk(og, ov, proj, voxels=vox, use_fft=True)
+    out = {}
+    for name, vol in vols.items():
+        v = vol.reshape(-1)
+        flat = (vox[:, 2].astype(np.int64) * ny + vox[:, 1]) * nx + vox[:, 0]
+        got = v[flat].double().cpu().numpy() if hasattr(v, "cpu") else v[flat]
+        out[name] = {"rel_rms": float(np.sqrt(np.mean((got - ref) ** 2) / np.mean(ref ** 2))),
+                     "max_rel": float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))}
+    return out, len(vox)
+
+
+def time_plan(plan, proj, vol, steps, warmup, stream, dist):
+    """Times `steps` full FDKs: returns (total seconds max over ranks, mean filter ms, mean BP ms)."""
+    import torch
+    for _ in range(warmup):
+        plan.prepare(proj, stream=stream)
+        plan.backproject(vol, stream=stream)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    start.record(stream)
+    for s in range(steps):
+        ev[s][0].record(stream)
+        plan.prepare(proj, stream=stream)
+        ev[s][1].record(stream)
+        plan.backproject(vol, stream=stream)
+        ev[s][2].record(stream)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    total = start.elapsed_time(stop) / 1000.0
+    filt = float(np.mean([e[0].elapsed_time(e[1]) for e in ev]))
+    bp = float(np.mean([e[1].elapsed_time(e[2]) for e in ev]))
+    if dist:
+        t = torch.tensor([total], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total = float(t.item())
+    return total, filt, bp
+
+
+def run_gct(args, cfg, rank, world, local_rank):
+    import torch
+    import gct_b200 as g
+    dist = world > 1
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    cg, vg = make_geometry(cfg)
+    nx, ny, nz = cfg["n"]
+    updates = nx * ny * nz * cg.num_views
+    proj = make_projections(cg, cfg, args.seed + rank, device)
+    stream = torch.cuda.current_stream()
+    plans = {
+        "mixed": g.FdkPlan(cg, vg, opts=g.FdkOptions(storage=g.STORAGE_F16, z_per_thread=args.zpt)),
+        "fp32": g.FdkPlan(cg, vg, opts=g.FdkOptions(storage=g.STORAGE_F32, z_per_thread=args.zpt)),
+    }
+    vols = {k: torch.empty(vg.shape, dtype=torch.float32, device=device) for k in plans}
+    for k, p in plans.items():
+        p.execute(proj, vols[k], stream=stream)
+    torch.cuda.synchronize()
+
+    errors, nsamp = (None, 0)
+    if rank == 0 and not args.no_error:
+        errors, nsamp = oracle_errors(cg, cfg, proj, vols, args.seed)
+
+    results = {}
+    clocks = None
+    for name in ("fp32", "mixed"):
+        sampler = ClockSampler(local_rank) if name == "mixed" else None
+        total, filt_ms, bp_ms = time_plan(plans[name], proj, vols[name], args.steps, args.warmup, stream, dist)
+        if sampler:
+            clocks = sampler.stop()
+        results[name] = dict(total=total, filt_ms=filt_ms, bp_ms=bp_ms,
+                             gups=updates * world * args.steps / total / 1e9)
+
+    e2e = None
+    if not args.no_e2e:
+        plan = plans["mixed"]
+        host_proj = torch.empty(proj.shape, dtype=torch.float32, pin_memory=True)
+        host_proj.copy_(proj)
+        host_vol = torch.empty(vg.shape, dtype=torch.float32, pin_memory=True)
+        hp, hv = host_proj.numpy(), host_vol.numpy()
+        for _ in range(max(1, args.warmup)):
+            plan.execute_host(hp, hv, stream=stream)
+        if dist:
+            torch.distributed.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            plan.execute_host(hp, hv, stream=stream)
+        te = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([te], device=device, dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            te = float(t.item())
+        e2e = {"value": updates * world * args.steps / te / 1e9, "unit": "GUPS",
+               "h2d_bytes_per_step": int(proj.numel() * 4), "d2h_bytes_per_step": int(host_vol.numel() * 4),
+               "ms_per_step": 1000.0 * te / args.steps, "path": "gct_fdk_execute_host (pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        # same sampled rows of the device input, so the baseline reconstructs identical data
+        r_lo, r_hi = sample_rows(cg.num_rows)
+        rows = proj[:, r_lo:r_hi, :].contiguous().cpu().numpy()
+        v, threads, sample, _ = oracle_sample(cfg, args.seed, proj_rows=rows)
+        cpu = {"value": v, "unit": "GUPS", "cores": threads, "kind": "port", "sample": sample}
+
+    if rank != 0:
+        return
+    hbm, peak_kind = measured_peaks()
+    mixed = results["mixed"]
+    bytes_per_update = 8  # four FP16 bilinear taps
+    achieved = updates * bytes_per_update / (mixed["bp_ms"] / 1000.0) / 1e9
+    traffic = profiled_traffic(f"backproject_{args.config}_f16.md")
+    line = {
+        "metric": "FDK backprojection GUPS (voxel x view updates / s), mixed precision", "value": mixed["gups"],
+        "unit": "GUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * mixed["total"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32-accumulate/f16-storage", "data": "synthetic",
+        "config": {"workload": args.config, "description": cfg["label"], "volume": list(cfg["n"]),
+                   "views": cfg["nv"], "detector": [cfg["nc"], cfg["nr"]], "phantom": f"{cfg['n_ell']} seeded ellipsoids",
+                   "noise": f"Poisson I0={cfg['i0']:g}" if cfg["i0"] else "none", "l2": "inputs larger than L2, no flush",
+                   "parallelism": f"replicas x{world}"},
+        "recons_per_s": world * args.steps / mixed["total"],
+        "stages_ms": {"filter": mixed["filt_ms"], "backproject": mixed["bp_ms"]},
+        "fp32": {"value": results["fp32"]["gups"], "unit": "GUPS",
+                 "recons_per_s": world * args.steps / results["fp32"]["total"],
+                 "stages_ms": {"filter": results["fp32"]["filt_ms"], "backproject": results["fp32"]["bp_ms"]}},
+        "speedup_mixed_vs_fp32": mixed["gups"] / results["fp32"]["gups"],
+        "error_vs_fp64_oracle": ({"voxels": nsamp, **errors} if errors else None),
+        "roofline": {"bound": "hbm", "kernel": "backproject (FP16 quads)", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_update": bytes_per_update,
+                     "traffic": traffic},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "clocks": clocks,
+        "gpu_launches": 4 * args.steps,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    cfg = CONFIGS[args.config]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, cfg, rank)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local_rank))
+    try:
+        run_gct(args, cfg, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

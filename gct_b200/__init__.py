@@ -1,0 +1,15 @@
+"""gct_b200: B200-native FDK reconstruction with GCT's geometry and reconstruct() API.
+
+The compute path is the CUDA library ``libgct_fdk.so`` (sm_100a) behind the C ABI in
+``include/gct_fdk.h``; this package is its Python host mirror.
+"""
+from ._lib import GctError, load as load_library, library_path
+from .geometry import (ApodFunc, AxialCTGeom, ConeBeamProjGeomParams, CTGeom, DetFanArc, DetFanLine,
+                       DetParallel, EqDistSampler, FanBeamProjGeomParams, GeomKind, Parallel1DProjGeomParams,
+                       Parallel2DProjGeomParams, ProjectionStack, ProjGeom, ProjGeomFactory, ReconImg,
+                       ReconImgGeom, RotationGeom, RotationParams, RotDir, is_valid_axial_recon, kind_of,
+                       parker_weights, ramp_filter_taps, VIEW_DTYPE)
+from .recon import (FILTER_FFT, FILTER_TOEPLITZ_BF16X3, STORAGE_F16, STORAGE_F32, FdkOptions, FdkPlan,
+                    FiltParams, forward_project, phantom_project, reconstruct)
+
+__all__ = [name for name in dir() if not name.startswith("_")]

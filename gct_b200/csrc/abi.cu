@@ -1,0 +1,675 @@
+// C ABI of the FDK engine (include/gct_fdk.h): plans, execution, stage entry points and the
+// host geometry functions. All failures become a gct_status plus a thread-local message.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/gct_fdk.h"
+#include "geometry.hpp"
+#include "kernels.hpp"
+#include "project.hpp"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+gct_status set_error(gct_status s, const std::string &msg)
+{
+    g_last_error = msg;
+    return s;
+}
+
+void cuda_check(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return;
+    const gct_status s = (e == cudaErrorMemoryAllocation) ? GCT_ERR_OUT_OF_MEMORY : GCT_ERR_CUDA;
+    cudaGetLastError();  // clear the sticky-free error state for the next call
+    gct::fail(s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class F>
+gct_status guarded(F &&f)
+{
+    try {
+        f();
+        return GCT_OK;
+    } catch (const gct::GctError &e) {
+        return set_error(e.status, e.msg);
+    } catch (const std::bad_alloc &) {
+        return set_error(GCT_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception &e) {
+        return set_error(GCT_ERR_INVALID_ARG, e.what());
+    }
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { reset(); }
+    void reset()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count, const char *what)
+    {
+        reset();
+        if (count == 0) return;
+        cuda_check(cudaMalloc(reinterpret_cast<void **>(&p), count * sizeof(T)), what);
+        n = count;
+    }
+    void upload(const T *host, size_t count, const char *what)
+    {
+        alloc(count, what);
+        if (count) cuda_check(cudaMemcpy(p, host, count * sizeof(T), cudaMemcpyHostToDevice), what);
+    }
+};
+
+bool orthonormal(const double *a, const double *b, double tol)
+{
+    auto dot = [](const double *x, const double *y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; };
+    return std::fabs(dot(a, a) - 1.0) < tol && std::fabs(dot(b, b) - 1.0) < tol && std::fabs(dot(a, b)) < tol;
+}
+
+}  // namespace
+
+struct gct_fdk_plan {
+    int device = 0;
+    int num_sms = 148;
+    gct_geom_kind kind = GCT_GEOM_CONE_FLAT;
+    gct::Family family = gct::Family::Projective;
+    std::vector<gct_view_geom> views;
+    gct_ct_geom geom{};
+    gct_vol_geom vol{};
+    gct_filt_params filt{};
+    gct_fdk_opts opts{};
+    gct::RotationInfo rot;
+    bool z_affine = true;
+    unsigned L = 0;
+    int nv = 0, nr = 0, nc = 0;
+    float l1 = 0.f;
+    int zpt = 8, bx = 32, by = 8;
+    DevBuf<float4> fview;
+    DevBuf<float> parker;
+    DevBuf<float2> H, tw;
+    DevBuf<float> coefs;
+    DevBuf<float> vscale, vinv, amax;
+    DevBuf<unsigned char> work;
+    // staging for gct_fdk_execute_host
+    DevBuf<float> host_proj, host_vol;
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t> chunk_events;
+
+    ~gct_fdk_plan()
+    {
+        for (cudaEvent_t e : chunk_events) cudaEventDestroy(e);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
+    }
+
+    size_t quad_bytes() const { return opts.storage == GCT_STORAGE_F16 ? 8 : 16; }
+    size_t workspace_bytes() const
+    {
+        return static_cast<size_t>(nv) * (nr + 2 * gct::kQuadPad) * (nc + 2 * gct::kQuadPad) * quad_bytes();
+    }
+};
+
+namespace {
+
+void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
+                const gct_filt_params *filt, const gct_fdk_opts *opts)
+{
+    gct::check_ct_geom(g);
+    const auto kind = static_cast<gct_geom_kind>(g->kind);
+    gct::check_vol_geom(vol, gct::is_2d_detector(kind));
+    p->kind = kind;
+    p->family = gct::family_of(kind);
+    p->views.assign(g->views, g->views + g->num_views);
+    p->geom = *g;
+    p->geom.views = p->views.data();
+    if (!gct::is_2d_detector(kind)) p->geom.det_col = gct_detector{1u, 1.0};
+    p->vol = *vol;
+    p->filt = filt ? *filt : gct_filt_params{1.0, GCT_APOD_NONE};
+    if (opts) p->opts = *opts;
+    if (p->opts.filter != GCT_FILTER_FFT && p->opts.filter != GCT_FILTER_TOEPLITZ_BF16X3)
+        gct::fail(GCT_ERR_INVALID_ARG, "unknown filter option");
+    if (p->opts.storage != GCT_STORAGE_F32 && p->opts.storage != GCT_STORAGE_F16)
+        gct::fail(GCT_ERR_INVALID_ARG, "unknown storage option");
+    if (p->opts.filter == GCT_FILTER_TOEPLITZ_BF16X3)
+        gct::fail(GCT_ERR_NOT_SUPPORTED, "Toeplitz GEMM filter is not built into this library");
+    if (!gct::rotation_info(p->geom, &p->rot))
+        gct::fail(GCT_ERR_INVALID_ARG, "Invalid X-ray source trajectory.");
+    p->nv = static_cast<int>(g->num_views);
+    p->nc = static_cast<int>(g->det_row.num_samples);
+    p->nr = static_cast<int>(p->geom.det_col.num_samples);
+    p->L = gct::fft_length(static_cast<unsigned>(p->nc));
+    if (p->L > 8192) gct::fail(GCT_ERR_NOT_SUPPORTED, "detector rows longer than 5461 samples");
+
+    // per-view derived geometry (FP64)
+    std::vector<gct::ViewDerived> vd(p->nv);
+    for (int v = 0; v < p->nv; ++v) {
+        vd[v] = gct::derive_view(kind, p->geom, static_cast<unsigned>(v));
+        if (p->family == gct::Family::Arc) {
+            const bool ok = gct::is_2d_detector(kind) ? (orthonormal(vd[v].eu, vd[v].ew, 1e-6) &&
+                                                         orthonormal(vd[v].eu, vd[v].ev, 1e-6) &&
+                                                         orthonormal(vd[v].ew, vd[v].ev, 1e-6))
+                                                      : orthonormal(vd[v].eu, vd[v].ew, 1e-6);
+            if (!ok) gct::fail(GCT_ERR_NOT_SUPPORTED, "arc-detector views need an orthonormal detector basis");
+        }
+        if (p->family != gct::Family::Affine && !(vd[v].sid > 0.0 && vd[v].sdd > 0.0))
+            gct::fail(GCT_ERR_INVALID_ARG, "source distances must be positive");
+        if (kind == GCT_GEOM_CONE_PARALLEL && !(vd[v].sid > 0.0 && vd[v].sdd > 0.0))
+            gct::fail(GCT_ERR_INVALID_ARG, "source distances must be positive");
+    }
+    // final scale of reconFDK (src/cuda/recon/fdk_axial.cuh:196-199): x rot_ang_incr if > 0
+    const double dtheta = p->rot.incr > 0.0 ? p->rot.incr : 1.0;
+    std::vector<double> wscale(p->nv);
+    for (int v = 0; v < p->nv; ++v) wscale[v] = dtheta * vd[v].bp_const;
+    std::vector<float> coefs = gct::bp_coefficients(p->geom, p->vol, vd, wscale, &p->z_affine);
+
+    std::vector<float4> fview(p->nv);
+    for (int v = 0; v < p->nv; ++v)
+        fview[v] = make_float4(static_cast<float>(vd[v].c0), static_cast<float>(vd[v].r0),
+                               static_cast<float>(vd[v].sdd), 0.f);
+    const std::vector<double> parker_d = gct::parker_table(p->geom, p->rot);
+    std::vector<float> parker(parker_d.begin(), parker_d.end());
+    const std::vector<double> taps = gct::ramp_taps(kind, g->det_row, p->filt);
+    double l1 = 0.0;
+    for (double t : taps) l1 += std::fabs(t);
+    p->l1 = static_cast<float>(l1);
+    const auto Hd = gct::filter_spectrum(taps, p->L);
+    std::vector<float2> H(p->L), tw(p->L);
+    for (unsigned k = 0; k < p->L; ++k) {
+        H[k] = make_float2(static_cast<float>(Hd[k].real()), static_cast<float>(Hd[k].imag()));
+        const double ang = -2.0 * 3.14159265358979323846 * k / p->L;
+        tw[k] = make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(std::sin(ang)));
+    }
+
+    cuda_check(cudaGetDevice(&p->device), "cudaGetDevice");
+    cudaDeviceProp prop{};
+    cuda_check(cudaGetDeviceProperties(&prop, p->device), "cudaGetDeviceProperties");
+    p->num_sms = prop.multiProcessorCount;
+    p->fview.upload(fview.data(), fview.size(), "plan geometry");
+    p->parker.upload(parker.data(), parker.size(), "plan Parker table");
+    p->H.upload(H.data(), H.size(), "plan filter spectrum");
+    p->tw.upload(tw.data(), tw.size(), "plan twiddles");
+    p->coefs.upload(coefs.data(), coefs.size(), "plan backprojection coefficients");
+    if (p->opts.storage == GCT_STORAGE_F16) {
+        p->vscale.alloc(p->nv, "plan view scales");
+        p->vinv.alloc(p->nv, "plan view scales");
+        p->amax.alloc(p->nv, "plan view maxima");
+    }
+    // backprojection launch shape
+    const bool vol3d = gct::is_2d_detector(kind);
+    p->zpt = p->opts.z_per_thread > 0 ? p->opts.z_per_thread : (vol3d ? 8 : 1);
+    if (p->zpt != 1 && p->zpt != 2 && p->zpt != 4 && p->zpt != 8 && p->zpt != 16)
+        gct::fail(GCT_ERR_INVALID_ARG, "z_per_thread must be 1, 2, 4, 8 or 16");
+    p->bx = p->opts.block_x > 0 ? p->opts.block_x : 32;
+    p->by = p->opts.block_y > 0 ? p->opts.block_y : 8;
+    if (p->bx * p->by > 256 || p->bx * p->by < 32)
+        gct::fail(GCT_ERR_INVALID_ARG, "backprojection block must hold 32..256 threads");
+}
+
+void run_filter(gct_fdk_plan *p, const float *proj, void *out, int mode, int vb, int vc, cudaStream_t s)
+{
+    if (vc <= 0) return;
+    const long long pix = static_cast<long long>(p->nr) * p->nc;
+    gct::FilterArgs fa;
+    fa.proj = proj + vb * pix;
+    fa.nv = vc;
+    fa.nr = p->nr;
+    fa.nc = p->nc;
+    fa.kind = p->kind;
+    fa.du = static_cast<float>(p->geom.det_row.sampling_width);
+    fa.dv = static_cast<float>(p->geom.det_col.sampling_width);
+    fa.fview = p->fview.p + vb;
+    fa.parker = p->parker.p + static_cast<long long>(vb) * p->nc;
+    fa.H = p->H.p;
+    fa.twiddle = p->tw.p;
+    fa.mode = mode;
+    if (mode == gct::kOutPlainF32) {
+        fa.out = static_cast<float *>(out) + vb * pix;
+    } else {
+        const long long qview = static_cast<long long>(p->nr + 2 * gct::kQuadPad) * (p->nc + 2 * gct::kQuadPad);
+        fa.out = static_cast<unsigned char *>(out) + vb * qview * static_cast<long long>(p->quad_bytes());
+    }
+    fa.vscale = (mode == gct::kOutQuadF16) ? p->vscale.p + vb : nullptr;
+    gct::launch_filter_fft(fa, static_cast<int>(p->L), p->num_sms, s);
+    cuda_check(cudaGetLastError(), "filter kernel launch");
+}
+
+void run_backproject(gct_fdk_plan *p, const void *quads, float *vol, int v_begin, int v_count,
+                     bool accumulate, cudaStream_t s)
+{
+    gct::BpArgs ba;
+    ba.quads = quads;
+    ba.qpitch = p->nc + 2 * gct::kQuadPad;
+    ba.qview = static_cast<long long>(p->nr + 2 * gct::kQuadPad) * ba.qpitch;
+    ba.coefs = p->coefs.p;
+    ba.vinv = (p->opts.storage == GCT_STORAGE_F16) ? p->vinv.p : nullptr;
+    ba.v_begin = v_begin;
+    ba.v_count = v_count;
+    ba.vol = vol;
+    ba.nx = static_cast<int>(p->vol.nx);
+    ba.ny = static_cast<int>(p->vol.ny);
+    ba.nz = static_cast<int>(p->vol.nz);
+    ba.umax = static_cast<float>(p->nc);
+    ba.vmax = static_cast<float>(p->nr);
+    ba.accumulate = accumulate ? 1 : 0;
+    gct::launch_backproject(ba, static_cast<int>(p->family), p->opts.storage, p->z_affine, p->zpt, p->bx,
+                            p->by, s);
+    cuda_check(cudaGetLastError(), "backprojection kernel launch");
+}
+
+void check_range(const gct_fdk_plan *p, uint32_t vb, uint32_t vc)
+{
+    if (static_cast<uint64_t>(vb) + vc > static_cast<uint64_t>(p->nv))
+        gct::fail(GCT_ERR_INVALID_ARG, "view range exceeds the number of views");
+}
+
+void *plan_workspace(gct_fdk_plan *p, void *workspace)
+{
+    if (workspace) return workspace;
+    if (!p->work.p) p->work.alloc(p->workspace_bytes(), "plan workspace");
+    return p->work.p;
+}
+
+void prepare(gct_fdk_plan *p, const float *proj, void *ws, int vb, int vc, cudaStream_t s)
+{
+    if (!proj) gct::fail(GCT_ERR_INVALID_ARG, "NULL projection pointer");
+    if (vc <= 0) return;
+    const bool f16 = p->opts.storage == GCT_STORAGE_F16;
+    if (f16) {
+        const long long pix = static_cast<long long>(p->nr) * p->nc;
+        cuda_check(cudaMemsetAsync(p->amax.p + vb, 0, sizeof(float) * vc, s), "view maxima reset");
+        gct::launch_view_absmax(proj + vb * pix, vc, pix, p->amax.p + vb, s);
+        gct::launch_view_scales(p->amax.p + vb, vc, p->l1, p->vscale.p + vb, p->vinv.p + vb, s);
+        cuda_check(cudaGetLastError(), "view scale kernels");
+    }
+    run_filter(p, proj, ws, f16 ? gct::kOutQuadF16 : gct::kOutQuadF32, vb, vc, s);
+}
+
+void execute(gct_fdk_plan *p, const float *proj, float *vol, void *workspace, cudaStream_t s)
+{
+    if (!proj || !vol) gct::fail(GCT_ERR_INVALID_ARG, "NULL projection or volume pointer");
+    void *ws = plan_workspace(p, workspace);
+    prepare(p, proj, ws, 0, p->nv, s);
+    run_backproject(p, ws, vol, 0, p->nv, false, s);
+}
+
+void execute_host(gct_fdk_plan *p, const float *proj_host, float *vol_host, cudaStream_t s)
+{
+    if (!proj_host || !vol_host) gct::fail(GCT_ERR_INVALID_ARG, "NULL projection or volume pointer");
+    const size_t pix = static_cast<size_t>(p->nr) * p->nc;
+    const size_t vol_n = static_cast<size_t>(p->vol.nx) * p->vol.ny * p->vol.nz;
+    if (!p->host_proj.p) p->host_proj.alloc(pix * p->nv, "staging projections");
+    if (!p->host_vol.p) p->host_vol.alloc(vol_n, "staging volume");
+    void *ws = plan_workspace(p, nullptr);
+    if (!p->copy_stream) cuda_check(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking), "copy stream");
+    // about 8 chunks, at least 16 views each
+    const int chunk = std::max(16, (p->nv + 7) / 8);
+    const int nchunks = (p->nv + chunk - 1) / chunk;
+    while (static_cast<int>(p->chunk_events.size()) < nchunks + 1) {
+        cudaEvent_t e;
+        cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+        p->chunk_events.push_back(e);
+    }
+    // the copy stream must not overwrite staging still read by a previous call on `s`
+    cuda_check(cudaEventRecord(p->chunk_events[nchunks], s), "event record");
+    cuda_check(cudaStreamWaitEvent(p->copy_stream, p->chunk_events[nchunks], 0), "stream wait");
+    for (int c = 0; c < nchunks; ++c) {
+        const int vb = c * chunk, vc = std::min(chunk, p->nv - vb);
+        cuda_check(cudaMemcpyAsync(p->host_proj.p + vb * pix, proj_host + vb * pix, sizeof(float) * pix * vc,
+                                   cudaMemcpyHostToDevice, p->copy_stream),
+                   "projection upload");
+        cuda_check(cudaEventRecord(p->chunk_events[c], p->copy_stream), "event record");
+        cuda_check(cudaStreamWaitEvent(s, p->chunk_events[c], 0), "stream wait");
+        prepare(p, p->host_proj.p, ws, vb, vc, s);
+        run_backproject(p, ws, p->host_vol.p, vb, vc, c > 0, s);
+    }
+    cuda_check(cudaMemcpyAsync(vol_host, p->host_vol.p, sizeof(float) * vol_n, cudaMemcpyDeviceToHost, s),
+               "volume download");
+    cuda_check(cudaStreamSynchronize(s), "reconstruction");
+}
+
+struct PlanHolder {
+    gct_fdk_plan *p = nullptr;
+    ~PlanHolder() { delete p; }
+};
+
+}  // namespace
+
+extern "C" {
+
+int32_t gct_abi_version(void) { return GCT_FDK_ABI_VERSION; }
+
+const char *gct_last_error_string(void) { return g_last_error.c_str(); }
+
+gct_status gct_proj_geom_create(int32_t kind, const gct_geom_params *params, uint32_t proj_idx,
+                                gct_view_geom *out)
+{
+    return guarded([&] {
+        if (!params || !out) gct::fail(GCT_ERR_INVALID_ARG, "NULL argument");
+        if (kind < GCT_GEOM_PARALLEL_1D || kind > GCT_GEOM_CONE_FLAT) gct::fail(GCT_ERR_INVALID_ARG, "unknown geometry kind");
+        *out = gct::make_view(static_cast<gct_geom_kind>(kind), *params, proj_idx);
+    });
+}
+
+gct_status gct_rotation_geom_get(const gct_ct_geom *geom, gct_rotation_geom *out, double *rot_ang,
+                                 double *rel_rot_ang)
+{
+    return guarded([&] {
+        gct::check_ct_geom(geom);
+        if (!out) gct::fail(GCT_ERR_INVALID_ARG, "NULL output");
+        gct::RotationInfo ri;
+        if (!gct::rotation_info(*geom, &ri)) gct::fail(GCT_ERR_INVALID_ARG, "Invalid X-ray source trajectory.");
+        out->dir = ri.dir;
+        out->rot_ang_incr = ri.incr;
+        out->rot_ang_range = ri.range;
+        out->num_proj_per_rot = ri.num_proj_per_rot;
+        if (rot_ang) std::copy(ri.rot_ang.begin(), ri.rot_ang.end(), rot_ang);
+        if (rel_rot_ang) std::copy(ri.rel_rot_ang.begin(), ri.rel_rot_ang.end(), rel_rot_ang);
+    });
+}
+
+gct_status gct_is_valid_axial_recon(const gct_ct_geom *geom, uint32_t proj_num_cols,
+                                    uint32_t proj_num_rows, uint32_t num_proj, int32_t verbose,
+                                    int32_t *valid)
+{
+    return guarded([&] {
+        gct::check_ct_geom(geom);
+        if (!valid) gct::fail(GCT_ERR_INVALID_ARG, "NULL output");
+        bool ok = true;
+        const auto kind = static_cast<gct_geom_kind>(geom->kind);
+        // checkProjDetConsistency (src/cpp/recon/check_validity.h:30-64)
+        if (proj_num_cols != geom->det_row.num_samples) {
+            ok = false;
+            if (verbose)
+                std::fprintf(stderr,
+                             "Inconsistent projection and detector geometry data.\n"
+                             "Number of columns of projection image:: %u\nNumber of detector columns:: %u\n",
+                             proj_num_cols, geom->det_row.num_samples);
+        }
+        if (ok && gct::is_2d_detector(kind) && proj_num_rows != geom->det_col.num_samples) {
+            ok = false;
+            if (verbose)
+                std::fprintf(stderr,
+                             "Inconsistent projection and detector geometry data.\n"
+                             "Number of rows of projection image:: %u\nNumber of detector rows:: %u\n",
+                             proj_num_rows, geom->det_col.num_samples);
+        }
+        // checkProjViewConsistency (check_validity.h:77-108)
+        if (ok && num_proj != geom->num_views) {
+            ok = false;
+            if (verbose) {
+                std::fprintf(stderr, "%s\n",
+                             num_proj > geom->num_views
+                                 ? "Projection geometry parameters are not available for all projection images."
+                                 : "Projection images are not available for all projection geometries.");
+                std::fprintf(stderr, "Number of projection images:: %u\nNumber of projection geometry objects:: %u\n",
+                             num_proj, geom->num_views);
+            }
+        }
+        *valid = ok ? 1 : 0;
+    });
+}
+
+gct_status gct_ramp_filter_taps(int32_t kind, const gct_detector *det_row,
+                                const gct_filt_params *params, double *taps)
+{
+    return guarded([&] {
+        if (!det_row || !taps) gct::fail(GCT_ERR_INVALID_ARG, "NULL argument");
+        if (kind < GCT_GEOM_PARALLEL_1D || kind > GCT_GEOM_CONE_FLAT) gct::fail(GCT_ERR_INVALID_ARG, "unknown geometry kind");
+        const gct_filt_params fp = params ? *params : gct_filt_params{1.0, GCT_APOD_NONE};
+        const auto t = gct::ramp_taps(static_cast<gct_geom_kind>(kind), *det_row, fp);
+        std::copy(t.begin(), t.end(), taps);
+    });
+}
+
+gct_status gct_parker_weights(const gct_ct_geom *geom, float *weights)
+{
+    return guarded([&] {
+        gct::check_ct_geom(geom);
+        if (!weights) gct::fail(GCT_ERR_INVALID_ARG, "NULL output");
+        gct::RotationInfo ri;
+        if (!gct::rotation_info(*geom, &ri)) gct::fail(GCT_ERR_INVALID_ARG, "Invalid X-ray source trajectory.");
+        const auto w = gct::parker_table(*geom, ri);
+        for (size_t i = 0; i < w.size(); ++i) weights[i] = static_cast<float>(w[i]);
+    });
+}
+
+gct_status gct_fdk_plan_create(const gct_ct_geom *geom, const gct_vol_geom *vol,
+                               const gct_filt_params *filt, const gct_fdk_opts *opts,
+                               gct_fdk_plan **out)
+{
+    return guarded([&] {
+        if (!out) gct::fail(GCT_ERR_INVALID_ARG, "NULL plan output");
+        *out = nullptr;
+        PlanHolder h;
+        h.p = new gct_fdk_plan();
+        build_plan(h.p, geom, vol, filt, opts);
+        *out = h.p;
+        h.p = nullptr;
+    });
+}
+
+gct_status gct_fdk_plan_destroy(gct_fdk_plan *plan)
+{
+    return guarded([&] {
+        if (!plan) return;
+        DeviceGuard dg(plan->device);
+        delete plan;
+    });
+}
+
+gct_status gct_fdk_plan_workspace_bytes(const gct_fdk_plan *plan, uint64_t *bytes)
+{
+    return guarded([&] {
+        if (!plan || !bytes) gct::fail(GCT_ERR_INVALID_ARG, "NULL argument");
+        *bytes = plan->workspace_bytes();
+    });
+}
+
+gct_status gct_fdk_execute(gct_fdk_plan *plan, const float *proj_dev, float *vol_dev, void *workspace,
+                           void *stream)
+{
+    return guarded([&] {
+        if (!plan) gct::fail(GCT_ERR_INVALID_ARG, "NULL plan");
+        DeviceGuard dg(plan->device);
+        execute(plan, proj_dev, vol_dev, workspace, static_cast<cudaStream_t>(stream));
+    });
+}
+
+gct_status gct_fdk_filter(gct_fdk_plan *plan, const float *proj_dev, float *filtered_dev, void *stream)
+{
+    return guarded([&] {
+        if (!plan || !proj_dev || !filtered_dev) gct::fail(GCT_ERR_INVALID_ARG, "NULL argument");
+        DeviceGuard dg(plan->device);
+        run_filter(plan, proj_dev, filtered_dev, gct::kOutPlainF32, 0, plan->nv, static_cast<cudaStream_t>(stream));
+    });
+}
+
+gct_status gct_fdk_prepare(gct_fdk_plan *plan, const float *proj_dev, void *workspace, uint32_t view_begin,
+                           uint32_t view_count, void *stream)
+{
+    return guarded([&] {
+        if (!plan) gct::fail(GCT_ERR_INVALID_ARG, "NULL plan");
+        check_range(plan, view_begin, view_count);
+        DeviceGuard dg(plan->device);
+        prepare(plan, proj_dev, plan_workspace(plan, workspace), static_cast<int>(view_begin),
+                static_cast<int>(view_count), static_cast<cudaStream_t>(stream));
+    });
+}
+
+gct_status gct_fdk_backproject(gct_fdk_plan *plan, const void *workspace, float *vol_dev, uint32_t view_begin,
+                               uint32_t view_count, int32_t accumulate, void *stream)
+{
+    return guarded([&] {
+        if (!plan || !vol_dev) gct::fail(GCT_ERR_INVALID_ARG, "NULL argument");
+        check_range(plan, view_begin, view_count);
+        DeviceGuard dg(plan->device);
+        const void *ws = workspace ? workspace : plan->work.p;
+        if (!ws) gct::fail(GCT_ERR_INVALID_ARG, "no workspace: run gct_fdk_prepare first or pass one");
+        run_backproject(plan, ws, vol_dev, static_cast<int>(view_begin), static_cast<int>(view_count),
+                        accumulate != 0, static_cast<cudaStream_t>(stream));
+    });
+}
+
+gct_status gct_fdk_execute_host(gct_fdk_plan *plan, const float *proj_host, float *vol_host, void *stream)
+{
+    return guarded([&] {
+        if (!plan) gct::fail(GCT_ERR_INVALID_ARG, "NULL plan");
+        DeviceGuard dg(plan->device);
+        execute_host(plan, proj_host, vol_host, static_cast<cudaStream_t>(stream));
+    });
+}
+
+gct_status gct_reconstruct_ex(const gct_ct_geom *geom, const gct_vol_geom *vol,
+                              const gct_filt_params *filt, const gct_fdk_opts *opts,
+                              const float *proj_host, float *vol_host)
+{
+    return guarded([&] {
+        if (!proj_host || !vol_host) gct::fail(GCT_ERR_INVALID_ARG, "NULL projection or volume pointer");
+        PlanHolder h;
+        h.p = new gct_fdk_plan();
+        build_plan(h.p, geom, vol, filt, opts);
+        gct_fdk_plan *p = h.p;
+        const size_t proj_n = static_cast<size_t>(p->nv) * p->nr * p->nc;
+        const size_t vol_n = static_cast<size_t>(p->vol.nx) * p->vol.ny * p->vol.nz;
+        DevBuf<float> dproj, dvol;
+        dproj.alloc(proj_n, "projection stack");
+        dvol.alloc(vol_n, "volume");
+        cudaStream_t s = nullptr;
+        cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+        std::unique_ptr<CUstream_st, void (*)(cudaStream_t)> sg(s, [](cudaStream_t x) { cudaStreamDestroy(x); });
+        cuda_check(cudaMemcpyAsync(dproj.p, proj_host, proj_n * sizeof(float), cudaMemcpyHostToDevice, s),
+                   "projection upload");
+        execute(p, dproj.p, dvol.p, nullptr, s);
+        cuda_check(cudaMemcpyAsync(vol_host, dvol.p, vol_n * sizeof(float), cudaMemcpyDeviceToHost, s),
+                   "volume download");
+        cuda_check(cudaStreamSynchronize(s), "reconstruction");
+    });
+}
+
+gct_status gct_reconstruct(const gct_ct_geom *geom, const gct_vol_geom *vol, const float *proj_host,
+                           float *vol_host)
+{
+    return gct_reconstruct_ex(geom, vol, nullptr, nullptr, proj_host, vol_host);
+}
+
+namespace {
+std::vector<gct::ProjView> proj_views(const gct_ct_geom &g)
+{
+    const auto kind = static_cast<gct_geom_kind>(g.kind);
+    std::vector<gct::ProjView> pv(g.num_views);
+    for (unsigned v = 0; v < g.num_views; ++v) {
+        const gct::ViewDerived d = gct::derive_view(kind, g, v);
+        gct::ProjView &o = pv[v];
+        for (int i = 0; i < 3; ++i) {
+            o.src[i] = d.src[i];
+            o.eu[i] = d.eu[i];
+            o.ev[i] = d.ev[i];
+            o.ew[i] = d.ew[i];
+        }
+        o.sdd = d.sdd;
+        o.c0 = d.c0;
+        o.r0 = d.r0;
+        o.extra = d.theta;
+        o.zscale = (kind == GCT_GEOM_CONE_PARALLEL) ? d.sid / d.sdd : 1.0;
+    }
+    return pv;
+}
+}  // namespace
+
+gct_status gct_phantom_project(const gct_ct_geom *geom, const gct_ellipsoid *ellipsoids,
+                               uint32_t num_ellipsoids, float *proj_dev, void *stream)
+{
+    return guarded([&] {
+        gct::check_ct_geom(geom);
+        if (!proj_dev || (num_ellipsoids && !ellipsoids)) gct::fail(GCT_ERR_INVALID_ARG, "NULL argument");
+        const auto kind = static_cast<gct_geom_kind>(geom->kind);
+        const auto pv = proj_views(*geom);
+        const cudaStream_t s = static_cast<cudaStream_t>(stream);
+        DevBuf<gct::ProjView> dv;
+        DevBuf<gct_ellipsoid> de;
+        dv.upload(pv.data(), pv.size(), "phantom geometry");
+        de.upload(ellipsoids, num_ellipsoids, "phantom ellipsoids");
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int nr = gct::is_2d_detector(kind) ? static_cast<int>(geom->det_col.num_samples) : 1;
+        gct::launch_phantom(dv.p, kind, static_cast<int>(geom->num_views), nr,
+                            static_cast<int>(geom->det_row.num_samples), geom->det_row.sampling_width,
+                            gct::is_2d_detector(kind) ? geom->det_col.sampling_width : 1.0, de.p,
+                            static_cast<int>(num_ellipsoids), !gct::is_2d_detector(kind), proj_dev, sms, s);
+        cuda_check(cudaGetLastError(), "phantom kernel launch");
+        cuda_check(cudaStreamSynchronize(s), "phantom projection");  // buffers are freed on return
+    });
+}
+
+gct_status gct_forward_project(const gct_ct_geom *geom, const gct_vol_geom *vol, const float *vol_dev,
+                               float step_vox, float *proj_dev, void *stream)
+{
+    return guarded([&] {
+        gct::check_ct_geom(geom);
+        const auto kind = static_cast<gct_geom_kind>(geom->kind);
+        const bool vol3d = gct::is_2d_detector(kind);
+        gct::check_vol_geom(vol, vol3d);
+        if (!vol_dev || !proj_dev) gct::fail(GCT_ERR_INVALID_ARG, "NULL argument");
+        if (!(step_vox > 0.f)) gct::fail(GCT_ERR_INVALID_ARG, "step must be positive");
+        const auto pv = proj_views(*geom);
+        gct::VolBox box{};
+        const unsigned n[3] = {vol->nx, vol->ny, vol->nz};
+        const double w[3] = {vol->dx, vol->dy, vol3d ? vol->dz : 1.0};
+        for (int a = 0; a < 3; ++a) {
+            const double mid = (a == 2 && !vol3d) ? 0.0 : vol->mid[a];
+            box.w[a] = w[a];
+            box.lo[a] = mid - (n[a] - 1.0) * w[a] / 2.0;
+            box.hi[a] = mid + (n[a] - 1.0) * w[a] / 2.0;
+        }
+        box.nx = static_cast<int>(vol->nx);
+        box.ny = static_cast<int>(vol->ny);
+        box.nz = static_cast<int>(vol->nz);
+        box.planar = !vol3d;
+        const cudaStream_t s = static_cast<cudaStream_t>(stream);
+        DevBuf<gct::ProjView> dv;
+        dv.upload(pv.data(), pv.size(), "projector geometry");
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int nr = vol3d ? static_cast<int>(geom->det_col.num_samples) : 1;
+        gct::launch_forward(dv.p, kind, static_cast<int>(geom->num_views), nr,
+                            static_cast<int>(geom->det_row.num_samples), geom->det_row.sampling_width,
+                            vol3d ? geom->det_col.sampling_width : 1.0, vol_dev, box, step_vox, proj_dev, sms, s);
+        cuda_check(cudaGetLastError(), "forward projector launch");
+        cuda_check(cudaStreamSynchronize(s), "forward projection");
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,471 @@
+// Host-side FP64 geometry. Each function cites the reference routine whose behaviour it keeps;
+// the arithmetic is done in double instead of the reference's float.
+#include "geometry.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <numeric>
+
+namespace gct {
+
+namespace {
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kTwoPi = 2.0 * kPi;
+
+double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+double norm3(const double *a) { return std::sqrt(dot3(a, a)); }
+void cross3(const double *a, const double *b, double *c)
+{
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+}  // namespace
+
+[[noreturn]] void fail(gct_status s, const std::string &msg) { throw GctError{s, msg}; }
+
+Family family_of(gct_geom_kind kind)
+{
+    switch (kind) {
+        case GCT_GEOM_PARALLEL_1D:
+        case GCT_GEOM_PARALLEL_2D:
+        case GCT_GEOM_CONE_PARALLEL: return Family::Affine;
+        case GCT_GEOM_FAN_LINE:
+        case GCT_GEOM_CONE_FLAT: return Family::Projective;
+        case GCT_GEOM_FAN_ARC:
+        case GCT_GEOM_CONE_CYL: return Family::Arc;
+    }
+    fail(GCT_ERR_INVALID_ARG, "unknown geometry kind");
+}
+
+bool is_2d_detector(gct_geom_kind kind) { return kind >= GCT_GEOM_PARALLEL_2D; }
+
+// src/cpp/geom/utils.h:338-348 (wrapFrom0To2PI).
+double wrap_0_2pi(double a)
+{
+    while (a < 0.0) a += kTwoPi;
+    return (a >= kTwoPi) ? std::remainder(a, kTwoPi) : a;
+}
+
+// src/cpp/geom/utils.h:370-389 (quadrantIndex).
+unsigned quadrant_index(double a)
+{
+    const double w = wrap_0_2pi(a);
+    if (w >= 0.0 && w < kPi / 2.0) return 1u;
+    if (w >= kPi / 2.0 && w < kPi) return 2u;
+    if (w >= kPi && w < 1.5 * kPi) return 3u;
+    return 4u;
+}
+
+// src/cpp/geom/rotation_geom.cpp:255-295 (Detail::rotAng).
+double view_rot_angle(gct_geom_kind kind, const gct_view_geom &v)
+{
+    if (family_of(kind) == Family::Affine) return wrap_0_2pi(v.rot_ang);
+    return wrap_0_2pi(std::atan2(v.src_pos[1], v.src_pos[0]));
+}
+
+// src/cpp/geom/rotation_geom.cpp:7-43 (Detail::rotDir).
+bool rotation_dir(const std::vector<double> &ang, int *dir)
+{
+    if (ang.size() < 2) return false;
+    const double a0 = wrap_0_2pi(ang[0]), a1 = wrap_0_2pi(ang[1]);
+    const unsigned q0 = quadrant_index(a0), q1 = quadrant_index(a1);
+    if (q0 == 1u && q1 == 4u) {
+        *dir = GCT_ROT_CCW;
+    } else if (q0 == 4u && q1 == 1u) {
+        *dir = GCT_ROT_CW;
+    } else {
+        const double diff = a1 - a0;
+        if (diff > 0.0)
+            *dir = GCT_ROT_CW;
+        else if (diff < 0.0)
+            *dir = GCT_ROT_CCW;
+        else
+            return false;
+    }
+    return true;
+}
+
+// src/cpp/geom/rotation_geom.cpp:45-74 (Detail::relRotAngles).
+bool rel_rot_angles(const std::vector<double> &ang, std::vector<double> *rel)
+{
+    int dir = 0;
+    if (!rotation_dir(ang, &dir)) return false;
+    rel->clear();
+    rel->reserve(ang.size());
+    const double first = ang.front();
+    for (double a : ang) rel->push_back(wrap_0_2pi(dir == GCT_ROT_CCW ? first - a : a - first));
+    return true;
+}
+
+// src/cpp/geom/rotation_geom.cpp:76-91 (Detail::rotAngIncr): mean of wrapped differences.
+bool rot_ang_incr(const std::vector<double> &rel, double *incr)
+{
+    if (rel.empty()) return false;
+    double sum = 0.0;
+    for (size_t i = 0; i + 1 < rel.size(); ++i) sum += wrap_0_2pi(rel[i + 1] - rel[i]);
+    *incr = sum / static_cast<double>(rel.size() - 1);
+    return true;
+}
+
+// src/cpp/geom/rotation_geom.cpp:93-104 (Detail::rotAngRange).
+bool rot_ang_range(const std::vector<double> &rel, double *range)
+{
+    double incr = 0.0;
+    if (!rot_ang_incr(rel, &incr)) return false;
+    *range = incr + *std::max_element(rel.begin(), rel.end());
+    return true;
+}
+
+// src/cpp/geom/rotation_geom.cpp:106-134 (Detail::numProjPerRot).
+bool num_proj_per_rot(const std::vector<double> &rel, unsigned *n)
+{
+    if (rel.empty() || rel.front() != 0.0) return false;
+    for (size_t i = 1; i < rel.size(); ++i) {
+        if (std::fabs(rel[i]) < 1e-6) {
+            *n = static_cast<unsigned>(i);
+            return true;
+        }
+    }
+    *n = static_cast<unsigned>(rel.size());
+    return true;
+}
+
+// src/cpp/geom/rotation_geom.h:90-115 (getRotationGeom).
+bool rotation_info(const gct_ct_geom &g, RotationInfo *out)
+{
+    const auto kind = static_cast<gct_geom_kind>(g.kind);
+    out->rot_ang.resize(g.num_views);
+    for (unsigned v = 0; v < g.num_views; ++v) out->rot_ang[v] = view_rot_angle(kind, g.views[v]);
+    if (!rotation_dir(out->rot_ang, &out->dir)) return false;
+    if (!rel_rot_angles(out->rot_ang, &out->rel_rot_ang)) return false;
+    if (!rot_ang_incr(out->rel_rot_ang, &out->incr)) return false;
+    if (!rot_ang_range(out->rel_rot_ang, &out->range)) return false;
+    if (!num_proj_per_rot(out->rel_rot_ang, &out->num_proj_per_rot)) return false;
+    return true;
+}
+
+void check_ct_geom(const gct_ct_geom *g)
+{
+    if (!g) fail(GCT_ERR_INVALID_ARG, "geometry is NULL");
+    if (g->kind < GCT_GEOM_PARALLEL_1D || g->kind > GCT_GEOM_CONE_FLAT)
+        fail(GCT_ERR_INVALID_ARG, "unknown geometry kind " + std::to_string(g->kind));
+    const auto kind = static_cast<gct_geom_kind>(g->kind);
+    if (g->num_views == 0 || !g->views)
+        fail(GCT_ERR_INVALID_ARG, "Empty collection of projection geometry.");
+    if (g->det_row.num_samples == 0 || !(g->det_row.sampling_width > 0.0))
+        fail(GCT_ERR_INVALID_ARG, "detector row sampler must have samples and a positive width");
+    if (is_2d_detector(kind)) {
+        if (g->det_col.num_samples == 0 || !(g->det_col.sampling_width > 0.0))
+            fail(GCT_ERR_INVALID_ARG, "detector column sampler must have samples and a positive width");
+    } else if (g->det_col.num_samples > 1) {
+        fail(GCT_ERR_INVALID_ARG, "1D detector kinds take det_col.num_samples <= 1");
+    }
+    if (g->det_row.num_samples > 16384 || (is_2d_detector(kind) && g->det_col.num_samples > 65536))
+        fail(GCT_ERR_NOT_SUPPORTED, "detector larger than 16384 columns or 65536 rows");
+}
+
+void check_vol_geom(const gct_vol_geom *v, bool volume_3d)
+{
+    if (!v) fail(GCT_ERR_INVALID_ARG, "volume geometry is NULL");
+    // src/cpp/geom/recon_img_geom.h:57-70 (isSamplingValid).
+    if (v->nx == 0 || v->ny == 0 || v->nz == 0)
+        fail(GCT_ERR_INVALID_ARG, "The number of samples in any dimension cannot be zero.");
+    if (!(v->dx > 0.0) || !(v->dy > 0.0) || (volume_3d && !(v->dz > 0.0)))
+        fail(GCT_ERR_INVALID_ARG,
+             "The sampling width of the image in any dimension cannot be zero or negative.");
+    if (!volume_3d && v->nz != 1) fail(GCT_ERR_INVALID_ARG, "2D images take nz = 1");
+}
+
+// src/cpp/io/geom_reader/proj_geom_factory_params.cpp:8-108 with the cone-beam rotation of
+// proj_geom_cb_factory.cpp:14-48 (R_z(dir*theta) applied to the basis u=(0,1,0), v=(0,0,-1),
+// w=(-1,0,0) and to the source (SID, 0, -pitch*theta)) and the fan-beam reduction of
+// proj_geom_fb_factory.cpp:13-45 (keep x, y; the fan-beam path drops the pitch).
+gct_view_geom make_view(gct_geom_kind kind, const gct_geom_params &p, unsigned idx)
+{
+    gct_view_geom v{};
+    const double theta = p.init_ang + p.ang_incr * static_cast<double>(idx);
+    v.det_row_center = p.det_row_center;
+    if (family_of(kind) == Family::Affine) {
+        v.rot_ang = theta;
+        if (kind != GCT_GEOM_PARALLEL_1D) v.det_col_center = p.det_col_center;
+        if (kind == GCT_GEOM_CONE_PARALLEL) {
+            v.src_det_dist = p.src_det_dist;
+            v.src_iso_dist = p.src_iso_dist;
+        }
+        return v;
+    }
+    const bool fan = !is_2d_detector(kind);
+    const double phi = static_cast<double>(p.rot_dir) * theta;
+    const double c = std::cos(phi), s = std::sin(phi);
+    const double pitch = fan ? 0.0 : p.hel_pitch;
+    v.src_det_dist = p.src_det_dist;
+    v.src_iso_dist = p.src_iso_dist;
+    v.src_pos[0] = p.src_iso_dist * c;
+    v.src_pos[1] = p.src_iso_dist * s;
+    v.src_pos[2] = fan ? 0.0 : -pitch * theta;
+    v.det_row_dir[0] = -s;
+    v.det_row_dir[1] = c;
+    v.det_row_dir[2] = 0.0;
+    if (!fan) {
+        v.det_col_center = p.det_col_center;
+        v.det_col_dir[0] = 0.0;
+        v.det_col_dir[1] = 0.0;
+        v.det_col_dir[2] = -1.0;
+    }
+    if (kind == GCT_GEOM_FAN_ARC || kind == GCT_GEOM_CONE_CYL) {
+        v.iso_ray_dir[0] = -c;
+        v.iso_ray_dir[1] = -s;
+        v.iso_ray_dir[2] = 0.0;
+    }
+    return v;
+}
+
+// src/cpp/recon/ramp_filter.h:22-56 (RampFilter::kernel, M(t), apodFact in ramp_filter.cpp:5-20)
+// and src/cpp/recon/proj_filt_kernel.cpp:5-45 (projFiltKernel, (b/sin b)^2 for the arc).
+std::vector<double> ramp_taps(gct_geom_kind kind, const gct_detector &det_row,
+                              const gct_filt_params &fp)
+{
+    const int n = static_cast<int>(det_row.num_samples);
+    const double a = fp.apod_func == GCT_APOD_HANN ? 0.5 : fp.apod_func == GCT_APOD_HAMMING ? 0.54 : 1.0;
+    const double fc = fp.cut_off_freq;
+    const double sw = det_row.sampling_width;
+    auto M = [](double t) { return t == 0.0 ? 0.5 : std::sin(t) / t + (std::cos(t) - 1.0) / (t * t); };
+    std::vector<double> h(n);
+    const bool arc = kind == GCT_GEOM_FAN_ARC || kind == GCT_GEOM_CONE_CYL;
+    for (int j = 0; j < n; ++j) {
+        const int off = j - n / 2;
+        const double nd = static_cast<double>(off);
+        double c = (fc * fc / (2.0 * sw)) *
+                   (a * M(fc * kPi * nd) + ((1.0 - a) / 2.0) * M(kPi * fc * nd + kPi) +
+                    ((1.0 - a) / 2.0) * M(kPi * fc * nd - kPi));
+        if (arc && off != 0) {
+            const double beta = nd * sw;
+            const double r = beta / std::sin(beta);
+            c *= r * r;
+        }
+        h[j] = c;
+    }
+    return h;
+}
+
+// src/cuda/recon/parker_weighting.cuh:19-58 (fanAngle, fanAngleDet), :80-105 (parkerWeightFan),
+// :132-176 (getParkerWeights; fan angles from view 0, relative angles reversed for CCW, weights
+// only when the range exceeds pi) and :181-200 (parallel kinds: 1 or 0.5).
+std::vector<double> parker_table(const gct_ct_geom &g, const RotationInfo &ri)
+{
+    const auto kind = static_cast<gct_geom_kind>(g.kind);
+    const unsigned nc = g.det_row.num_samples, nv = g.num_views;
+    std::vector<double> w(static_cast<size_t>(nc) * nv, 1.0);
+    if (family_of(kind) == Family::Affine) {
+        const bool half = ri.incr > 0.0 && ri.range <= ri.incr + kPi;
+        std::fill(w.begin(), w.end(), half ? 1.0 : 0.5);
+        return w;
+    }
+    if (!(ri.range > kPi)) return w;  // reference leaves these uninitialised; defined as 1 here
+    const gct_view_geom &v0 = g.views[0];
+    const bool arc = kind == GCT_GEOM_FAN_ARC || kind == GCT_GEOM_CONE_CYL;
+    std::vector<double> gamma(nc);
+    for (unsigned c = 0; c < nc; ++c) {
+        const double t = (static_cast<double>(c) - v0.det_row_center) * g.det_row.sampling_width;
+        gamma[c] = arc ? t : std::atan2(t, v0.src_det_dist);
+    }
+    std::vector<double> rel = ri.rel_rot_ang;
+    if (ri.dir == GCT_ROT_CCW) std::reverse(rel.begin(), rel.end());
+    const double phi = ri.range;
+    for (unsigned v = 0; v < nv; ++v) {
+        const double b = rel[v];
+        for (unsigned c = 0; c < nc; ++c) {
+            const double gm = gamma[c];
+            const double t2 = 2.0 * gm + phi - kPi, t3 = 2.0 * gm + kPi, t4 = phi;
+            double wt = 0.0;
+            if (b >= 0.0 && b <= t2) {
+                const double s = std::sin(kPi * b / (2.0 * (phi - kPi) + 4.0 * gm));
+                wt = s * s;
+            } else if (b >= t2 && b <= t3) {
+                wt = 1.0;
+            } else if (b >= t3 && b <= t4) {
+                const double s = std::sin(kPi * (phi - b) / (2.0 * (phi - kPi) - 4.0 * gm));
+                wt = s * s;
+            }
+            w[static_cast<size_t>(v) * nc + c] = wt;
+        }
+    }
+    return w;
+}
+
+unsigned fft_length(unsigned n)
+{
+    const long need = std::max<long>(2L * n - 2 - n / 2, static_cast<long>(n) - 1 + n / 2);
+    unsigned L = 64;
+    while (static_cast<long>(L) <= need) L *= 2u;
+    return L;
+}
+
+std::vector<std::complex<double>> filter_spectrum(const std::vector<double> &taps, unsigned L)
+{
+    const int n = static_cast<int>(taps.size());
+    std::vector<double> hc(L, 0.0);
+    for (int j = 0; j < n; ++j) {
+        const int off = j - n / 2;
+        hc[static_cast<unsigned>((off % static_cast<int>(L) + static_cast<int>(L)) % static_cast<int>(L))] += taps[j];
+    }
+    std::vector<double> cs(L), sn(L);
+    for (unsigned m = 0; m < L; ++m) {
+        cs[m] = std::cos(kTwoPi * m / L);
+        sn[m] = std::sin(kTwoPi * m / L);
+    }
+    std::vector<std::complex<double>> H(L);
+    for (unsigned k = 0; k < L; ++k) {
+        double re = 0.0, im = 0.0;
+        for (unsigned m = 0; m < L; ++m) {
+            if (hc[m] == 0.0) continue;
+            const unsigned idx = static_cast<unsigned>((static_cast<unsigned long long>(k) * m) % L);
+            re += hc[m] * cs[idx];
+            im -= hc[m] * sn[idx];
+        }
+        H[k] = std::complex<double>(re / L, im / L);
+    }
+    return H;
+}
+
+// Per-view quantities as the reference's CTGeomDev stores them (src/cuda/geom/ct_geom_dev.cu:
+// SID = |src_pos| for the fan and cone kinds (:84, :145, :302, :398), the fan-line iso-ray as
+// rot90(det_row_dir) (:154), the flat detector normal as det_row_dir x det_col_dir (:407)).
+ViewDerived derive_view(gct_geom_kind kind, const gct_ct_geom &g, unsigned vi)
+{
+    const gct_view_geom &v = g.views[vi];
+    ViewDerived d;
+    d.c0 = v.det_row_center;
+    d.r0 = is_2d_detector(kind) ? v.det_col_center : 0.0;
+    d.theta = v.rot_ang;
+    const bool fan1d = kind == GCT_GEOM_FAN_ARC || kind == GCT_GEOM_FAN_LINE;
+    switch (kind) {
+        case GCT_GEOM_PARALLEL_1D:
+        case GCT_GEOM_PARALLEL_2D: d.bp_const = 1.0; break;
+        case GCT_GEOM_CONE_PARALLEL:
+            d.sdd = v.src_det_dist;
+            d.sid = v.src_iso_dist;
+            d.bp_const = 1.0;
+            break;
+        default: {
+            d.sdd = v.src_det_dist;
+            for (int i = 0; i < 3; ++i) {
+                d.src[i] = v.src_pos[i];
+                d.eu[i] = v.det_row_dir[i];
+            }
+            if (fan1d) {
+                d.src[2] = 0.0;
+                d.eu[2] = 0.0;
+            }
+            d.sid = norm3(d.src);
+            if (kind == GCT_GEOM_FAN_LINE) {
+                d.ew[0] = -d.eu[1];
+                d.ew[1] = d.eu[0];
+                d.ew[2] = 0.0;
+            } else if (kind == GCT_GEOM_CONE_FLAT) {
+                for (int i = 0; i < 3; ++i) d.ev[i] = v.det_col_dir[i];
+                cross3(d.eu, d.ev, d.ew);
+            } else {  // arc kinds
+                for (int i = 0; i < 3; ++i) d.ew[i] = v.iso_ray_dir[i];
+                if (fan1d) d.ew[2] = 0.0;
+                if (kind == GCT_GEOM_CONE_CYL)
+                    for (int i = 0; i < 3; ++i) d.ev[i] = v.det_col_dir[i];
+            }
+            d.bp_const = (family_of(kind) == Family::Projective) ? d.sdd * d.sid : d.sid;
+            break;
+        }
+    }
+    return d;
+}
+
+// Per-view coefficients in voxel-index space (i, j, k) -> detector pixel coordinates.
+// Voxel centres follow src/cuda/geom/coord_trans_img.cuh:52-66: first = mid - (n-1)*w/2.
+// Mapping formulas follow src/cuda/geom/coord_trans_proj.cuh:157-345 (projMapping) with
+// DCSToPCS (:142-145): pixel = coord / width + centre.
+std::vector<float> bp_coefficients(const gct_ct_geom &g, const gct_vol_geom &vol,
+                                   const std::vector<ViewDerived> &vd,
+                                   const std::vector<double> &wscale, bool *z_affine)
+{
+    const auto kind = static_cast<gct_geom_kind>(g.kind);
+    const bool vol3d = is_2d_detector(kind);
+    const double X0[3] = {vol.mid[0] - (vol.nx - 1.0) * vol.dx / 2.0,
+                          vol.mid[1] - (vol.ny - 1.0) * vol.dy / 2.0,
+                          vol3d ? vol.mid[2] - (vol.nz - 1.0) * vol.dz / 2.0 : 0.0};
+    const double DX[3] = {vol.dx, vol.dy, vol3d ? vol.dz : 0.0};
+    const double du = g.det_row.sampling_width;
+    const double dv = vol3d ? g.det_col.sampling_width : 1.0;
+    std::vector<float> out(static_cast<size_t>(g.num_views) * kCoefPerView, 0.0f);
+    bool affine_z = true;
+    // affine form of e . (X - S): value at (0,0,0) and slopes per index step.
+    auto aff = [&](const double *e, const double *S, double *c4) {
+        double base[3];
+        for (int i = 0; i < 3; ++i) base[i] = X0[i] - S[i];
+        c4[0] = dot3(e, base);
+        for (int i = 0; i < 3; ++i) c4[1 + i] = e[i] * DX[i];
+    };
+    for (unsigned v = 0; v < g.num_views; ++v) {
+        const ViewDerived &d = vd[v];
+        float *c = &out[static_cast<size_t>(v) * kCoefPerView];
+        switch (family_of(kind)) {
+            case Family::Affine: {
+                // detCoordAxialParallel (coord_trans_proj.cuh:157-166): x cos(t+pi/2) + y sin(t+pi/2).
+                const double t = d.theta + kPi / 2.0;
+                const double ct = std::cos(t), st = std::sin(t);
+                c[0] = static_cast<float>((X0[0] * ct + X0[1] * st) / du + d.c0);
+                c[1] = static_cast<float>(DX[0] * ct / du);
+                c[2] = static_cast<float>(DX[1] * st / du);
+                double vk = 0.0, v0 = 0.0;
+                if (kind == GCT_GEOM_PARALLEL_2D) {  // t = -z
+                    v0 = -X0[2] / dv + d.r0;
+                    vk = -DX[2] / dv;
+                } else if (kind == GCT_GEOM_CONE_PARALLEL) {  // t = -z * SDD / SID
+                    const double m = d.sdd / d.sid;
+                    v0 = -X0[2] * m / dv + d.r0;
+                    vk = -DX[2] * m / dv;
+                }
+                c[3] = static_cast<float>(v0);
+                c[4] = static_cast<float>(vk);
+                c[5] = static_cast<float>(wscale[v]);
+                break;
+            }
+            case Family::Projective: {
+                double U[4], V[4] = {0, 0, 0, 0}, D[4];
+                aff(d.eu, d.src, U);
+                aff(d.ew, d.src, D);
+                if (vol3d) aff(d.ev, d.src, V);
+                for (int i = 0; i < 4; ++i) {
+                    c[i] = static_cast<float>(d.sdd / du * U[i] + d.c0 * D[i]);
+                    c[4 + i] = vol3d ? static_cast<float>(d.sdd / dv * V[i] + d.r0 * D[i]) : 0.0f;
+                    c[8 + i] = static_cast<float>(D[i]);
+                }
+                c[12] = static_cast<float>(wscale[v]);
+                if (U[3] != 0.0 || D[3] != 0.0) affine_z = false;
+                break;
+            }
+            case Family::Arc: {
+                double A[4], B[4], T[4] = {0, 0, 0, 0};
+                aff(d.eu, d.src, A);
+                aff(d.ew, d.src, B);
+                if (vol3d) aff(d.ev, d.src, T);
+                for (int i = 0; i < 4; ++i) {
+                    c[i] = static_cast<float>(A[i]);
+                    c[4 + i] = static_cast<float>(B[i]);
+                    c[8 + i] = static_cast<float>(T[i]);
+                }
+                c[12] = static_cast<float>(1.0 / du);
+                c[13] = static_cast<float>(d.c0);
+                c[14] = static_cast<float>(vol3d ? d.sdd / dv : 0.0);
+                c[15] = static_cast<float>(d.r0);
+                c[16] = static_cast<float>(wscale[v]);
+                if (A[3] != 0.0 || B[3] != 0.0 || T[1] != 0.0 || T[2] != 0.0) affine_z = false;
+                break;
+            }
+        }
+    }
+    *z_affine = affine_z;
+    return out;
+}
+
+}  // namespace gct

@@ -1,0 +1,58 @@
+// Host-side launch interfaces of the FDK kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gct {
+
+// Zero padding (entries per side) of the bilinear-quad layout of filtered projections.
+constexpr int kQuadPad = 2;
+
+enum FilterOut : int { kOutPlainF32 = 0, kOutQuadF32 = 1, kOutQuadF16 = 2 };
+
+struct FilterArgs {
+    const float *proj = nullptr;   // [nv][nr][nc] raw projections
+    int nv = 0, nr = 0, nc = 0;
+    int kind = 0;                  // gct_geom_kind
+    float du = 0.f, dv = 0.f;      // row / column sampler widths
+    const float4 *fview = nullptr; // per view: (det_row_center, det_col_center, sdd, 0)
+    const float *parker = nullptr; // [nv][nc]
+    const float2 *H = nullptr;     // [L] filter spectrum, scaled by 1/L
+    const float2 *twiddle = nullptr; // [L] exp(-2 pi i m / L)
+    int mode = kOutPlainF32;
+    void *out = nullptr;           // plain: [nv][nr][nc] f32; quads: [nv][nr+4][nc+4]
+    const float *vscale = nullptr; // per-view output scale for quads (nullable = 1)
+};
+
+// Fused cosine + Parker weighting, zero padding, FFT convolution with the ramp filter and the
+// epilogue into the requested layout. L is the power-of-two FFT length.
+void launch_filter_fft(const FilterArgs &a, int L, int num_sms, cudaStream_t s);
+size_t filter_fft_smem_bytes(int L);
+
+// Per-view |max| of the raw projections (amax must be zeroed) and the FP16 power-of-two scale
+// that maps the bound amax * l1 (l1 = sum |taps|) below 2^14; writes vscale and 1/vscale.
+void launch_view_absmax(const float *proj, int nv, long long pix_per_view, float *amax,
+                        cudaStream_t s);
+void launch_view_scales(const float *amax, int nv, float l1, float *vscale, float *vinv,
+                        cudaStream_t s);
+
+struct BpArgs {
+    const void *quads = nullptr;
+    int qpitch = 0;                // nc + 4
+    long long qview = 0;           // (nr + 4) * (nc + 4)
+    const float *coefs = nullptr;  // [nv][kCoefPerView]
+    const float *vinv = nullptr;   // per-view scale of the stored values (nullable = 1)
+    int v_begin = 0, v_count = 0;
+    float *vol = nullptr;
+    int nx = 0, ny = 0, nz = 0;
+    float umax = 0.f, vmax = 0.f;  // nc, nr
+    int accumulate = 0;
+};
+
+// Voxel-driven backprojection. family: 0 affine, 1 projective, 2 arc. storage: 0 f32, 1 f16.
+// z_affine selects the column kernel (u and the denominator constant along z).
+void launch_backproject(const BpArgs &a, int family, int storage, bool z_affine, int zpt,
+                        int bx, int by, cudaStream_t s);
+
+}  // namespace gct

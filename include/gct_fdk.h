@@ -1,0 +1,299 @@
+/*
+ * gct_fdk.h -- C ABI of the B200-native FDK (Feldkamp-Davis-Kress) reconstruction engine.
+ *
+ * This is the drop-in boundary for GCT's axial FDK path. Every entry point below names the
+ * reference interface it replaces (paths are relative to the satidev/gct project root).
+ * The ABI uses plain C types only: pointers, sizes, doubles and PODs. No C++ or torch types
+ * cross it, so a ctypes / cgo / JNI / N-API binding needs nothing but this file.
+ *
+ * Conventions
+ *   - Every function returns gct_status. GCT_OK is 0. On failure, gct_last_error_string()
+ *     returns a thread-local, human-readable message. The reference reports the same
+ *     conditions with std::runtime_error / std::invalid_argument
+ *     (src/cuda/utils/check_error.cu:6-36); the C++ header gct_fdk.hpp turns a non-OK
+ *     status back into std::runtime_error.
+ *   - Geometry is FP64 on the host. Projections and volumes are float32.
+ *   - Projection stack layout: [view][row][col], col fastest
+ *     (src/cpp/data/projection_stack.h:12-36). A 1D detector has one row.
+ *   - Volume layout: [z][y][x], x fastest (src/cpp/data/recon_img.h:20-33). A 2D image has
+ *     nz = 1.
+ *   - "stream" arguments are cudaStream_t passed as void*; NULL is the legacy default stream.
+ *   - Device pointers must live on the device that is current when the plan was created.
+ */
+#ifndef GCT_FDK_H
+#define GCT_FDK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GCT_FDK_ABI_VERSION 1
+
+typedef enum gct_status {
+    GCT_OK = 0,
+    GCT_ERR_INVALID_ARG = 1,   /* bad geometry, sizes or pointers */
+    GCT_ERR_OUT_OF_MEMORY = 2, /* a device or host allocation failed */
+    GCT_ERR_BUDGET = 3,        /* request does not fit the configured device-memory budget */
+    GCT_ERR_TIMEOUT = 4,       /* a bounded wait ran out */
+    GCT_ERR_CUDA = 5,          /* a CUDA runtime call failed */
+    GCT_ERR_NOT_SUPPORTED = 6, /* option not available for this geometry or device */
+    GCT_ERR_NOT_READY = 7,     /* asynchronous work still in flight (poll again) */
+    GCT_ERR_CANCELLED = 8      /* request was cancelled before it ran */
+} gct_status;
+
+/* The seven axial detector configurations: GCT::Geom::ProjGeom<DetRow, DetCol...>
+ * (src/cpp/geom/proj_geom.h:21-103), i.e. the seven reconstruct() overloads
+ * (src/cuda/recon/recon_wrappers.cuh:15-43). */
+typedef enum gct_geom_kind {
+    GCT_GEOM_PARALLEL_1D = 0,   /* <DetParallel>                 -> 2D image */
+    GCT_GEOM_FAN_ARC = 1,       /* <DetFanArc>                   -> 2D image */
+    GCT_GEOM_FAN_LINE = 2,      /* <DetFanLine>                  -> 2D image */
+    GCT_GEOM_PARALLEL_2D = 3,   /* <DetParallel, DetParallel>    -> 3D volume */
+    GCT_GEOM_CONE_PARALLEL = 4, /* <DetParallel, DetFanLine>     -> 3D volume (rebinned) */
+    GCT_GEOM_CONE_CYL = 5,      /* <DetFanArc, DetFanLine>       -> 3D volume */
+    GCT_GEOM_CONE_FLAT = 6      /* <DetFanLine, DetFanLine>      -> 3D volume */
+} gct_geom_kind;
+
+/* Rotation direction: GCT::Geom::RotDir (src/cpp/geom/rotation_geom.h:10-14). */
+typedef enum gct_rot_dir { GCT_ROT_CCW = -1, GCT_ROT_CW = 1 } gct_rot_dir;
+
+/* Apodisation window: GCT::Recon::ApodFunc (src/cpp/io/parameters/filt_parameters.h:9-13). */
+typedef enum gct_apod_func { GCT_APOD_NONE = 0, GCT_APOD_HANN = 1, GCT_APOD_HAMMING = 2 } gct_apod_func;
+
+/* Uniform 1D detector sampler: GCT::Geom::Sampler1D (src/cpp/geom/sampling_info.h:144-153).
+ * sampling_width is in mm for DetParallel / DetFanLine and in radians for DetFanArc. */
+typedef struct gct_detector {
+    uint32_t num_samples;
+    double sampling_width;
+} gct_detector;
+
+/* Per-view projection geometry: the union of the ProjGeom<...> fields
+ * (src/cpp/geom/proj_geom.h:21-103). Fields a kind does not use are ignored.
+ *   PARALLEL_1D/2D : rot_ang, det_row_center (, det_col_center)
+ *   CONE_PARALLEL  : rot_ang, src_det_dist, src_iso_dist, det_row_center, det_col_center
+ *   FAN_LINE       : src_det_dist, det_row_center, src_pos[0..1], det_row_dir[0..1]
+ *   FAN_ARC        : FAN_LINE fields + iso_ray_dir[0..1]
+ *   CONE_FLAT      : src_det_dist, centres, src_pos, det_row_dir, det_col_dir
+ *   CONE_CYL       : CONE_FLAT fields + iso_ray_dir
+ * Distances in mm, angles in radians, centres in detector pixels. */
+typedef struct gct_view_geom {
+    double rot_ang;
+    double det_row_center;
+    double det_col_center;
+    double src_det_dist;
+    double src_iso_dist;
+    double src_pos[3];
+    double det_row_dir[3];
+    double det_col_dir[3];
+    double iso_ray_dir[3];
+} gct_view_geom;
+
+/* CT geometry of a scan: GCT::Geom::CTGeom / AxialCTGeom (src/cpp/geom/ct_geom.h:18-53,
+ * src/cpp/geom/axial_ct_geom.h:8-13). det_col.num_samples must be 1 for the 1D kinds. */
+typedef struct gct_ct_geom {
+    int32_t kind; /* gct_geom_kind */
+    gct_detector det_row;
+    gct_detector det_col;
+    uint32_t num_views;
+    const gct_view_geom *views; /* num_views entries, host memory */
+} gct_ct_geom;
+
+/* Reconstruction grid: GCT::Geom::ReconImgGeom<2|3> (src/cpp/geom/recon_img_geom.h:15-30).
+ * For a 2D image set nz = 1; dz and mid[2] are then ignored. */
+typedef struct gct_vol_geom {
+    uint32_t nx, ny, nz;
+    double dx, dy, dz;
+    double mid[3];
+} gct_vol_geom;
+
+/* Ramp-filter parameters: GCT::Recon::FiltParams (src/cpp/io/parameters/filt_parameters.h:14-18).
+ * The reference's defaults are cut_off_freq = 1 and GCT_APOD_NONE. */
+typedef struct gct_filt_params {
+    double cut_off_freq;
+    int32_t apod_func; /* gct_apod_func */
+} gct_filt_params;
+
+/* Rotation analysis: GCT::Geom::RotationGeom (src/cpp/geom/rotation_geom.h:16-24). */
+typedef struct gct_rotation_geom {
+    int32_t dir; /* gct_rot_dir */
+    double rot_ang_incr;
+    double rot_ang_range;
+    uint32_t num_proj_per_rot;
+} gct_rotation_geom;
+
+/* Ideal circular-trajectory parameters: the union of Parallel1DProjGeomParams,
+ * FanBeamProjGeomParams, Parallel2DProjGeomParams and ConeBeamProjGeomParams with their
+ * RotationParams (src/cpp/io/parameters/proj_geom_params.h:16-58). */
+typedef struct gct_geom_params {
+    double det_row_center;
+    double det_col_center;
+    double src_det_dist;
+    double src_iso_dist;
+    int32_t rot_dir; /* gct_rot_dir */
+    double init_ang;
+    double ang_incr;
+    uint32_t num_proj;
+    double hel_pitch;
+} gct_geom_params;
+
+/* Execution options. Zero-initialise for defaults. */
+enum {
+    GCT_FILTER_FFT = 0,             /* own row-batched shared-memory FFT, FP32 arithmetic */
+    GCT_FILTER_TOEPLITZ_BF16X3 = 1  /* 3-term split BF16 Toeplitz GEMM on tcgen05, FP32 accumulate */
+};
+enum {
+    GCT_STORAGE_F32 = 0, /* filtered projections kept in FP32 */
+    GCT_STORAGE_F16 = 1  /* filtered projections kept in FP16 with a per-view power-of-two scale */
+};
+typedef struct gct_fdk_opts {
+    int32_t filter;        /* GCT_FILTER_* */
+    int32_t storage;       /* GCT_STORAGE_* */
+    int32_t z_per_thread;  /* backprojection voxels per thread along z; 0 = tuned default */
+    int32_t block_x;       /* backprojection block shape; 0 = tuned default */
+    int32_t block_y;
+    int32_t reserved[3];
+} gct_fdk_opts;
+
+typedef struct gct_fdk_plan gct_fdk_plan;
+
+/* ---- version / errors ------------------------------------------------------------------ */
+int32_t gct_abi_version(void);
+const char *gct_last_error_string(void);
+
+/* ---- geometry (host, FP64) ------------------------------------------------------------- */
+
+/* Replaces GCT::Geom::ProjGeomFactory<DetRow, DetCol...>::create(params, proj_idx)
+ * (src/cpp/io/geom_reader/proj_geom_factory_params.cpp:8-108, with the rotation of
+ * src/cpp/io/geom_reader/proj_geom_cb_factory.cpp:14-48 and the fan-beam reduction of
+ * src/cpp/io/geom_reader/proj_geom_fb_factory.cpp:13-45), evaluated in FP64. */
+gct_status gct_proj_geom_create(int32_t kind, const gct_geom_params *params, uint32_t proj_idx,
+                                gct_view_geom *out);
+
+/* Replaces GCT::Geom::getRotationGeom (src/cpp/geom/rotation_geom.h:90-115,
+ * src/cpp/geom/rotation_geom.cpp:7-134). rot_ang / rel_rot_ang may be NULL; otherwise they
+ * receive num_views angles each. Returns GCT_ERR_INVALID_ARG where the reference returns
+ * std::nullopt (and CTGeom's constructor throws "Invalid X-ray source trajectory"). */
+gct_status gct_rotation_geom_get(const gct_ct_geom *geom, gct_rotation_geom *out,
+                                 double *rot_ang, double *rel_rot_ang);
+
+/* Replaces GCT::Recon::isValidAxialRecon (src/cpp/recon/check_validity.h:66-75).
+ * *valid receives 1 or 0; with verbose != 0 the reasons are printed to stderr. */
+gct_status gct_is_valid_axial_recon(const gct_ct_geom *geom, uint32_t proj_num_cols,
+                                    uint32_t proj_num_rows, uint32_t num_proj, int32_t verbose,
+                                    int32_t *valid);
+
+/* Replaces GCT::Recon::projFiltKernel / RampFilter::kernel
+ * (src/cpp/recon/proj_filt_kernel.cpp:5-45, src/cpp/recon/ramp_filter.h:29-56): the
+ * det_row.num_samples spatial taps, tap j at offset n = j - num_samples/2. FP64. */
+gct_status gct_ramp_filter_taps(int32_t kind, const gct_detector *det_row,
+                                const gct_filt_params *params, double *taps);
+
+/* Replaces GCT::Recon::CUDA::getParkerWeights (src/cuda/recon/parker_weighting.cuh:132-200):
+ * weights[view][col] (num_views x det_row.num_samples), window bounds in FP64. For fan and
+ * cone kinds whose angular range is <= pi the reference leaves its buffer uninitialised
+ * (parker_weighting.cuh:163-175); here those weights are defined as 1. */
+gct_status gct_parker_weights(const gct_ct_geom *geom, float *weights);
+
+/* ---- FDK plans (device) ---------------------------------------------------------------- */
+
+/* Builds a reusable reconstruction plan on the current CUDA device: FP64 per-view geometry,
+ * filter spectrum and Parker table, uploaded once. Replaces the per-call set-up inside
+ * GCT::Recon::CUDA::reconFDK (src/cuda/recon/fdk_axial.cuh:68-205): CTGeomDev, the
+ * RampFilteringFFT constructor and getParkerWeights. filt and opts may be NULL. */
+gct_status gct_fdk_plan_create(const gct_ct_geom *geom, const gct_vol_geom *vol,
+                               const gct_filt_params *filt, const gct_fdk_opts *opts,
+                               gct_fdk_plan **out);
+gct_status gct_fdk_plan_destroy(gct_fdk_plan *plan);
+
+/* Device bytes of scratch that gct_fdk_execute needs (the filtered-projection stack). */
+gct_status gct_fdk_plan_workspace_bytes(const gct_fdk_plan *plan, uint64_t *bytes);
+
+/* Full FDK on device buffers, asynchronous on `stream`: fused cosine + Parker weighting and
+ * ramp filtering, then backprojection and the angular-increment scale. proj_dev is
+ * [view][row][col] float32, vol_dev receives [z][y][x] float32 (overwritten). workspace may be
+ * NULL, in which case the plan allocates (once) and keeps its own. Replaces the device part of
+ * reconFDKHighMem (src/cuda/recon/fdk_axial.cuh:151-205). */
+gct_status gct_fdk_execute(gct_fdk_plan *plan, const float *proj_dev, float *vol_dev,
+                           void *workspace, void *stream);
+
+/* Stage entry points of the same plan, for tests and for callers that pipeline stages.
+ * gct_fdk_filter writes the weighted, ramp-filtered projections as plain float32
+ * [view][row][col] (what RampFilteringFFT::runFiltering leaves in the stack after
+ * runCosWeighting and runParkerWeighting, src/cuda/recon/fdk_axial.cuh:165-171), without the
+ * backprojection scales. */
+gct_status gct_fdk_filter(gct_fdk_plan *plan, const float *proj_dev, float *filtered_dev,
+                          void *stream);
+
+/* The two device stages of gct_fdk_execute over a view range [view_begin, view_begin+count):
+ *   gct_fdk_prepare      weights + ramp-filters those views of proj_dev (the full stack pointer)
+ *                        into the workspace in the backprojector's layout;
+ *   gct_fdk_backproject  backprojects those views of the workspace into vol_dev, overwriting it
+ *                        (accumulate = 0) or adding to it (accumulate = 1), angular scale included.
+ * Running prepare + backproject over all views equals gct_fdk_execute. Splitting the views lets a
+ * caller overlap uploads of later views with work on earlier ones (the streaming replacement for
+ * reconFDKLowMem, src/cuda/recon/fdk_axial.cuh:91-149). */
+gct_status gct_fdk_prepare(gct_fdk_plan *plan, const float *proj_dev, void *workspace,
+                           uint32_t view_begin, uint32_t view_count, void *stream);
+gct_status gct_fdk_backproject(gct_fdk_plan *plan, const void *workspace, float *vol_dev,
+                               uint32_t view_begin, uint32_t view_count, int32_t accumulate,
+                               void *stream);
+
+/* Host buffers through a plan: uploads proj_host in view chunks on a copy stream while earlier
+ * chunks are filtered and backprojected (accumulating) on `stream`, then downloads the volume and
+ * synchronises. Device staging buffers are owned by the plan and reused across calls. Pass pinned
+ * host memory for the copies to overlap. */
+gct_status gct_fdk_execute_host(gct_fdk_plan *plan, const float *proj_host, float *vol_host,
+                                void *stream);
+
+/* Host-to-host drop-in: replaces void GCT::Recon::CUDA::reconstruct(cg, proj, vol)
+ * (src/cuda/recon/recon_wrappers.cuh:15-43, recon_wrappers.cu:7-55). Synchronous, default
+ * FiltParams, FP32 path; proj_host and vol_host are plain host arrays. */
+gct_status gct_reconstruct(const gct_ct_geom *geom, const gct_vol_geom *vol,
+                           const float *proj_host, float *vol_host);
+
+/* Same as gct_reconstruct with explicit filter parameters and execution options. */
+gct_status gct_reconstruct_ex(const gct_ct_geom *geom, const gct_vol_geom *vol,
+                              const gct_filt_params *filt, const gct_fdk_opts *opts,
+                              const float *proj_host, float *vol_host);
+
+/* ---- projection (device) ---------------------------------------------------------------- */
+
+/* Analytic phantom: an ellipsoid with centre c (mm), semi-axes a (mm), rotation angle
+ * phi about z (radians) and attenuation mu (1/mm). For 2D kinds only x, y are used and the
+ * ellipsoid acts as an ellipse. */
+typedef struct gct_ellipsoid {
+    double center[3];
+    double semi_axes[3];
+    double phi;
+    double mu;
+} gct_ellipsoid;
+
+/* Exact line integrals of a sum of ellipsoids along every detector ray of the geometry,
+ * written to proj_dev [view][row][col]. Generates the synthetic inputs of the benchmarks. The
+ * reference has no counterpart (its inputs come from files). */
+gct_status gct_phantom_project(const gct_ct_geom *geom, const gct_ellipsoid *ellipsoids,
+                               uint32_t num_ellipsoids, float *proj_dev, void *stream);
+
+/* Ray-driven forward projector of a voxel volume (trilinear samples every step_vox voxel
+ * lengths along each ray), writing proj_dev [view][row][col]. Replaces the unfinished 1D
+ * parallel ray-marcher of src/cuda/recon/forward_proj.cuh:13-102 for all seven kinds. */
+gct_status gct_forward_project(const gct_ct_geom *geom, const gct_vol_geom *vol,
+                               const float *vol_dev, float step_vox, float *proj_dev,
+                               void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#endif /* GCT_FDK_H */

@@ -1,0 +1,80 @@
+"""Geometry cases shared by the tests: one builder per reference detector configuration.
+
+The parameters follow the reference's FDK integration tests (test/cuda/recon/fdk_axial_tests.cu:
+15-537) scaled down so the FP64 oracle finishes in seconds: 360 or fewer views over 360 degrees,
+detector centres at (n - 1) / 2, SID/SDD 500/1000 or 1000/1536, 1 mm voxels.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+import gct_b200 as g
+from oracle import oracle as orc
+
+KINDS = ["parallel_1d", "fan_arc", "fan_line", "parallel_2d", "cone_parallel", "cone_cyl", "cone_flat"]
+
+# seeded ellipses / ellipsoids (cx, cy, cz, ax, ay, az, phi, mu)
+PHANTOM = [
+    (0.0, 0.0, 0.0, 40.0, 34.0, 30.0, 0.0, 0.020),
+    (-12.0, 8.0, 4.0, 9.0, 14.0, 10.0, 0.4, 0.012),
+    (15.0, -10.0, -6.0, 7.0, 5.0, 8.0, -0.7, -0.008),
+    (3.0, 18.0, 2.0, 4.0, 6.0, 5.0, 1.1, 0.015),
+]
+
+
+@dataclass
+class Case:
+    name: str
+    cg: g.AxialCTGeom
+    og: orc.Geometry
+    vg: g.ReconImgGeom
+    ov: orc.Volume
+
+
+def make_case(name: str, nv: int = 120, nc: int = 96, nr: int = 24, n: int = 48, nz: int = 8,
+              rot_dir: g.RotDir = g.RotDir.CW, range_rad: float = 2 * math.pi, init_ang: float = 0.0,
+              vox: float = 1.0, mid=(0.0, 0.0, 0.0)) -> Case:
+    incr = range_rad / nv
+    c0, r0 = (nc - 1) / 2.0, (nr - 1) / 2.0
+    rot = g.RotationParams(rot_dir, init_ang, incr, nv)
+    if name == "parallel_1d":
+        det = (g.DetParallel(nc, 0.9),)
+        params = g.Parallel1DProjGeomParams(c0, rot)
+    elif name == "fan_arc":
+        det = (g.DetFanArc(nc, 0.11 / nc * 2.0),)
+        params = g.FanBeamProjGeomParams(c0, rot, 1000.0, 500.0)
+    elif name == "fan_line":
+        det = (g.DetFanLine(nc, 2.0),)
+        params = g.FanBeamProjGeomParams(c0, rot, 1536.0, 1000.0)
+    elif name == "parallel_2d":
+        det = (g.DetParallel(nc, 0.9), g.DetParallel(nr, 1.14))
+        params = g.Parallel2DProjGeomParams(c0, rot, r0)
+    elif name == "cone_parallel":
+        det = (g.DetParallel(nc, 0.9), g.DetFanLine(nr, 1.14))
+        params = g.ConeBeamProjGeomParams(c0, rot, 1536.0, 1000.0, r0)
+    elif name == "cone_cyl":
+        det = (g.DetFanArc(nc, 0.11 / nc * 2.0), g.DetFanLine(nr, 1.14))
+        params = g.ConeBeamProjGeomParams(c0, rot, 1000.0, 500.0, r0)
+    elif name == "cone_flat":
+        det = (g.DetFanLine(nc, 2.0), g.DetFanLine(nr, 2.0))
+        params = g.ConeBeamProjGeomParams(c0, rot, 1000.0, 500.0, r0)
+    else:
+        raise KeyError(name)
+    cg = g.AxialCTGeom.from_params(det, params)
+    kind = int(cg.kind)
+    og = orc.Geometry(kind, nc, det[0].sampling_width, cg.views, nr if len(det) > 1 else 1,
+                      det[1].sampling_width if len(det) > 1 else 1.0)
+    if len(det) > 1:
+        vg = g.ReconImgGeom(g.EqDistSampler(n, vox), g.EqDistSampler(n, vox), g.EqDistSampler(nz, vox), mid)
+        ov = orc.Volume(n, n, nz, vox, vox, vox, tuple(mid))
+    else:
+        vg = g.ReconImgGeom(g.EqDistSampler(n, vox), g.EqDistSampler(n, vox), None, mid[:2])
+        ov = orc.Volume(n, n, 1, vox, vox, 1.0, (mid[0], mid[1], 0.0))
+    return Case(name, cg, og, vg, ov)
+
+
+def oracle_projections(case: Case) -> np.ndarray:
+    return orc.phantom(case.og, np.array(PHANTOM)).astype(np.float32)
