@@ -42,6 +42,10 @@ CONFIGS = {
                     n=(512, 512, 512), vox=0.5, range=2 * math.pi, n_ell=16, i0=1e5,
                     label="flat-panel cone-beam full scan, 512^3 at 0.5 mm, 720 views, 1024x768 at 0.4 mm, "
                           "SOD 750, SDD 1200"),
+    "cone256": dict(kind="cone_flat", nv=360, nc=512, nr=384, du=0.8, dv=0.8, sod=750.0, sdd=1200.0,
+                    n=(256, 256, 256), vox=1.0, range=2 * math.pi, n_ell=16, i0=1e5,
+                    label="flat-panel cone-beam full scan, 256^3 at 1 mm, 360 views, 512x384 at 0.8 mm, "
+                          "SOD 750, SDD 1200 (profiling-size case)"),
     "short384": dict(kind="cone_flat", nv=496, nc=1240, nr=960, du=0.3, dv=0.3, sod=785.0, sdd=1200.0,
                      n=(512, 512, 384), vox=0.5, range=None, n_ell=16, i0=None,
                      label="flat-panel cone-beam short scan (pi + fan), 512x512x384, 496 views, 1240x960 at 0.3 mm, "

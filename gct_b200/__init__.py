@@ -8,7 +8,7 @@ from .geometry import (ApodFunc, AxialCTGeom, ConeBeamProjGeomParams, CTGeom, De
                        DetParallel, EqDistSampler, FanBeamProjGeomParams, GeomKind, Parallel1DProjGeomParams,
                        Parallel2DProjGeomParams, ProjectionStack, ProjGeom, ProjGeomFactory, ReconImg,
                        ReconImgGeom, RotationGeom, RotationParams, RotDir, is_valid_axial_recon, kind_of,
-                       parker_weights, ramp_filter_taps, VIEW_DTYPE)
+                       map_point, parker_weights, ramp_filter_taps, VIEW_DTYPE)
 from .recon import (FILTER_FFT, FILTER_TOEPLITZ_BF16X3, STORAGE_F16, STORAGE_F32, FdkOptions, FdkPlan,
                     FiltParams, forward_project, phantom_project, reconstruct)
 

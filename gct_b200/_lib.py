@@ -88,6 +88,8 @@ SIGNATURES = {
                                  P(C.c_int32)],
     "gct_ramp_filter_taps": [C.c_int32, P(gct_detector), P(gct_filt_params), P(C.c_double)],
     "gct_parker_weights": [P(gct_ct_geom), P(C.c_float)],
+    "gct_map_point": [P(gct_ct_geom), P(gct_vol_geom), C.c_uint32, P(C.c_double), P(C.c_double),
+                      P(C.c_double), P(C.c_double), P(C.c_double)],
     "gct_fdk_plan_create": [P(gct_ct_geom), P(gct_vol_geom), P(gct_filt_params), P(gct_fdk_opts), P(VP)],
     "gct_fdk_plan_destroy": [VP],
     "gct_fdk_plan_workspace_bytes": [VP, P(C.c_uint64)],

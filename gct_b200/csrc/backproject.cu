@@ -4,10 +4,17 @@
 // every view is copied into a cudaArray and one launch per view reads it through a bilinear
 // texture and does vol += val * w (src/cuda/recon/back_proj.cuh:16-104), a full volume
 // read-modify-write per view. Here one launch covers a range of views: each thread owns one
-// (x, y) column and zpt voxels along z, keeps their sums in registers across all views and
-// writes the volume once. Per view, the column's detector column u, its bilinear split and the
-// backprojection weight are computed once (they do not depend on z for circular trajectories),
-// and each voxel costs one row coordinate, one 8- or 16-byte quad load and three lerps.
+// (x, y) column and ZPT voxels along z, keeps their sums in registers across all views and
+// writes the volume once.
+//
+// Column kernel (circular trajectories, "z-affine" geometry): per view, the column's detector
+// column u, its bilinear split, the weight (projective and parallel kinds) and the row coordinate
+// v(z) = v0 + z * vs are set up once. Each voxel then costs one FMA for v, a magic-number floor
+// split, one IMAD.WIDE address, one 8- or 16-byte load of a bilinear-coefficient quad, two FMAs
+// (one HFMA2 plus one FMA for FP16 storage) and the accumulate. A column segment whose rows all fall outside
+// the detector contributes exactly zero (the reference's texture border) and is skipped; one that
+// lies fully on the detector runs without per-voxel clamps.
+//
 // Mappings follow projMapping (src/cuda/geom/coord_trans_proj.cuh:157-345) through per-view
 // coefficients in voxel-index space that the host derives in FP64.
 #include "../../include/gct_fdk.h"
@@ -20,6 +27,8 @@ namespace {
 
 constexpr int kViewsPerChunk = 128;
 constexpr int kC = kCoefPerView;
+constexpr float kShift = 12582912.0f;  // 1.5 * 2^23
+constexpr int kShiftBits = 0x4B400000;  // bit pattern of kShift
 
 // Coefficient layouts (per view, kCoefPerView floats):
 //  affine     : [0..2] u0, ui, uj; [3..4] v0, vk; [5] wscale
@@ -32,32 +41,119 @@ constexpr int kC = kCoefPerView;
 // Each affine form is c0 + ci*i + cj*j + ck*k in voxel indices.
 __device__ __forceinline__ int wscale_slot(int family) { return family == 0 ? 5 : family == 1 ? 12 : 16; }
 
-template <class Q>
-__device__ __forceinline__ float bilerp(const typename Q::storage *col, int qpitch, float fu,
-                                        float v, float vmax)
+// Bilinear value of a stored coefficient quad (A, B, C, D) at column fraction fu in [0, 1] and
+// centred row fraction fvc in [-0.5, 0.5]: (A + fu B) + fvc (C + fu D). The per-column form of fu
+// (U) is precomputed once per view.
+struct LerpF32 {
+    using S = float4;
+    using U = float;
+    static __device__ __forceinline__ U ucol(float fu) { return fu; }
+    static __device__ __forceinline__ float lerp(float4 q, U fu, float fvc)
+    {
+        return fmaf(fvc, fmaf(fu, q.w, q.z), fmaf(fu, q.y, q.x));
+    }
+};
+struct LerpF16 {
+    using S = uint2;  // .x = (A, C), .y = (B, D) as half2
+    using U = __half2;
+    static __device__ __forceinline__ U ucol(float fu) { return __float2half2_rn(fu); }
+    static __device__ __forceinline__ float lerp(uint2 q, U fu2, float fvc)
+    {
+        const __half2 ac = *reinterpret_cast<__half2 *>(&q.x);
+        const __half2 bd = *reinterpret_cast<__half2 *>(&q.y);
+        const float2 e = __half22float2(__hfma2(fu2, bd, ac));  // (A + fu B, C + fu D)
+        return fmaf(fvc, e.y, e.x);
+    }
+};
+template <class Q> struct LerpOf;
+template <> struct LerpOf<QuadF32> { using type = LerpF32; };
+template <> struct LerpOf<QuadF16> { using type = LerpF16; };
+
+struct ConstWeight {
+    float w;
+    __device__ __forceinline__ float at(int) const { return w; }
+};
+struct ArcWeight {  // wscale / (rho^2 + T(z)^2), T(z) = T0 + z tk
+    float ws, rho2, T0, tk;
+    __device__ __forceinline__ float at(int z) const
+    {
+        const float T = fmaf(tk, static_cast<float>(z), T0);
+        return ws * rcp_approx(fmaf(T, T, rho2));
+    }
+};
+
+// Accumulates one view into the ZPT voxels of a column. The row coordinate enters as
+// vm(z) = v(z) - 0.5 = vm0 + z vs; the 1.5 * 2^23 shifter rounds it to the quad row iv (the
+// floor of v, or v - 1 at integers) and leaves the centred fraction vm - iv in [-0.5, 0.5].
+// `base` is arranged so that base + bits(t) * stride addresses quad row iv + kQuadPad, where
+// bits(t) is the float bit pattern of the shifted coordinate.
+template <class L, int ZPT, bool CLAMP, class W>
+__device__ __forceinline__ void column(unsigned long long base, int stride, typename L::U fu, float vm0, float vs,
+                                       float vmax, const W &wt, float (&acc)[ZPT])
 {
-    v = fminf(fmaxf(v, -1.0f), vmax);
-    int iv;
-    float fv;
-    split_coord(v, iv, fv);
-    const float4 q = Q::unpack(Q::load(col + (iv + kQuadPad) * qpitch));
-    const float top = fmaf(fu, q.y - q.x, q.x);
-    const float bot = fmaf(fu, q.w - q.z, q.z);
-    return fmaf(fv, bot - top, top);
+#pragma unroll
+    for (int z = 0; z < ZPT; ++z) {
+        float vm = fmaf(vs, static_cast<float>(z), vm0);
+        if (CLAMP) vm = fminf(fmaxf(vm, -1.5f), vmax - 0.5f);
+        const float t = vm + kShift;
+        const float fvc = vm - (t - kShift);
+        const auto *p = reinterpret_cast<const typename L::S *>(
+            base + static_cast<unsigned long long>(static_cast<long long>(__float_as_int(t)) * stride));
+        acc[z] = fmaf(wt.at(z), L::lerp(__ldg(p), fu, fvc), acc[z]);
+    }
+}
+
+template <class L, int ZPT, class W>
+__device__ __forceinline__ void column_dispatch(const typename L::S *view, int qpitch, float u, float v0, float vs,
+                                                float umax, float vmax, const W &wt, float (&acc)[ZPT])
+{
+    if (!(u >= -1.0f && u <= umax)) return;  // the column's rays miss the detector: zero
+    int iu;
+    float fu;
+    split_coord(u, iu, fu);
+    const float va = v0, vb = fmaf(vs, static_cast<float>(ZPT - 1), v0);
+    const float lo = fminf(va, vb), hi = fmaxf(va, vb);
+    if (hi < -1.0f || lo > vmax) return;  // every voxel of the segment projects off the detector
+    const int stride = qpitch * static_cast<int>(sizeof(typename L::S));
+    const unsigned long long base =
+        reinterpret_cast<unsigned long long>(view + iu + kQuadPad) -
+        static_cast<unsigned long long>(static_cast<long long>(kShiftBits - kQuadPad) * stride);
+    const typename L::U fuc = L::ucol(fu);
+    if (lo >= -1.0f && hi <= vmax)
+        column<L, ZPT, false>(base, stride, fuc, v0 - 0.5f, vs, vmax, wt, acc);
+    else
+        column<L, ZPT, true>(base, stride, fuc, v0 - 0.5f, vs, vmax, wt, acc);
+}
+
+// Clamped bilinear sample at (u, v) for the per-voxel (non-z-affine) kernels.
+template <class L>
+__device__ __forceinline__ float sample(const typename L::S *view, int qpitch, float u, float v, float umax,
+                                        float vmax)
+{
+    u = fminf(fmaxf(u, -1.0f), umax);
+    const float vm = fminf(fmaxf(v, -1.0f), vmax) - 0.5f;
+    int iu;
+    float fu;
+    split_coord(u, iu, fu);
+    const float t = vm + kShift;
+    const int iv = __float_as_int(t) - kShiftBits;
+    const float fvc = vm - (t - kShift);
+    return L::lerp(__ldg(view + (iv + kQuadPad) * qpitch + iu + kQuadPad), L::ucol(fu), fvc);
 }
 
 template <int FAMILY, class Q, int ZPT, bool ZAFFINE>
 __global__ void __launch_bounds__(256) bp_kernel(BpArgs a)
 {
+    using L = typename LerpOf<Q>::type;
+    using S = typename L::S;
     __shared__ float4 s_coef[kViewsPerChunk * kC / 4];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k0 = blockIdx.z * ZPT;
     const bool active = i < a.nx && j < a.ny;
-    const float fi = static_cast<float>(i), fj = static_cast<float>(j);
+    const float fi = static_cast<float>(i), fj = static_cast<float>(j), fk0 = static_cast<float>(k0);
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     const int nthr = blockDim.x * blockDim.y;
-    using S = typename Q::storage;
     const S *quads = static_cast<const S *>(a.quads);
 
     float acc[ZPT];
@@ -80,51 +176,27 @@ __global__ void __launch_bounds__(256) bp_kernel(BpArgs a)
             const float *c = reinterpret_cast<const float *>(s_coef) + vv * kC;
             const S *view = quads + static_cast<long long>(a.v_begin + vc + vv) * a.qview;
             if (FAMILY == 0) {
-                // parallel kinds: u = u0 + ui i + uj j, v = v0 + vk k, weight constant
-                float u = fmaf(c[2], fj, fmaf(c[1], fi, c[0]));
-                u = fminf(fmaxf(u, -1.0f), a.umax);
-                int iu;
-                float fu;
-                split_coord(u, iu, fu);
-                const S *col = view + iu + kQuadPad;
-                const float w = c[5];
-#pragma unroll
-                for (int z = 0; z < ZPT; ++z) {
-                    const float v = fmaf(c[4], static_cast<float>(k0 + z), c[3]);
-                    acc[z] = fmaf(w, bilerp<Q>(col, a.qpitch, fu, v, a.vmax), acc[z]);
-                }
+                // parallel kinds: u = u0 + ui i + uj j, v = v0 + vk k, constant weight
+                const float u = fmaf(c[2], fj, fmaf(c[1], fi, c[0]));
+                column_dispatch<L, ZPT>(view, a.qpitch, u, fmaf(c[4], fk0, c[3]), c[4], a.umax, a.vmax,
+                                        ConstWeight{c[5]}, acc);
             } else if (FAMILY == 1) {
                 if (ZAFFINE) {
                     const float D = fmaf(c[10], fj, fmaf(c[9], fi, c[8]));
                     const float inv = rcp_approx(D);
-                    float u = fmaf(c[2], fj, fmaf(c[1], fi, c[0])) * inv;
-                    u = fminf(fmaxf(u, -1.0f), a.umax);
-                    int iu;
-                    float fu;
-                    split_coord(u, iu, fu);
-                    const S *col = view + iu + kQuadPad;
-                    const float w = c[12] * inv * inv;
-                    const float vs = c[7] * inv;
-                    const float v0 = fmaf(c[7], static_cast<float>(k0), fmaf(c[6], fj, fmaf(c[5], fi, c[4]))) * inv;
-#pragma unroll
-                    for (int z = 0; z < ZPT; ++z) {
-                        const float v = fmaf(vs, static_cast<float>(z), v0);
-                        acc[z] = fmaf(w, bilerp<Q>(col, a.qpitch, fu, v, a.vmax), acc[z]);
-                    }
+                    const float u = fmaf(c[2], fj, fmaf(c[1], fi, c[0])) * inv;
+                    const float v0 = fmaf(c[7], fk0, fmaf(c[6], fj, fmaf(c[5], fi, c[4]))) * inv;
+                    column_dispatch<L, ZPT>(view, a.qpitch, u, v0, c[7] * inv, a.umax, a.vmax,
+                                            ConstWeight{c[12] * inv * inv}, acc);
                 } else {
 #pragma unroll
                     for (int z = 0; z < ZPT; ++z) {
-                        const float fk = static_cast<float>(k0 + z);
+                        const float fk = fk0 + static_cast<float>(z);
                         const float D = fmaf(c[11], fk, fmaf(c[10], fj, fmaf(c[9], fi, c[8])));
                         const float inv = rcp_approx(D);
-                        float u = fmaf(c[3], fk, fmaf(c[2], fj, fmaf(c[1], fi, c[0]))) * inv;
+                        const float u = fmaf(c[3], fk, fmaf(c[2], fj, fmaf(c[1], fi, c[0]))) * inv;
                         const float v = fmaf(c[7], fk, fmaf(c[6], fj, fmaf(c[5], fi, c[4]))) * inv;
-                        u = fminf(fmaxf(u, -1.0f), a.umax);
-                        int iu;
-                        float fu;
-                        split_coord(u, iu, fu);
-                        acc[z] = fmaf(c[12] * inv * inv,
-                                      bilerp<Q>(view + iu + kQuadPad, a.qpitch, fu, v, a.vmax), acc[z]);
+                        acc[z] = fmaf(c[12] * inv * inv, sample<L>(view, a.qpitch, u, v, a.umax, a.vmax), acc[z]);
                     }
                 }
             } else {
@@ -132,37 +204,23 @@ __global__ void __launch_bounds__(256) bp_kernel(BpArgs a)
                     const float A = fmaf(c[2], fj, fmaf(c[1], fi, c[0]));
                     const float B = fmaf(c[6], fj, fmaf(c[5], fi, c[4]));
                     const float rho2 = fmaf(A, A, B * B);
-                    float u = fmaf(atan2f(A, B), c[12], c[13]);
-                    u = fminf(fmaxf(u, -1.0f), a.umax);
-                    int iu;
-                    float fu;
-                    split_coord(u, iu, fu);
-                    const S *col = view + iu + kQuadPad;
-                    const float vs = c[14] * rsqrtf(rho2);
-                    const float T0 = fmaf(c[11], static_cast<float>(k0), c[8]);
-#pragma unroll
-                    for (int z = 0; z < ZPT; ++z) {
-                        const float T = fmaf(c[11], static_cast<float>(z), T0);
-                        const float v = fmaf(vs, T, c[15]);
-                        const float w = c[16] * rcp_approx(fmaf(T, T, rho2));
-                        acc[z] = fmaf(w, bilerp<Q>(col, a.qpitch, fu, v, a.vmax), acc[z]);
-                    }
+                    const float u = fmaf(atan2f(A, B), c[12], c[13]);
+                    const float vsr = c[14] * rsqrtf(rho2);
+                    const float T0 = fmaf(c[11], fk0, c[8]);
+                    column_dispatch<L, ZPT>(view, a.qpitch, u, fmaf(vsr, T0, c[15]), vsr * c[11], a.umax, a.vmax,
+                                            ArcWeight{c[16], rho2, T0, c[11]}, acc);
                 } else {
 #pragma unroll
                     for (int z = 0; z < ZPT; ++z) {
-                        const float fk = static_cast<float>(k0 + z);
+                        const float fk = fk0 + static_cast<float>(z);
                         const float A = fmaf(c[3], fk, fmaf(c[2], fj, fmaf(c[1], fi, c[0])));
                         const float B = fmaf(c[7], fk, fmaf(c[6], fj, fmaf(c[5], fi, c[4])));
                         const float T = fmaf(c[11], fk, fmaf(c[10], fj, fmaf(c[9], fi, c[8])));
                         const float rho2 = fmaf(A, A, B * B);
-                        float u = fmaf(atan2f(A, B), c[12], c[13]);
-                        u = fminf(fmaxf(u, -1.0f), a.umax);
-                        int iu;
-                        float fu;
-                        split_coord(u, iu, fu);
+                        const float u = fmaf(atan2f(A, B), c[12], c[13]);
                         const float v = fmaf(c[14] * rsqrtf(rho2), T, c[15]);
                         const float w = c[16] * rcp_approx(fmaf(T, T, rho2));
-                        acc[z] = fmaf(w, bilerp<Q>(view + iu + kQuadPad, a.qpitch, fu, v, a.vmax), acc[z]);
+                        acc[z] = fmaf(w, sample<L>(view, a.qpitch, u, v, a.umax, a.vmax), acc[z]);
                     }
                 }
             }

@@ -1,14 +1,20 @@
-// Row-batched ramp filter: cosine and Parker weights fused into the load, zero padding in
-// shared memory, a Stockham radix-4/2 FFT convolution with the ramp spectrum, and an epilogue
-// that writes either plain FP32 rows or the padded bilinear-quad layout used by the
-// backprojector. Two detector rows share one complex FFT (row a in the real part, row b in
-// the imaginary part): the ramp taps are real, so the two convolutions stay separated.
+// Row-batched ramp filter: cosine and Parker weights fused into the load, a Stockham radix-4/2
+// FFT convolution with the ramp spectrum in shared memory, and an epilogue that writes either
+// plain FP32 rows or the padded bilinear-coefficient quads read by the backprojector. Two
+// detector rows share one complex FFT (row a in the real part, row b in the imaginary part): the
+// ramp taps are real, so the two convolutions stay separated.
 //
 // Replaces runCosWeighting (src/cuda/recon/cos_weighting.cuh:225-263), runParkerWeighting
 // (src/cuda/recon/parker_weighting.cuh:202-230) and RampFilteringFFT::runFiltering
 // (src/cuda/recon/ramp_filtering_fft.cuh:208-219): the reference pads to nextPow2(2N), runs
-// cuFFT R2C/C2R and crops at N/2; here the taps are placed circularly so the crop disappears and
-// the shortest alias-free power of two (> 1.5 N) is used.
+// cuFFT R2C/C2R and crops at N/2 in five passes over HBM; here the taps are placed circularly so
+// the crop disappears, the shortest alias-free power of two (> 1.5 N) is used, and each row is
+// read once and written once.
+//
+// Work split: one CTA per (view, segment of rows). A CTA walks its rows in order, keeps the
+// previous filtered row in shared memory and writes the quad of row r once rows r and r + 1 are
+// known, so every quad is written whole by one CTA. Each segment filters one extra row (the first
+// row of the next segment) to close its last quad.
 #include "../../include/gct_fdk.h"
 #include "common.cuh"
 #include "kernels.hpp"
@@ -52,59 +58,84 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 
-// One Stockham stage of radix R (4 or 2) with span Ns (Govindaraju et al., SC'08): butterfly j
-// reads src[j + r L/R], applies the twiddle W_L^(r (j mod Ns) L/(Ns R)), and writes the R-point
-// DFT to dst[(j / Ns) Ns R + (j mod Ns) + r Ns]. The output after all stages is in natural order.
-template <int L, int NT>
-__device__ __forceinline__ void stage_r4(const float2 *__restrict__ src, float2 *__restrict__ dst,
-                                         const float2 *__restrict__ tw, int Ns, int tid)
+// Shared-memory index with one float2 of padding per 16: strided Stockham writes then spread
+// over all banks.
+__device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
+
+// One Stockham stage (Govindaraju et al., SC'08). Butterfly j reads x[j + r L/R], multiplies by
+// the twiddle W_{R Ns}^(r (j mod Ns)) and writes its R-point DFT to
+// y[(j / Ns) Ns R + (j mod Ns) + r Ns]; after all stages the output is in natural order.
+// Twiddles of a stage with span Ns live contiguously at tw[Ns + k], k < Ns.
+// LAST fuses the pointwise product with the spectrum H and the conjugation that turns the next
+// forward FFT into the inverse.
+template <int L, int NT, bool LAST>
+__device__ __forceinline__ void stage_r4(const float2 *src, float2 *dst, const float2 *tw, const float2 *H,
+                                         int Ns, int tid)
 {
-#pragma unroll
     for (int j = tid; j < L / 4; j += NT) {
         const int k = j & (Ns - 1);
-        float2 v0 = src[j], v1 = src[j + L / 4], v2 = src[j + L / 2], v3 = src[j + 3 * L / 4];
+        float2 v0 = src[pad(j)], v1 = src[pad(j + L / 4)], v2 = src[pad(j + L / 2)], v3 = src[pad(j + 3 * L / 4)];
         if (Ns > 1) {
-            const int step = k * (L / (4 * Ns));
-            v1 = cmul(v1, tw[step]);
-            v2 = cmul(v2, tw[2 * step]);
-            v3 = cmul(v3, tw[3 * step]);
+            const float2 w1 = tw[Ns + k];
+            const float2 w2 = cmul(w1, w1);
+            v1 = cmul(v1, w1);
+            v2 = cmul(v2, w2);
+            v3 = cmul(v3, cmul(w2, w1));
         }
         const float2 t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3);
         const float2 d = csub(v1, v3);
         const float2 t3 = make_float2(d.y, -d.x);  // -i * (v1 - v3)
         const int idx = (j - k) * 4 + k;
-        dst[idx] = cadd(t0, t2);
-        dst[idx + Ns] = cadd(t1, t3);
-        dst[idx + 2 * Ns] = csub(t0, t2);
-        dst[idx + 3 * Ns] = csub(t1, t3);
+        float2 y[4] = {cadd(t0, t2), cadd(t1, t3), csub(t0, t2), csub(t1, t3)};
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            float2 o = y[r];
+            if (LAST) {
+                o = cmul(o, __ldg(H + idx + r * Ns));
+                o.y = -o.y;
+            }
+            dst[pad(idx + r * Ns)] = o;
+        }
     }
 }
 
-template <int L, int NT>
-__device__ __forceinline__ void stage_r2(const float2 *__restrict__ src, float2 *__restrict__ dst,
-                                         const float2 *__restrict__ tw, int Ns, int tid)
+template <int L, int NT, bool LAST>
+__device__ __forceinline__ void stage_r2(const float2 *src, float2 *dst, const float2 *tw, const float2 *H,
+                                         int Ns, int tid)
 {
-#pragma unroll
     for (int j = tid; j < L / 2; j += NT) {
         const int k = j & (Ns - 1);
-        float2 v0 = src[j], v1 = src[j + L / 2];
-        if (Ns > 1) v1 = cmul(v1, tw[k * (L / (2 * Ns))]);
+        float2 v0 = src[pad(j)], v1 = src[pad(j + L / 2)];
+        if (Ns > 1) v1 = cmul(v1, tw[Ns + k]);
         const int idx = (j - k) * 2 + k;
-        dst[idx] = cadd(v0, v1);
-        dst[idx + Ns] = csub(v0, v1);
+        float2 y0 = cadd(v0, v1), y1 = csub(v0, v1);
+        if (LAST) {
+            y0 = cmul(y0, __ldg(H + idx));
+            y0.y = -y0.y;
+            y1 = cmul(y1, __ldg(H + idx + Ns));
+            y1.y = -y1.y;
+        }
+        dst[pad(idx)] = y0;
+        dst[pad(idx + Ns)] = y1;
     }
 }
 
-// Forward FFT of L points from `a`; ping-pongs between a and b, returns the result buffer.
-template <int LOG2L, int NT>
-__device__ __forceinline__ float2 *fft(float2 *a, float2 *b, const float2 *tw, int tid)
+// Remaining stages of an L-point FFT whose first radix-4 stage (Ns = 1) is already in `a`.
+// Ping-pongs between a and b; returns the buffer holding the result.
+template <int LOG2L, int NT, bool FUSE_H>
+__device__ __forceinline__ float2 *fft_rest(float2 *a, float2 *b, const float2 *tw, const float2 *H, int tid)
 {
     constexpr int L = 1 << LOG2L;
+    constexpr int NR4 = LOG2L / 2;
     float2 *src = a, *dst = b;
-    int Ns = 1;
+    int Ns = 4;
 #pragma unroll
-    for (int s = 0; s < LOG2L / 2; ++s) {
-        stage_r4<L, NT>(src, dst, tw, Ns, tid);
+    for (int s = 1; s < NR4; ++s) {
+        const bool last = (s == NR4 - 1) && !(LOG2L & 1);
+        if (FUSE_H && last)
+            stage_r4<L, NT, true>(src, dst, tw, H, Ns, tid);
+        else
+            stage_r4<L, NT, false>(src, dst, tw, H, Ns, tid);
         __syncthreads();
         float2 *t = src;
         src = dst;
@@ -112,7 +143,10 @@ __device__ __forceinline__ float2 *fft(float2 *a, float2 *b, const float2 *tw, i
         Ns *= 4;
     }
     if (LOG2L & 1) {
-        stage_r2<L, NT>(src, dst, tw, Ns, tid);
+        if (FUSE_H)
+            stage_r2<L, NT, true>(src, dst, tw, H, Ns, tid);
+        else
+            stage_r2<L, NT, false>(src, dst, tw, H, Ns, tid);
         __syncthreads();
         float2 *t = src;
         src = dst;
@@ -121,118 +155,153 @@ __device__ __forceinline__ float2 *fft(float2 *a, float2 *b, const float2 *tw, i
     return src;
 }
 
+// First radix-4 stage of the inverse transform (input already conjugated in smem).
+template <int L, int NT>
+__device__ __forceinline__ void first_stage_smem(const float2 *src, float2 *dst, int tid)
+{
+    stage_r4<L, NT, false>(src, dst, nullptr, nullptr, 1, tid);
+}
+
+// Bilinear-coefficient quad of rows (top, bot) at column c: with fu in [0, 1] and the centred row
+// fraction fv' in [-0.5, 0.5], the bilinear value is (A + fu B) + fv' (C + fu D).
+struct QuadCoef {
+    float A, B, C, D;
+};
+__device__ __forceinline__ QuadCoef quad_coef(float p00, float p01, float p10, float p11)
+{
+    const float l = p00 + p10, r = p01 + p11;
+    return {0.5f * l, 0.5f * (r - l), p10 - p00, (p11 - p01) - (p10 - p00)};
+}
+
 template <int MODE>
-__device__ __forceinline__ void store_row(const FilterArgs &a, long long row, const float2 *res,
-                                          bool imag, int tid, int nthreads)
+__device__ __forceinline__ void store_quad(void *out, long long qidx, QuadCoef q)
+{
+    if (MODE == kOutQuadF32) {
+        static_cast<float4 *>(out)[qidx] = make_float4(q.A, q.B, q.C, q.D);
+    } else {
+        const __half2 lo = __floats2half2_rn(q.A, q.C), hi = __floats2half2_rn(q.B, q.D);
+        uint2 u;
+        u.x = *reinterpret_cast<const unsigned *>(&lo);
+        u.y = *reinterpret_cast<const unsigned *>(&hi);
+        static_cast<uint2 *>(out)[qidx] = u;
+    }
+}
+
+// Writes quad row `r` (detector row r, padded index r + kQuadPad) of view v from the filtered
+// rows `top` (row r) and `bot` (row r + 1); either may be NULL for a zero row. Values are scaled
+// by `sc`. Rows read from the FFT buffer use its padded indexing and sign.
+template <int MODE>
+__device__ __forceinline__ void write_quad_row(const FilterArgs &a, int v, int r, const float *top,
+                                               const float2 *bot, bool bot_imag, float sc, int tid, int nthr)
 {
     const int nc = a.nc;
-    if (MODE == kOutPlainF32) {
-        float *out = static_cast<float *>(a.out) + row * nc;
-        for (int c = tid; c < nc; c += nthreads) out[c] = imag ? -res[c].y : res[c].x;
-        return;
-    }
-    const int v = static_cast<int>(row / a.nr);
-    const int r = static_cast<int>(row - static_cast<long long>(v) * a.nr);
-    const float sc = a.vscale ? a.vscale[v] : 1.0f;
     const int qpitch = nc + 2 * kQuadPad;
-    const long long qview = static_cast<long long>(a.nr + 2 * kQuadPad) * qpitch;
-    auto val = [&](int c) -> float {
-        if (c < 0 || c >= nc) return 0.0f;
-        return sc * (imag ? -res[c].y : res[c].x);
+    const long long row0 = (static_cast<long long>(v) * (a.nr + 2 * kQuadPad) + (r + kQuadPad)) * qpitch;
+    auto tv = [&](int c) -> float { return (top && c >= 0 && c < nc) ? top[c] : 0.0f; };
+    auto bv = [&](int c) -> float {
+        if (!bot || c < 0 || c >= nc) return 0.0f;
+        const float2 z = bot[pad(c)];
+        return sc * (bot_imag ? -z.y : z.x);
     };
-    for (int cq = tid; cq < qpitch; cq += nthreads) {
+    for (int cq = tid; cq < qpitch; cq += nthr) {
         const int c = cq - kQuadPad;
-        const float lo = val(c), hi = val(c + 1);
-        const long long own = static_cast<long long>(v) * qview + static_cast<long long>(r + kQuadPad) * qpitch + cq;
-        const long long prv = own - qpitch;
-        if (MODE == kOutQuadF32) {
-            float2 *q = reinterpret_cast<float2 *>(static_cast<float4 *>(a.out));
-            const float2 pair = make_float2(lo, hi);
-            const float2 zero = make_float2(0.f, 0.f);
-            q[2 * own] = pair;          // own row: .xy
-            q[2 * prv + 1] = pair;      // previous row: .zw
-            if (r == 0) {
-                q[2 * (prv - qpitch)] = zero;
-                q[2 * (prv - qpitch) + 1] = zero;
-                q[2 * prv] = zero;
-            }
-            if (r == a.nr - 1) {
-                q[2 * own + 1] = zero;
-                q[2 * (own + qpitch)] = zero;
-                q[2 * (own + qpitch) + 1] = zero;
-                q[2 * (own + 2 * qpitch)] = zero;
-                q[2 * (own + 2 * qpitch) + 1] = zero;
-            }
-        } else {
-            __half2 *q = reinterpret_cast<__half2 *>(static_cast<uint2 *>(a.out));
-            const __half2 pair = __floats2half2_rn(lo, hi);
-            const __half2 zero = __floats2half2_rn(0.f, 0.f);
-            q[2 * own] = pair;
-            q[2 * prv + 1] = pair;
-            if (r == 0) {
-                q[2 * (prv - qpitch)] = zero;
-                q[2 * (prv - qpitch) + 1] = zero;
-                q[2 * prv] = zero;
-            }
-            if (r == a.nr - 1) {
-                q[2 * own + 1] = zero;
-                q[2 * (own + qpitch)] = zero;
-                q[2 * (own + qpitch) + 1] = zero;
-                q[2 * (own + 2 * qpitch)] = zero;
-                q[2 * (own + 2 * qpitch) + 1] = zero;
-            }
-        }
+        store_quad<MODE>(a.out, row0 + cq, quad_coef(tv(c), tv(c + 1), bv(c), bv(c + 1)));
     }
 }
 
 template <int LOG2L, int MODE>
-__global__ void __launch_bounds__(256) filter_fft_kernel(FilterArgs a)
+__global__ void __launch_bounds__(256) filter_fft_kernel(FilterArgs a, int seg_rows, int nseg)
 {
     constexpr int L = 1 << LOG2L;
     constexpr int NT = (L / 4 < 256) ? L / 4 : 256;
+    constexpr int LP = L + L / 16;
     extern __shared__ float2 smem[];
-    float2 *tw = smem, *b0 = smem + L, *b1 = smem + 2 * L;
+    float2 *tw = smem, *b0 = smem + L, *b1 = smem + L + LP;
+    float *yprev = reinterpret_cast<float *>(smem + L + 2 * LP);
     const int tid = threadIdx.x;
     for (int m = tid; m < L; m += NT) tw[m] = a.twiddle[m];
 
-    const long long nrows = static_cast<long long>(a.nv) * a.nr;
-    const long long npairs = (nrows + 1) / 2;
-    const int nc = a.nc;
-    for (long long p = blockIdx.x; p < npairs; p += gridDim.x) {
-        const long long ra = 2 * p, rb = 2 * p + 1;
-        const bool has_b = rb < nrows;
-        const int va = static_cast<int>(ra / a.nr), r_a = static_cast<int>(ra - static_cast<long long>(va) * a.nr);
-        const int vb = has_b ? static_cast<int>(rb / a.nr) : va;
-        const int r_b = has_b ? static_cast<int>(rb - static_cast<long long>(vb) * a.nr) : 0;
-        const float4 ga = __ldg(&a.fview[va]), gb = __ldg(&a.fview[vb]);
-        const float *pa = a.proj + ra * nc, *pb = a.proj + rb * nc;
-        const float *wa = a.parker + static_cast<long long>(va) * nc;
-        const float *wb = a.parker + static_cast<long long>(vb) * nc;
-        for (int k = tid; k < L; k += NT) {
-            float2 z = make_float2(0.f, 0.f);
-            if (k < nc) {
-                z.x = __ldg(pa + k) * __ldg(wa + k) *
-                      cos_weight(a.kind, ga.x, ga.y, ga.z, a.du, a.dv, k, r_a);
-                if (has_b)
-                    z.y = __ldg(pb + k) * __ldg(wb + k) *
-                          cos_weight(a.kind, gb.x, gb.y, gb.z, a.du, a.dv, k, r_b);
+    const int nc = a.nc, nr = a.nr;
+    for (long long blk = blockIdx.x; blk < static_cast<long long>(a.nv) * nseg; blk += gridDim.x) {
+        const int v = static_cast<int>(blk / nseg), s = static_cast<int>(blk - static_cast<long long>(v) * nseg);
+        const int r0 = s * seg_rows, r1 = min(r0 + seg_rows, nr);
+        const bool quads = MODE != kOutPlainF32;
+        const int last_row = (quads && r1 < nr) ? r1 : r1 - 1;  // quads: one extra row closes the segment
+        const float4 gv = __ldg(&a.fview[v]);
+        const float *wpk = a.parker + static_cast<long long>(v) * nc;
+        const float sc = (quads && a.vscale) ? a.vscale[v] : 1.0f;
+        int prev_row = r0 - 1;
+        bool have_prev = false;
+        if (quads && s == 0) {
+            write_quad_row<MODE>(a, v, -2, nullptr, nullptr, false, sc, tid, NT);
+            for (int c = tid; c < nc; c += NT) yprev[c] = 0.0f;  // row -1 is zero
+            have_prev = true;
+        }
+        __syncthreads();
+        for (int ra = r0; ra <= last_row; ra += 2) {
+            const bool has_b = ra + 1 <= last_row;
+            const float *pa = a.proj + (static_cast<long long>(v) * nr + ra) * nc;
+            const float *pb = pa + nc;
+            // load, weight and first radix-4 stage straight from global memory
+            for (int j = tid; j < L / 4; j += NT) {
+                float2 x[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int k = j + q * (L / 4);
+                    x[q] = make_float2(0.f, 0.f);
+                    if (k < nc) {
+                        const float w = __ldg(wpk + k);
+                        x[q].x = __ldg(pa + k) * w * cos_weight(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k, ra);
+                        if (has_b) x[q].y = __ldg(pb + k) * w * cos_weight(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k, ra + 1);
+                    }
+                }
+                const float2 t0 = cadd(x[0], x[2]), t1 = csub(x[0], x[2]), t2 = cadd(x[1], x[3]);
+                const float2 d = csub(x[1], x[3]);
+                const float2 t3 = make_float2(d.y, -d.x);
+                b0[pad(4 * j)] = cadd(t0, t2);
+                b0[pad(4 * j + 1)] = cadd(t1, t3);
+                b0[pad(4 * j + 2)] = csub(t0, t2);
+                b0[pad(4 * j + 3)] = csub(t1, t3);
             }
-            b0[k] = z;
+            __syncthreads();
+            float2 *spec = fft_rest<LOG2L, NT, true>(b0, b1, tw, a.H, tid);  // conj(FFT(x) H)
+            float2 *other = (spec == b0) ? b1 : b0;
+            first_stage_smem<L, NT>(spec, other, tid);
+            __syncthreads();
+            float2 *res = fft_rest<LOG2L, NT, false>(other, spec, tw, a.H, tid);  // conj of the filtered rows
+            // rows: ra in .x, ra + 1 in -.y
+            for (int h = 0; h < (has_b ? 2 : 1); ++h) {
+                const int rr = ra + h;
+                if (!quads) {
+                    if (rr < r1) {
+                        float *out = static_cast<float *>(a.out) + (static_cast<long long>(v) * nr + rr) * nc;
+                        for (int c = tid; c < nc; c += NT) out[c] = h ? -res[pad(c)].y : res[pad(c)].x;
+                    }
+                    continue;
+                }
+                if (have_prev) write_quad_row<MODE>(a, v, prev_row, yprev, res, h == 1, sc, tid, NT);
+                __syncthreads();
+                for (int c = tid; c < nc; c += NT) yprev[c] = sc * (h ? -res[pad(c)].y : res[pad(c)].x);
+                prev_row = rr;
+                have_prev = true;
+                __syncthreads();
+            }
+            __syncthreads();
         }
-        __syncthreads();
-        float2 *res = fft<LOG2L, NT>(b0, b1, tw, tid);
-        for (int k = tid; k < L; k += NT) {
-            const float2 y = cmul(res[k], __ldg(&a.H[k]));
-            res[k] = make_float2(y.x, -y.y);  // conj: the second forward FFT acts as the inverse
+        if (quads && r1 == nr) {  // last segment: rows nr-1 (bottom neighbour zero), nr and nr+1
+            write_quad_row<MODE>(a, v, nr - 1, yprev, nullptr, false, sc, tid, NT);
+            write_quad_row<MODE>(a, v, nr, nullptr, nullptr, false, sc, tid, NT);
+            write_quad_row<MODE>(a, v, nr + 1, nullptr, nullptr, false, sc, tid, NT);
         }
-        __syncthreads();
-        float2 *other = (res == b0) ? b1 : b0;
-        float2 *out = fft<LOG2L, NT>(res, other, tw, tid);
-        // out holds conj(IFFT): row a in .x, row b in -.y
-        store_row<MODE>(a, ra, out, false, tid, NT);
-        if (has_b) store_row<MODE>(a, rb, out, true, tid, NT);
         __syncthreads();
     }
+}
+
+template <int LOG2L>
+size_t smem_bytes_log2(int nc)
+{
+    constexpr int L = 1 << LOG2L;
+    return (static_cast<size_t>(L) + 2 * (L + L / 16)) * sizeof(float2) + static_cast<size_t>(nc) * sizeof(float);
 }
 
 template <int LOG2L>
@@ -240,28 +309,24 @@ void launch_log2(const FilterArgs &a, int num_sms, cudaStream_t s)
 {
     constexpr int L = 1 << LOG2L;
     constexpr int NT = (L / 4 < 256) ? L / 4 : 256;
-    const size_t smem = 3ull * L * sizeof(float2);
-    const long long npairs = (static_cast<long long>(a.nv) * a.nr + 1) / 2;
-    const int per_sm = static_cast<int>((227 * 1024) / (smem + 1024));
-    long long grid = static_cast<long long>(num_sms) * (per_sm > 0 ? per_sm : 1) * 4;
-    if (grid > npairs) grid = npairs;
-    if (grid < 1) grid = 1;
+    const size_t smem = smem_bytes_log2<LOG2L>(a.nc);
+    // segments of about 64 rows (one extra filtered row each); shorter segments when views are few
+    int seg_rows = 64;
+    while (seg_rows > 2 && static_cast<long long>(a.nv) * ((a.nr + seg_rows - 1) / seg_rows) < 4LL * num_sms)
+        seg_rows /= 2;
+    if (seg_rows > a.nr) seg_rows = a.nr;
+    const int nseg = (a.nr + seg_rows - 1) / seg_rows;
+    long long grid = static_cast<long long>(a.nv) * nseg;
+    const long long cap = static_cast<long long>(num_sms) * 64;
+    if (grid > cap) grid = cap;
+    auto go = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        kern<<<static_cast<unsigned>(grid), NT, smem, s>>>(a, seg_rows, nseg);
+    };
     switch (a.mode) {
-        case kOutPlainF32:
-            cudaFuncSetAttribute(filter_fft_kernel<LOG2L, kOutPlainF32>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-            filter_fft_kernel<LOG2L, kOutPlainF32><<<static_cast<unsigned>(grid), NT, smem, s>>>(a);
-            break;
-        case kOutQuadF32:
-            cudaFuncSetAttribute(filter_fft_kernel<LOG2L, kOutQuadF32>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-            filter_fft_kernel<LOG2L, kOutQuadF32><<<static_cast<unsigned>(grid), NT, smem, s>>>(a);
-            break;
-        default:
-            cudaFuncSetAttribute(filter_fft_kernel<LOG2L, kOutQuadF16>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-            filter_fft_kernel<LOG2L, kOutQuadF16><<<static_cast<unsigned>(grid), NT, smem, s>>>(a);
-            break;
+        case kOutPlainF32: go(filter_fft_kernel<LOG2L, kOutPlainF32>); break;
+        case kOutQuadF32: go(filter_fft_kernel<LOG2L, kOutQuadF32>); break;
+        default: go(filter_fft_kernel<LOG2L, kOutQuadF16>); break;
     }
 }
 
@@ -282,7 +347,9 @@ __global__ void view_scales_kernel(const float *amax, int nv, float l1, float *v
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= nv) return;
-    const float bound = amax[v] * l1;
+    // quad coefficients are sums and differences of up to four filtered values: keep 4 * bound
+    // below 2^14 so FP16 never overflows
+    const float bound = 4.0f * amax[v] * l1;
     float e = 0.f;
     if (bound > 0.f && isfinite(bound)) e = fminf(fmaxf(floorf(log2f(16384.f / bound)), -100.f), 100.f);
     vscale[v] = exp2f(e);
@@ -291,7 +358,19 @@ __global__ void view_scales_kernel(const float *amax, int nv, float l1, float *v
 
 }  // namespace
 
-size_t filter_fft_smem_bytes(int L) { return 3ull * L * sizeof(float2); }
+size_t filter_fft_smem_bytes(int L, int nc)
+{
+    switch (L) {
+        case 64: return smem_bytes_log2<6>(nc);
+        case 128: return smem_bytes_log2<7>(nc);
+        case 256: return smem_bytes_log2<8>(nc);
+        case 512: return smem_bytes_log2<9>(nc);
+        case 1024: return smem_bytes_log2<10>(nc);
+        case 2048: return smem_bytes_log2<11>(nc);
+        case 4096: return smem_bytes_log2<12>(nc);
+        default: return smem_bytes_log2<13>(nc);
+    }
+}
 
 void launch_filter_fft(const FilterArgs &a, int L, int num_sms, cudaStream_t s)
 {

@@ -41,10 +41,13 @@ Family family_of(gct_geom_kind kind)
 
 bool is_2d_detector(gct_geom_kind kind) { return kind >= GCT_GEOM_PARALLEL_2D; }
 
-// src/cpp/geom/utils.h:338-348 (wrapFrom0To2PI).
+// src/cpp/geom/utils.h:338-348 (wrapFrom0To2PI). The reference wraps FP32 angles against its FP32
+// 2*pi, so an angle within one FP32 step (4.8e-7 rad) of 2*pi wraps to 0 there; the same band
+// is snapped here so FP32-sourced angles (e.g. float(2*pi)) analyse identically in FP64.
 double wrap_0_2pi(double a)
 {
     while (a < 0.0) a += kTwoPi;
+    if (std::fabs(a - kTwoPi) <= 4.8e-7) return 0.0;
     return (a >= kTwoPi) ? std::remainder(a, kTwoPi) : a;
 }
 

@@ -19,7 +19,7 @@ struct FilterArgs {
     const float4 *fview = nullptr; // per view: (det_row_center, det_col_center, sdd, 0)
     const float *parker = nullptr; // [nv][nc]
     const float2 *H = nullptr;     // [L] filter spectrum, scaled by 1/L
-    const float2 *twiddle = nullptr; // [L] exp(-2 pi i m / L)
+    const float2 *twiddle = nullptr; // [L] per-stage twiddles: tw[Ns + k] = exp(-2 pi i k / (R Ns))
     int mode = kOutPlainF32;
     void *out = nullptr;           // plain: [nv][nr][nc] f32; quads: [nv][nr+4][nc+4]
     const float *vscale = nullptr; // per-view output scale for quads (nullable = 1)
@@ -28,7 +28,7 @@ struct FilterArgs {
 // Fused cosine + Parker weighting, zero padding, FFT convolution with the ramp filter and the
 // epilogue into the requested layout. L is the power-of-two FFT length.
 void launch_filter_fft(const FilterArgs &a, int L, int num_sms, cudaStream_t s);
-size_t filter_fft_smem_bytes(int L);
+size_t filter_fft_smem_bytes(int L, int nc);
 
 // Per-view |max| of the raw projections (amax must be zeroed) and the FP16 power-of-two scale
 // that maps the bound amax * l1 (l1 = sum |taps|) below 2^14; writes vscale and 1/vscale.

@@ -395,5 +395,19 @@ def parker_weights(cg: AxialCTGeom) -> np.ndarray:
     return w
 
 
+def map_point(cg: AxialCTGeom, vol_geom: ReconImgGeom, view: int, ijk) -> tuple:
+    """(xyz, col, row, weight) of fractional voxel index ``ijk`` in ``view``, evaluated on the host
+    from the same per-view coefficients the backprojection kernels use."""
+    dp = C.POINTER(C.c_double)
+    idx = np.zeros(3)
+    idx[:len(ijk)] = ijk
+    xyz = np.zeros(3)
+    col, row, w = C.c_double(), C.c_double(), C.c_double()
+    _lib.check(_lib.load().gct_map_point(C.byref(cg.struct()), C.byref(vol_geom.struct()), int(view),
+                                         idx.ctypes.data_as(dp), xyz.ctypes.data_as(dp), C.byref(col),
+                                         C.byref(row), C.byref(w)))
+    return xyz, col.value, row.value, w.value
+
+
 def deg(x: float) -> float:
     return x * math.pi / 180.0

@@ -201,6 +201,16 @@ gct_status gct_ramp_filter_taps(int32_t kind, const gct_detector *det_row,
  * (parker_weighting.cuh:163-175); here those weights are defined as 1. */
 gct_status gct_parker_weights(const gct_ct_geom *geom, float *weights);
 
+/* Evaluates, on the host in double precision, the per-view backprojection coefficients the
+ * kernels use (derived in FP64, stored as FP32) at fractional voxel index (i, j, k) of `vol`:
+ * world position xyz (mm; src/cuda/geom/coord_trans_img.cuh:52-66), detector pixel coordinates
+ * col/row (src/cuda/geom/coord_trans_proj.cuh:142-145 after projMapping :157-345) and the
+ * backprojection weight (without the angular-increment scale). For the 1D kinds row is 0 and k
+ * is ignored. Any pointer except geom/vol/ijk may be NULL. */
+gct_status gct_map_point(const gct_ct_geom *geom, const gct_vol_geom *vol, uint32_t view,
+                         const double ijk[3], double xyz[3], double *col, double *row,
+                         double *weight);
+
 /* ---- FDK plans (device) ---------------------------------------------------------------- */
 
 /* Builds a reusable reconstruction plan on the current CUDA device: FP64 per-view geometry,

@@ -98,9 +98,12 @@ int or_make_view(int kind, const double *p, unsigned idx, or_view *v)
     return 0;
 }
 
+/* utils.h:338-348; angles within one FP32 step below 2 pi wrap to 0, as the reference's FP32 wrap
+ * does for FP32 inputs (its 2 pi constant is float(2 pi)) */
 static double wrap2pi(double a)
 {
     while (a < 0.0) a += OR_TWO_PI;
+    if (fabs(a - OR_TWO_PI) <= 4.8e-7) return 0.0;
     return (a >= OR_TWO_PI) ? remainder(a, OR_TWO_PI) : a;
 }
 
