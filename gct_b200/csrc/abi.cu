@@ -7,7 +7,9 @@
 #include <complex>
 #include <cstdio>
 #include <cstring>
+#include <cstdint>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -608,6 +610,65 @@ gct_status gct_fdk_execute_host(gct_fdk_plan *plan, const float *proj_host, floa
         if (!plan) gct::fail(GCT_ERR_INVALID_ARG, "NULL plan");
         DeviceGuard dg(plan->device);
         execute_host(plan, proj_host, vol_host, static_cast<cudaStream_t>(stream));
+    });
+}
+
+}  // extern "C"
+
+// ---- execution without device allocation ---------------------------------------------------
+// Scratch of gct_fdk_execute_noalloc: filtered-projection quads of one chunk of views. The array
+// lives on every device that loads the library. Host code must not pass its name to a kernel
+// (on the host it is only a stand-in); the device address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[GCT_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxNoAllocDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[kMaxNoAllocDevices] = {};
+
+// Device address of the scratch on `dev` (the current device), looked up once per device.
+unsigned char *noalloc_scratch(int dev)
+{
+    if (dev < 0 || dev >= kMaxNoAllocDevices) gct::fail(GCT_ERR_NOT_SUPPORTED, "device index beyond 63");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        cuda_check(cudaGetSymbolAddress(&p, g_noalloc_scratch), "scratch address lookup");
+        g_noalloc_addr[dev] = p;
+    }
+    return static_cast<unsigned char *>(g_noalloc_addr[dev]);
+}
+
+void execute_noalloc(gct_fdk_plan *p, const float *proj, float *vol, cudaStream_t s)
+{
+    if (!proj || !vol) gct::fail(GCT_ERR_INVALID_ARG, "NULL projection or volume pointer");
+    const size_t per_view =
+        static_cast<size_t>(p->nr + 2 * gct::kQuadPad) * (p->nc + 2 * gct::kQuadPad) * p->quad_bytes();
+    if (per_view > GCT_NOALLOC_SCRATCH_BYTES)
+        gct::fail(GCT_ERR_BUDGET, "one view needs " + std::to_string(per_view) +
+                                      " bytes of filtered-projection scratch; the allocation-free path holds " +
+                                      std::to_string(GCT_NOALLOC_SCRATCH_BYTES) + " bytes");
+    const int chunk = static_cast<int>(std::min<size_t>(static_cast<size_t>(p->nv), GCT_NOALLOC_SCRATCH_BYTES / per_view));
+    unsigned char *scratch = noalloc_scratch(p->device);
+    for (int vb = 0; vb < p->nv; vb += chunk) {
+        const int vc = std::min(chunk, p->nv - vb);
+        // prepare() and run_backproject() place view v at workspace + v * per_view; shifting the
+        // base by vb views puts this chunk at the start of the scratch.
+        void *ws = reinterpret_cast<void *>(reinterpret_cast<uintptr_t>(scratch) - static_cast<uintptr_t>(vb) * per_view);
+        prepare(p, proj, ws, vb, vc, s);
+        run_backproject(p, ws, vol, vb, vc, vb > 0, s);
+    }
+}
+}  // namespace
+
+extern "C" {
+
+gct_status gct_fdk_execute_noalloc(gct_fdk_plan *plan, const float *proj_dev, float *vol_dev, void *stream)
+{
+    return guarded([&] {
+        if (!plan) gct::fail(GCT_ERR_INVALID_ARG, "NULL plan");
+        DeviceGuard dg(plan->device);
+        execute_noalloc(plan, proj_dev, vol_dev, static_cast<cudaStream_t>(stream));
     });
 }
 

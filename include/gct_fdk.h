@@ -262,6 +262,23 @@ gct_status gct_fdk_backproject(gct_fdk_plan *plan, const void *workspace, float 
 gct_status gct_fdk_execute_host(gct_fdk_plan *plan, const float *proj_host, float *vol_host,
                                 void *stream);
 
+/* Full FDK on device buffers without allocating device memory. No counterpart in the reference.
+ * For callers that cannot allocate device memory when they reconstruct: a host application whose
+ * own memory manager has already reserved the device's memory, or an acquisition loop that
+ * forbids allocation once it is running. Such a caller creates the plan at start-up and then
+ * calls this instead of gct_fdk_execute (which allocates its workspace on first use).
+ * The filtered projections go through a fixed scratch array of GCT_NOALLOC_SCRATCH_BYTES
+ * (64 MiB) that the library holds on every device that loads it, until the process exits; the
+ * views are processed in chunks that fit it. A geometry whose single view needs more than that
+ * is rejected with GCT_ERR_BUDGET. The first call on a device looks up the scratch address
+ * (cudaGetSymbolAddress) with that device current; make that first call before any stream
+ * capture. All calls share the one scratch array: calls whose GPU work overlaps (other streams,
+ * other threads, other plans) race on it and must be serialised by the caller. Nothing in it
+ * needs to start at zero; each call overwrites what it reads. */
+#define GCT_NOALLOC_SCRATCH_BYTES (64ull << 20)
+gct_status gct_fdk_execute_noalloc(gct_fdk_plan *plan, const float *proj_dev, float *vol_dev,
+                                   void *stream);
+
 /* Host-to-host drop-in: replaces void GCT::Recon::CUDA::reconstruct(cg, proj, vol)
  * (src/cuda/recon/recon_wrappers.cuh:15-43, recon_wrappers.cu:7-55). Synchronous, default
  * FiltParams, FP32 path; proj_host and vol_host are plain host arrays. */
