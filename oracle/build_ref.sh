@@ -1,11 +1,20 @@
 #!/usr/bin/env bash
-# Compiles satidev/gct's own host-callable sources, where they lie under the reference tree, with
-# the harness oracle/ref_host.cu into oracle/_ref/libgct_ref_host.so (TEST INFRASTRUCTURE ONLY).
+# Builds satidev/gct's own code, compiled from its sources where they lie under the reference tree,
+# into oracle/_ref/ (TEST INFRASTRUCTURE ONLY; nothing is copied out of the reference tree):
 #
-# Only translation units that build without the reference's missing Eigen submodule are used:
-#   src/cpp/recon/ramp_filter.cpp, src/cpp/recon/proj_filt_kernel.cpp, src/cpp/geom/rotation_geom.cpp
-# and the header-only __host__ __device__ functions included by ref_host.cu. Nothing is copied
-# out of the reference tree; outputs go to oracle/_ref/ only.
+#   libgct_ref_host.so  the reference's host-callable functions (ramp taps, rotation analysis,
+#                       Parker and cosine weights, projMapping, voxel positions) behind the C
+#                       entry points of oracle/ref_host.cu, for the golden vectors and CPU tests;
+#   ref_fdk             the reference's CUDA FDK (GCT::Recon::CUDA::reconstruct and everything it
+#                       calls) for sm_100a, driven by oracle/ref_fdk_main.cu, for the GPU parity
+#                       tests against the reference itself.
+#
+# The reference's Eigen submodule is empty in its tree. The translation units used here compile
+# without it except for declarations in src/cpp/geom/projection_matrix.h, which
+# oracle/eigen_api/ satisfies with a minimal matrix API (the matrices built with it are never read
+# by a kernel). The Eigen-dependent sources (geom_math.cpp, eigen_utils.cpp, projection_matrix.cpp,
+# proj_geom_cb_factory.cpp) are not compiled; ref_fdk_main.cu defines the two functions of theirs
+# the FDK links against.
 set -euo pipefail
 REF="${GCT_REFERENCE_DIR:-/root/reference}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
@@ -16,11 +25,32 @@ if [ ! -d "$REF/src" ]; then
 fi
 mkdir -p "$OUT"
 NVCC="${NVCC:-nvcc}"
-FLAGS=(-std=c++20 -O2 --expt-relaxed-constexpr -Xcompiler -fPIC -I "$REF/src" -gencode arch=compute_100a,code=sm_100a)
+ARCH=(-gencode arch=compute_100a,code=sm_100a)
+FLAGS=(-std=c++20 -O2 --expt-relaxed-constexpr --expt-extended-lambda -Xcompiler -fPIC -w -I "$REF/src"
+       -I "$HERE/eigen_api" "${ARCH[@]}")
+
+# host functions library
 "$NVCC" "${FLAGS[@]}" -c "$HERE/ref_host.cu" -o "$OUT/ref_host.o"
-for src in cpp/recon/ramp_filter.cpp cpp/recon/proj_filt_kernel.cpp cpp/geom/rotation_geom.cpp; do
-    g++ -std=c++20 -O2 -fPIC -I "$REF/src" -c "$REF/src/$src" -o "$OUT/$(basename "$src" .cpp).o"
+CPP=(cpp/recon/ramp_filter.cpp cpp/recon/proj_filt_kernel.cpp cpp/geom/rotation_geom.cpp
+     cpp/data/proj_meta_info.cpp cpp/geom/vec_wcs.cpp)
+for src in "${CPP[@]}"; do
+    g++ -std=c++20 -O2 -fPIC -w -I "$REF/src" -c "$REF/src/$src" -o "$OUT/$(basename "$src" .cpp).o" &
 done
-"$NVCC" -shared -o "$OUT/libgct_ref_host.so" "$OUT/ref_host.o" "$OUT/ramp_filter.o" "$OUT/proj_filt_kernel.o" \
-    "$OUT/rotation_geom.o" -lcudart
-echo "$OUT/libgct_ref_host.so"
+wait
+"$NVCC" "${ARCH[@]}" -shared -o "$OUT/libgct_ref_host.so" "$OUT/ref_host.o" "$OUT/ramp_filter.o" \
+    "$OUT/proj_filt_kernel.o" "$OUT/rotation_geom.o" -lcudart
+
+# the reference's CUDA FDK
+CU=(cuda/recon/recon_wrappers.cu cuda/geom/ct_geom_dev.cu cuda/recon/parker_weighting.cu
+    cuda/recon/ramp_filtering_fft.cu cuda/utils/check_error.cu cuda/utils/cuda_config.cu)
+pids=()
+"$NVCC" "${FLAGS[@]}" -c "$HERE/ref_fdk_main.cu" -o "$OUT/ref_fdk_main.o" & pids+=($!)
+for src in "${CU[@]}"; do
+    "$NVCC" "${FLAGS[@]}" -c "$REF/src/$src" -o "$OUT/ref_$(basename "$src" .cu).o" & pids+=($!)
+done
+for p in "${pids[@]}"; do wait "$p"; done
+"$NVCC" "${ARCH[@]}" -o "$OUT/ref_fdk" "$OUT/ref_fdk_main.o" "$OUT"/ref_recon_wrappers.o "$OUT"/ref_ct_geom_dev.o \
+    "$OUT"/ref_parker_weighting.o "$OUT"/ref_ramp_filtering_fft.o "$OUT"/ref_check_error.o "$OUT"/ref_cuda_config.o \
+    "$OUT/ramp_filter.o" "$OUT/proj_filt_kernel.o" "$OUT/rotation_geom.o" "$OUT/proj_meta_info.o" "$OUT/vec_wcs.o" \
+    -lcufft -lcudart
+echo "$OUT/libgct_ref_host.so $OUT/ref_fdk"

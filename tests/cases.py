@@ -36,27 +36,31 @@ class Case:
 
 def make_case(name: str, nv: int = 120, nc: int = 96, nr: int = 24, n: int = 48, nz: int = 8,
               rot_dir: g.RotDir = g.RotDir.CW, range_rad: float = 2 * math.pi, init_ang: float = 0.0,
-              vox: float = 1.0, mid=(0.0, 0.0, 0.0)) -> Case:
+              vox: float = 1.0, mid=(0.0, 0.0, 0.0), reference_sizes: bool = False) -> Case:
+    """With reference_sizes, the detector widths are those of the reference's FDK integration
+    tests (parallel 0.8961 mm, arc 0.0017922 rad, line and flat 2.0 mm, rows 1.14 mm)."""
     incr = range_rad / nv
     c0, r0 = (nc - 1) / 2.0, (nr - 1) / 2.0
     rot = g.RotationParams(rot_dir, init_ang, incr, nv)
+    w_par = 0.8961 if reference_sizes else 0.9
+    w_arc = 0.0017922 if reference_sizes else 0.11 / nc * 2.0
     if name == "parallel_1d":
-        det = (g.DetParallel(nc, 0.9),)
+        det = (g.DetParallel(nc, w_par),)
         params = g.Parallel1DProjGeomParams(c0, rot)
     elif name == "fan_arc":
-        det = (g.DetFanArc(nc, 0.11 / nc * 2.0),)
+        det = (g.DetFanArc(nc, w_arc),)
         params = g.FanBeamProjGeomParams(c0, rot, 1000.0, 500.0)
     elif name == "fan_line":
         det = (g.DetFanLine(nc, 2.0),)
         params = g.FanBeamProjGeomParams(c0, rot, 1536.0, 1000.0)
     elif name == "parallel_2d":
-        det = (g.DetParallel(nc, 0.9), g.DetParallel(nr, 1.14))
+        det = (g.DetParallel(nc, w_par), g.DetParallel(nr, 1.14))
         params = g.Parallel2DProjGeomParams(c0, rot, r0)
     elif name == "cone_parallel":
-        det = (g.DetParallel(nc, 0.9), g.DetFanLine(nr, 1.14))
+        det = (g.DetParallel(nc, w_par), g.DetFanLine(nr, 1.14))
         params = g.ConeBeamProjGeomParams(c0, rot, 1536.0, 1000.0, r0)
     elif name == "cone_cyl":
-        det = (g.DetFanArc(nc, 0.11 / nc * 2.0), g.DetFanLine(nr, 1.14))
+        det = (g.DetFanArc(nc, w_arc), g.DetFanLine(nr, 1.14))
         params = g.ConeBeamProjGeomParams(c0, rot, 1000.0, 500.0, r0)
     elif name == "cone_flat":
         det = (g.DetFanLine(nc, 2.0), g.DetFanLine(nr, 2.0))
@@ -76,5 +80,9 @@ def make_case(name: str, nv: int = 120, nc: int = 96, nr: int = 24, n: int = 48,
     return Case(name, cg, og, vg, ov)
 
 
-def oracle_projections(case: Case) -> np.ndarray:
-    return orc.phantom(case.og, np.array(PHANTOM)).astype(np.float32)
+def oracle_projections(case: Case, scale: float = 1.0) -> np.ndarray:
+    """Float32 line integrals (FP64 oracle) of PHANTOM with positions and sizes scaled by `scale`."""
+    ph = np.array(PHANTOM)
+    ph[:, :6] *= scale
+    ph[:, 7] /= scale  # keep line integrals of the same order
+    return orc.phantom(case.og, ph).astype(np.float32)
