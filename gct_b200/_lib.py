@@ -92,6 +92,7 @@ SIGNATURES = {
                       P(C.c_double), P(C.c_double), P(C.c_double)],
     "gct_fdk_plan_create": [P(gct_ct_geom), P(gct_vol_geom), P(gct_filt_params), P(gct_fdk_opts), P(VP)],
     "gct_fdk_plan_destroy": [VP],
+    "gct_fdk_plan_check": [VP],
     "gct_fdk_plan_workspace_bytes": [VP, P(C.c_uint64)],
     "gct_fdk_execute": [VP, VP, VP, VP, VP],
     "gct_fdk_filter": [VP, VP, VP, VP],

@@ -1,5 +1,6 @@
 // C ABI of the FDK engine (include/gct_fdk.h): plans, execution, stage entry points and the
 // host geometry functions. All failures become a gct_status plus a thread-local message.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -14,6 +15,7 @@
 #include <vector>
 
 #include "../../include/gct_fdk.h"
+#include "filter_gemm.hpp"
 #include "geometry.hpp"
 #include "kernels.hpp"
 #include "project.hpp"
@@ -124,6 +126,11 @@ struct gct_fdk_plan {
     DevBuf<float> coefs;
     DevBuf<float> vscale, vinv, amax;
     DevBuf<unsigned char> work;
+    // Toeplitz-GEMM filter: B = T^T split into BF16 hi/lo [Np][Kp], A rows [nv*nr][Kp], FP32 rows
+    int Kp = 0, Np = 0;
+    DevBuf<__nv_bfloat16> th, tl, xh, xl;
+    DevBuf<float> ybuf;
+    DevBuf<int> gemm_err;
     // staging for gct_fdk_execute_host
     DevBuf<float> host_proj, host_vol;
     cudaStream_t copy_stream = nullptr;
@@ -163,8 +170,6 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
         gct::fail(GCT_ERR_INVALID_ARG, "unknown filter option");
     if (p->opts.storage != GCT_STORAGE_F32 && p->opts.storage != GCT_STORAGE_F16)
         gct::fail(GCT_ERR_INVALID_ARG, "unknown storage option");
-    if (p->opts.filter == GCT_FILTER_TOEPLITZ_BF16X3)
-        gct::fail(GCT_ERR_NOT_SUPPORTED, "Toeplitz GEMM filter is not built into this library");
     if (!gct::rotation_info(p->geom, &p->rot))
         gct::fail(GCT_ERR_INVALID_ARG, "Invalid X-ray source trajectory.");
     p->nv = static_cast<int>(g->num_views);
@@ -229,6 +234,29 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
     p->H.upload(H.data(), H.size(), "plan filter spectrum");
     p->tw.upload(tw.data(), tw.size(), "plan twiddles");
     p->coefs.upload(coefs.data(), coefs.size(), "plan backprojection coefficients");
+    if (p->opts.filter == GCT_FILTER_TOEPLITZ_BF16X3) {
+        // B = T^T with T[k][c] = g(c - k): row n holds g(n - k); taps g(m) = taps[m + nc/2]
+        p->Kp = gct::gemm_pad_k(p->nc);
+        p->Np = gct::gemm_pad_n(p->nc);
+        std::vector<__nv_bfloat16> bh(static_cast<size_t>(p->Np) * p->Kp, __float2bfloat16(0.f)), bl(bh);
+        for (int n = 0; n < p->nc; ++n)
+            for (int k = 0; k < p->nc; ++k) {
+                const int m = n - k + p->nc / 2;
+                if (m < 0 || m >= p->nc) continue;
+                const double t = taps[m];
+                const __nv_bfloat16 hi = __float2bfloat16(static_cast<float>(t));
+                bh[static_cast<size_t>(n) * p->Kp + k] = hi;
+                bl[static_cast<size_t>(n) * p->Kp + k] = __float2bfloat16(static_cast<float>(t - static_cast<double>(__bfloat162float(hi))));
+            }
+        p->th.upload(bh.data(), bh.size(), "Toeplitz matrix (hi)");
+        p->tl.upload(bl.data(), bl.size(), "Toeplitz matrix (lo)");
+        const size_t rows = static_cast<size_t>(p->nv) * p->nr;
+        p->xh.alloc(rows * p->Kp, "GEMM rows (hi)");
+        p->xl.alloc(rows * p->Kp, "GEMM rows (lo)");
+        p->ybuf.alloc(rows * p->nc, "GEMM filtered rows");
+        p->gemm_err.alloc(1, "GEMM status");
+        cuda_check(cudaMemset(p->gemm_err.p, 0, sizeof(int)), "GEMM status reset");
+    }
     if (p->opts.storage == GCT_STORAGE_F16) {
         p->vscale.alloc(p->nv, "plan view scales");
         p->vinv.alloc(p->nv, "plan view scales");
@@ -246,9 +274,63 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
         gct::fail(GCT_ERR_INVALID_ARG, "backprojection block must hold 32..256 threads");
 }
 
+// Toeplitz-GEMM form of run_filter: split, tcgen05 GEMM into FP32 rows, then quads (or the rows
+// themselves for the plain output).
+void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, int mode, int vb, int vc, cudaStream_t s)
+{
+    const long long row0 = static_cast<long long>(vb) * p->nr, rows = static_cast<long long>(vc) * p->nr;
+    gct::SplitArgs sa;
+    sa.proj = proj;
+    sa.row0 = row0;
+    sa.rows = rows;
+    sa.nr = p->nr;
+    sa.nc = p->nc;
+    sa.Kp = p->Kp;
+    sa.kind = p->kind;
+    sa.du = static_cast<float>(p->geom.det_row.sampling_width);
+    sa.dv = static_cast<float>(p->geom.det_col.sampling_width);
+    sa.fview = p->fview.p;
+    sa.parker = p->parker.p;
+    sa.xh = p->xh.p;
+    sa.xl = p->xl.p;
+    gct::launch_split(sa, p->num_sms, s);
+    cuda_check(cudaGetLastError(), "split kernel launch");
+    gct::GemmLaunch gl;
+    gl.xh = p->xh.p;
+    gl.xl = p->xl.p;
+    gl.a_rows = static_cast<long long>(p->nv) * p->nr;
+    gl.th = p->th.p;
+    gl.tl = p->tl.p;
+    gl.Np = p->Np;
+    gl.Kp = p->Kp;
+    gl.m_begin = static_cast<int>(row0);
+    gl.M = static_cast<int>(rows);
+    gl.N = p->nc;
+    gl.Y = (mode == gct::kOutPlainF32 ? static_cast<float *>(out) : p->ybuf.p) + row0 * p->nc;
+    gl.ldy = p->nc;
+    gl.err = p->gemm_err.p;
+    cuda_check(gct::launch_toeplitz_gemm(gl, p->num_sms, s), "Toeplitz GEMM launch");
+    if (mode == gct::kOutPlainF32) return;
+    gct::QuadArgs qa;
+    qa.Y = gl.Y;
+    qa.ldy = p->nc;
+    qa.v0 = vb;
+    qa.nv = vc;
+    qa.nr = p->nr;
+    qa.nc = p->nc;
+    qa.vscale = (mode == gct::kOutQuadF16) ? p->vscale.p : nullptr;
+    qa.out = out;
+    gct::launch_quads_from_rows(qa, mode, p->num_sms, s);
+    cuda_check(cudaGetLastError(), "quad kernel launch");
+}
+
 void run_filter(gct_fdk_plan *p, const float *proj, void *out, int mode, int vb, int vc, cudaStream_t s)
 {
     if (vc <= 0) return;
+    if (p->opts.filter == GCT_FILTER_TOEPLITZ_BF16X3) {
+        run_filter_gemm(p, proj, out, mode, vb, vc, s);
+        return;
+    }
     const long long pix = static_cast<long long>(p->nr) * p->nc;
     gct::FilterArgs fa;
     fa.proj = proj + vb * pix;
@@ -566,6 +648,22 @@ gct_status gct_fdk_execute(gct_fdk_plan *plan, const float *proj_dev, float *vol
         if (!plan) gct::fail(GCT_ERR_INVALID_ARG, "NULL plan");
         DeviceGuard dg(plan->device);
         execute(plan, proj_dev, vol_dev, workspace, static_cast<cudaStream_t>(stream));
+    });
+}
+
+gct_status gct_fdk_plan_check(gct_fdk_plan *plan)
+{
+    return guarded([&] {
+        if (!plan) gct::fail(GCT_ERR_INVALID_ARG, "NULL plan");
+        DeviceGuard dg(plan->device);
+        cuda_check(cudaDeviceSynchronize(), "device synchronisation");
+        if (!plan->gemm_err.p) return;
+        int e = 0;
+        cuda_check(cudaMemcpy(&e, plan->gemm_err.p, sizeof(int), cudaMemcpyDeviceToHost), "GEMM status read");
+        if (e) {
+            cuda_check(cudaMemset(plan->gemm_err.p, 0, sizeof(int)), "GEMM status reset");
+            gct::fail(GCT_ERR_TIMEOUT, "Toeplitz GEMM pipeline wait timed out (stage " + std::to_string(e) + ")");
+        }
     });
 }
 

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/gct_fdk.h"
 #include "kernels.hpp"
 
 namespace gct {
@@ -42,6 +43,35 @@ __device__ __forceinline__ void split_coord(float x, int &i, float &f)
     const float t = (x - 0.5f) + 12582912.0f;
     i = __float_as_int(t) - 0x4B400000;
     f = x - (t - 12582912.0f);
+}
+
+// Cosine pre-weight of pixel (c, r) of a view, per geometry (src/cuda/recon/cos_weighting.cuh:
+// 16-153). c0/r0 are the view's detector centres, du/dv the sampler widths.
+__device__ __forceinline__ float cos_weight_dev(int kind, float c0, float r0, float sdd, float du,
+                                            float dv, int c, int r)
+{
+    switch (kind) {
+        case GCT_GEOM_FAN_ARC: return cosf((static_cast<float>(c) - c0) * du);
+        case GCT_GEOM_FAN_LINE: {
+            const float u = (static_cast<float>(c) - c0) * du;
+            return sdd * rsqrtf(u * u + sdd * sdd);
+        }
+        case GCT_GEOM_CONE_PARALLEL: {
+            const float v = (static_cast<float>(r) - r0) * dv;
+            return sdd * rsqrtf(v * v + sdd * sdd);
+        }
+        case GCT_GEOM_CONE_CYL: {
+            const float g = (static_cast<float>(c) - c0) * du;
+            const float v = (static_cast<float>(r) - r0) * dv;
+            return cosf(g) * sdd * rsqrtf(v * v + sdd * sdd);
+        }
+        case GCT_GEOM_CONE_FLAT: {
+            const float u = (static_cast<float>(c) - c0) * du;
+            const float v = (static_cast<float>(r) - r0) * dv;
+            return sdd * rsqrtf(u * u + v * v + sdd * sdd);
+        }
+        default: return 1.0f;  // parallel kinds
+    }
 }
 
 __device__ __forceinline__ float rcp_approx(float x)

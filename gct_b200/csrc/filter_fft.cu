@@ -22,35 +22,6 @@
 namespace gct {
 namespace {
 
-// Cosine pre-weight of pixel (c, r) of a view, per geometry (src/cuda/recon/cos_weighting.cuh:
-// 16-153). c0/r0 are the view's detector centres, du/dv the sampler widths.
-__device__ __forceinline__ float cos_weight(int kind, float c0, float r0, float sdd, float du,
-                                            float dv, int c, int r)
-{
-    switch (kind) {
-        case GCT_GEOM_FAN_ARC: return cosf((static_cast<float>(c) - c0) * du);
-        case GCT_GEOM_FAN_LINE: {
-            const float u = (static_cast<float>(c) - c0) * du;
-            return sdd * rsqrtf(u * u + sdd * sdd);
-        }
-        case GCT_GEOM_CONE_PARALLEL: {
-            const float v = (static_cast<float>(r) - r0) * dv;
-            return sdd * rsqrtf(v * v + sdd * sdd);
-        }
-        case GCT_GEOM_CONE_CYL: {
-            const float g = (static_cast<float>(c) - c0) * du;
-            const float v = (static_cast<float>(r) - r0) * dv;
-            return cosf(g) * sdd * rsqrtf(v * v + sdd * sdd);
-        }
-        case GCT_GEOM_CONE_FLAT: {
-            const float u = (static_cast<float>(c) - c0) * du;
-            const float v = (static_cast<float>(r) - r0) * dv;
-            return sdd * rsqrtf(u * u + v * v + sdd * sdd);
-        }
-        default: return 1.0f;  // parallel kinds
-    }
-}
-
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -251,8 +222,8 @@ __global__ void __launch_bounds__(256) filter_fft_kernel(FilterArgs a, int seg_r
                     x[q] = make_float2(0.f, 0.f);
                     if (k < nc) {
                         const float w = __ldg(wpk + k);
-                        x[q].x = __ldg(pa + k) * w * cos_weight(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k, ra);
-                        if (has_b) x[q].y = __ldg(pb + k) * w * cos_weight(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k, ra + 1);
+                        x[q].x = __ldg(pa + k) * w * cos_weight_dev(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k, ra);
+                        if (has_b) x[q].y = __ldg(pb + k) * w * cos_weight_dev(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k, ra + 1);
                     }
                 }
                 const float2 t0 = cadd(x[0], x[2]), t1 = csub(x[0], x[2]), t2 = cadd(x[1], x[3]);

@@ -1,0 +1,421 @@
+// Ramp filter as a Toeplitz GEMM on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// The reference filters each detector row by FFT convolution (src/cuda/recon/ramp_filtering_fft.cuh:
+// 208-219). A row convolution with N taps is also the product of the row with an N x N Toeplitz
+// matrix T[k][c] = g(c - k), so a whole projection stack is one GEMM Y = X T with
+// M = views x rows, K = N = detector columns. Here it runs as a 3-term split-precision BF16 GEMM
+// with FP32 accumulation:
+//     X = Xh + Xl, T = Th + Tl (BF16 hi/lo parts),  Y = Xh Th + Xh Tl + Xl Th
+// (the dropped Xl Tl term is ~2^-16 relative). Stages:
+//   1. split_kernel: cosine x Parker weighting fused into the load, BF16 hi/lo split, zero padding
+//      of K to a multiple of 64;
+//   2. toeplitz_gemm_kernel: persistent, warp-specialised tcgen05 GEMM. Warp 0 issues TMA loads of
+//      128 x 64 A tiles and 256 x 64 B tiles (128B swizzle) into a 4-stage shared-memory ring;
+//      one thread of warp 1 issues tcgen05.mma (M 128, N 256, K 16) into one of two TMEM
+//      accumulators of 256 FP32 columns; warps 2-5 drain the other accumulator with tcgen05.ld and
+//      store FP32 rows. The three terms are one K loop of 3 K/64 steps.
+//   3. quads_from_rows_kernel: the filtered rows become the backprojector's bilinear-coefficient
+//      quads (FP32 or FP16 with the per-view scale).
+// Every mbarrier wait is bounded (2 s of %globaltimer); on timeout the kernel records an error
+// code, stops issuing work, frees its TMEM and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include "../../include/gct_fdk.h"
+#include "common.cuh"
+#include "filter_gemm.hpp"
+
+namespace gct {
+namespace {
+
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4, UMMA_K = 16;
+constexpr uint32_t A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int TMEM_COLS = 512;  // two accumulators of BN FP32 columns
+constexpr unsigned long long kWaitNs = 2000000000ull;
+
+// ---- small PTX wrappers --------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+// Bounded wait for phase `parity` of barrier `bar`; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    const unsigned long long t0 = global_ns();
+    while (true) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (global_ns() - t0 > kWaitNs) return false;
+    }
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int c0, int c1, uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major operand tile written by TMA with 128B swizzle: 8-row atoms of 128 B rows, atoms 1024 B
+// apart (SBO), LBO unused (1), descriptor version 1, layout type 2 (128B swizzle).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr)
+{
+    return static_cast<uint64_t>((addr >> 4) & 0x3FFFu) | (1ull << 16) | (static_cast<uint64_t>(1024 >> 4) << 32) |
+           (1ull << 46) | (2ull << 61);
+}
+// kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, M = 128, N = 256.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(BN >> 3) << 17) |
+                            (static_cast<uint32_t>(BM >> 4) << 24);
+
+__device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+#define GCT_LD32(r, taddr)                                                                                       \
+    asm volatile(                                                                                                \
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17," \
+        "%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"                                      \
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),          \
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),    \
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),  \
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])   \
+        : "r"(taddr))
+
+struct GemmParams {
+    int M;          // rows (views x detector rows)
+    int N;          // valid output columns (detector columns)
+    int m_begin;    // first row of this launch in the A tensor
+    int num_kb;     // K / 64 (padded K)
+    int m_tiles, n_tiles;
+    float *Y;       // [M][ldy] FP32, row m_begin + i at Y + i * ldy
+    int ldy;
+    int *err;       // set non-zero on a timed-out wait
+};
+
+__global__ void __launch_bounds__(192, 1)
+    toeplitz_gemm_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+                         const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
+                         GemmParams p)
+{
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    // bars: full[STAGES], empty[STAGES], tfull[2], tempty[2]; then the TMEM base address
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 4);
+    __shared__ int s_fail;
+    const volatile int *fail_flag = &s_fail;  // re-read on every loop test
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    auto full = [&](int s) { return smem_u32(bars + s); };
+    auto empty = [&](int s) { return smem_u32(bars + STAGES + s); };
+    auto tfull = [&](int a) { return smem_u32(bars + 2 * STAGES + a); };
+    auto tempty = [&](int a) { return smem_u32(bars + 2 * STAGES + 2 + a); };
+
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(full(s), 1);
+            mbar_init(empty(s), 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(tfull(a), 1);
+            mbar_init(tempty(a), 4);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const int total = p.m_tiles * p.n_tiles;
+    const int ksteps = 3 * p.num_kb;
+
+    if (warp == 0) {
+        if (lane == 0) {  // TMA producer
+            int stage = 0;
+            uint32_t phase = 0;
+            for (int t = blockIdx.x; t < total && !*fail_flag; t += gridDim.x) {
+                const int m0 = p.m_begin + (t / p.n_tiles) * BM, n0 = (t % p.n_tiles) * BN;
+                for (int ks = 0; ks < ksteps; ++ks) {
+                    const int seg = ks / p.num_kb, kb = ks - seg * p.num_kb;
+                    if (!mbar_wait(empty(stage), phase ^ 1)) {
+                        atomicExch(&s_fail, 1);
+                        break;
+                    }
+                    mbar_expect_tx(full(stage), STAGE_BYTES);
+                    const uint32_t sa = smem_u32(smem + stage * STAGE_BYTES);
+                    tma_load_2d(sa, seg == 2 ? &mAl : &mAh, kb * BK, m0, full(stage));
+                    tma_load_2d(sa + A_BYTES, seg == 1 ? &mBl : &mBh, kb * BK, n0, full(stage));
+                    if (++stage == STAGES) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {  // MMA issuer
+            int stage = 0, acc = 0;
+            uint32_t phase = 0, aphase = 0;
+            for (int t = blockIdx.x; t < total && !*fail_flag; t += gridDim.x) {
+                if (!mbar_wait(tempty(acc), aphase ^ 1)) {
+                    atomicExch(&s_fail, 2);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem_base + static_cast<uint32_t>(acc * BN);
+                bool ok = true;
+                for (int ks = 0; ks < ksteps; ++ks) {
+                    if (!mbar_wait(full(stage), phase)) {
+                        atomicExch(&s_fail, 3);
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sa = smem_u32(smem + stage * STAGE_BYTES);
+                    const uint64_t da = smem_desc(sa), db = smem_desc(sa + A_BYTES);
+#pragma unroll
+                    for (int k = 0; k < BK / UMMA_K; ++k)  // +32 B along K per step: +2 in the address field
+                        umma(d, da + 2 * k, db + 2 * k, (ks > 0 || k > 0) ? 1u : 0u);
+                    umma_commit(empty(stage));
+                    if (++stage == STAGES) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+                if (!ok) break;
+                umma_commit(tfull(acc));
+                if (++acc == 2) {
+                    acc = 0;
+                    aphase ^= 1;
+                }
+            }
+        }
+    } else {  // epilogue warps 2..5: TMEM lane quadrant (warp % 4)
+        const int q = warp & 3;
+        int acc = 0;
+        uint32_t aphase = 0;
+        for (int t = blockIdx.x; t < total && !*fail_flag; t += gridDim.x) {
+            const int mt = t / p.n_tiles, n0 = (t % p.n_tiles) * BN;
+            if (!mbar_wait(tfull(acc), aphase)) {
+                atomicExch(&s_fail, 4);
+                break;
+            }
+            tc_fence_after();
+            const int row = mt * BM + q * 32 + lane;  // relative to m_begin
+            float *yrow = p.Y + static_cast<long long>(row) * p.ldy;
+#pragma unroll 1
+            for (int ch = 0; ch < BN / 32; ++ch) {
+                uint32_t r[32];
+                const uint32_t taddr = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * BN + ch * 32);
+                GCT_LD32(r, taddr);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                const int c0 = n0 + ch * 32;
+                if (row < p.M) {
+                    if (c0 + 32 <= p.N && (p.ldy & 3) == 0) {
+                        float4 *dst = reinterpret_cast<float4 *>(yrow + c0);
+#pragma unroll
+                        for (int j = 0; j < 8; ++j)
+                            dst[j] = make_float4(__uint_as_float(r[4 * j]), __uint_as_float(r[4 * j + 1]),
+                                                 __uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3]));
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            if (c0 + j < p.N) yrow[c0 + j] = __uint_as_float(r[j]);
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(tempty(acc));
+            if (++acc == 2) {
+                acc = 0;
+                aphase ^= 1;
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && s_fail) atomicExch(p.err, s_fail);
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+// Cosine x Parker weighting and BF16 hi/lo split of rows [row0, row0 + rows) into [rows][Kp].
+__global__ void split_kernel(SplitArgs a)
+{
+    const long long total = static_cast<long long>(a.rows) * a.Kp;
+    for (long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+         idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int k = static_cast<int>(idx % a.Kp);
+        const long long rl = idx / a.Kp;
+        const long long row = a.row0 + rl;
+        float x = 0.f;
+        if (k < a.nc) {
+            const int v = static_cast<int>(row / a.nr), r = static_cast<int>(row - static_cast<long long>(v) * a.nr);
+            const float4 gv = __ldg(&a.fview[v]);
+            x = __ldg(a.proj + row * a.nc + k) * __ldg(a.parker + static_cast<long long>(v) * a.nc + k) *
+                cos_weight_dev(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k, r);
+        }
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
+        a.xh[row * a.Kp + k] = h;
+        a.xl[row * a.Kp + k] = l;
+    }
+}
+
+// Filtered rows Y (row stride ldy) of views [v0, v0 + nv) -> bilinear-coefficient quads.
+template <int MODE>
+__global__ void quads_from_rows_kernel(QuadArgs a)
+{
+    const int qpitch = a.nc + 2 * kQuadPad, qrows = a.nr + 2 * kQuadPad;
+    const long long per_view = static_cast<long long>(qpitch) * qrows;
+    const long long total = per_view * a.nv;
+    for (long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+         idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int vl = static_cast<int>(idx / per_view);
+        const long long rem = idx - static_cast<long long>(vl) * per_view;
+        const int r = static_cast<int>(rem / qpitch) - kQuadPad, c = static_cast<int>(rem % qpitch) - kQuadPad;
+        const int v = a.v0 + vl;
+        const float sc = a.vscale ? a.vscale[v] : 1.0f;
+        auto y = [&](int rr, int cc) -> float {
+            if (rr < 0 || rr >= a.nr || cc < 0 || cc >= a.nc) return 0.f;
+            return sc * a.Y[(static_cast<long long>(vl) * a.nr + rr) * a.ldy + cc];
+        };
+        const float p00 = y(r, c), p01 = y(r, c + 1), p10 = y(r + 1, c), p11 = y(r + 1, c + 1);
+        const float l = p00 + p10, rt = p01 + p11;
+        const float A = 0.5f * l, B = 0.5f * (rt - l), Cc = p10 - p00, D = (p11 - p01) - (p10 - p00);
+        const long long qidx = static_cast<long long>(v) * per_view + rem;
+        if (MODE == kOutQuadF32) {
+            static_cast<float4 *>(a.out)[qidx] = make_float4(A, B, Cc, D);
+        } else {
+            const __half2 lo = __floats2half2_rn(A, Cc), hi = __floats2half2_rn(B, D);
+            uint2 u;
+            u.x = *reinterpret_cast<const unsigned *>(&lo);
+            u.y = *reinterpret_cast<const unsigned *>(&hi);
+            static_cast<uint2 *>(a.out)[qidx] = u;
+        }
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void *ptr = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+    }
+    return fn;
+}
+
+// 2D BF16 tensor [rows][cols] (cols contiguous), box cols_box x rows_box, 128B swizzle.
+bool make_map(CUtensorMap *m, const void *base, unsigned long long rows, unsigned long long cols, unsigned rows_box)
+{
+    auto fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {cols, rows};
+    const cuuint64_t strides[1] = {cols * 2};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(BK), rows_box};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+int gemm_pad_k(int n) { return (n + BK - 1) / BK * BK; }
+int gemm_pad_n(int n) { return (n + BN - 1) / BN * BN; }
+size_t toeplitz_gemm_smem_bytes() { return STAGES * STAGE_BYTES + 1024 + 256; }
+
+void launch_split(const SplitArgs &a, int num_sms, cudaStream_t s)
+{
+    long long total = static_cast<long long>(a.rows) * a.Kp;
+    long long grid = (total + 255) / 256;
+    if (grid > static_cast<long long>(num_sms) * 32) grid = static_cast<long long>(num_sms) * 32;
+    split_kernel<<<static_cast<unsigned>(grid < 1 ? 1 : grid), 256, 0, s>>>(a);
+}
+
+void launch_quads_from_rows(const QuadArgs &a, int mode, int num_sms, cudaStream_t s)
+{
+    const long long total = static_cast<long long>(a.nv) * (a.nr + 2 * kQuadPad) * (a.nc + 2 * kQuadPad);
+    long long grid = (total + 255) / 256;
+    if (grid > static_cast<long long>(num_sms) * 32) grid = static_cast<long long>(num_sms) * 32;
+    if (mode == kOutQuadF32)
+        quads_from_rows_kernel<kOutQuadF32><<<static_cast<unsigned>(grid < 1 ? 1 : grid), 256, 0, s>>>(a);
+    else
+        quads_from_rows_kernel<kOutQuadF16><<<static_cast<unsigned>(grid < 1 ? 1 : grid), 256, 0, s>>>(a);
+}
+
+cudaError_t launch_toeplitz_gemm(const GemmLaunch &g, int num_sms, cudaStream_t s)
+{
+    CUtensorMap mAh, mAl, mBh, mBl;
+    if (!make_map(&mAh, g.xh, g.a_rows, g.Kp, BM) || !make_map(&mAl, g.xl, g.a_rows, g.Kp, BM) ||
+        !make_map(&mBh, g.th, g.Np, g.Kp, BN) || !make_map(&mBl, g.tl, g.Np, g.Kp, BN))
+        return cudaErrorInvalidValue;
+    GemmParams p;
+    p.M = g.M;
+    p.N = g.N;
+    p.m_begin = g.m_begin;
+    p.num_kb = g.Kp / BK;
+    p.m_tiles = (g.M + BM - 1) / BM;
+    p.n_tiles = g.Np / BN;
+    p.Y = g.Y;
+    p.ldy = g.ldy;
+    p.err = g.err;
+    const int tiles = p.m_tiles * p.n_tiles;
+    const int grid = tiles < num_sms ? tiles : num_sms;
+    const size_t smem = toeplitz_gemm_smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(toeplitz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    toeplitz_gemm_kernel<<<grid, 192, smem, s>>>(mAh, mAl, mBh, mBl, p);
+    return cudaGetLastError();
+}
+
+}  // namespace gct

@@ -1,0 +1,47 @@
+// Launch interfaces of the Toeplitz-GEMM ramp filter (filter_gemm.cu).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace gct {
+
+int gemm_pad_k(int n);  // K padded to the 64-column tile
+int gemm_pad_n(int n);  // N padded to the 256-column tile
+size_t toeplitz_gemm_smem_bytes();
+
+struct SplitArgs {
+    const float *proj = nullptr;  // [views][nr][nc], full stack
+    long long row0 = 0;           // first global row (view * nr + row)
+    long long rows = 0;
+    int nr = 0, nc = 0, Kp = 0;
+    int kind = 0;
+    float du = 0.f, dv = 0.f;
+    const float4 *fview = nullptr;
+    const float *parker = nullptr;
+    __nv_bfloat16 *xh = nullptr, *xl = nullptr;  // [all rows][Kp]
+};
+void launch_split(const SplitArgs &a, int num_sms, cudaStream_t s);
+
+struct GemmLaunch {
+    const __nv_bfloat16 *xh = nullptr, *xl = nullptr;  // A: [a_rows][Kp]
+    long long a_rows = 0;
+    const __nv_bfloat16 *th = nullptr, *tl = nullptr;  // B = T^T: [Np][Kp]
+    int Np = 0, Kp = 0;
+    int m_begin = 0, M = 0, N = 0;
+    float *Y = nullptr;  // row m_begin + i at Y + i * ldy
+    int ldy = 0;
+    int *err = nullptr;
+};
+cudaError_t launch_toeplitz_gemm(const GemmLaunch &g, int num_sms, cudaStream_t s);
+
+struct QuadArgs {
+    const float *Y = nullptr;  // filtered rows of views [v0, v0 + nv), row stride ldy
+    int ldy = 0;
+    int v0 = 0, nv = 0, nr = 0, nc = 0;
+    const float *vscale = nullptr;
+    void *out = nullptr;       // quads of the full stack
+};
+void launch_quads_from_rows(const QuadArgs &a, int mode, int num_sms, cudaStream_t s);
+
+}  // namespace gct

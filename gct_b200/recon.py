@@ -158,6 +158,10 @@ class FdkPlan:
         _lib.check(self._lib.gct_fdk_filter(self._handle, C.c_void_p(_ptr(proj)), C.c_void_p(_ptr(out)),
                                             C.c_void_p(_stream(stream))))
 
+    def check(self) -> None:
+        """Synchronises and raises GctError if the plan's kernels recorded a failure."""
+        _lib.check(self._lib.gct_fdk_plan_check(self._handle))
+
     def close(self) -> None:
         if self._handle:
             _lib.check(self._lib.gct_fdk_plan_destroy(self._handle))

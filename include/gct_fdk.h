@@ -222,6 +222,10 @@ gct_status gct_fdk_plan_create(const gct_ct_geom *geom, const gct_vol_geom *vol,
                                gct_fdk_plan **out);
 gct_status gct_fdk_plan_destroy(gct_fdk_plan *plan);
 
+/* Synchronises the device and reports a failure recorded asynchronously by the plan's kernels:
+ * GCT_ERR_TIMEOUT if a bounded pipeline wait of the Toeplitz-GEMM filter ran out. */
+gct_status gct_fdk_plan_check(gct_fdk_plan *plan);
+
 /* Device bytes of scratch that gct_fdk_execute needs (the filtered-projection stack). */
 gct_status gct_fdk_plan_workspace_bytes(const gct_fdk_plan *plan, uint64_t *bytes);
 
