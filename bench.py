@@ -66,6 +66,8 @@ def parse_args():
     ap.add_argument("--config", choices=sorted(CONFIGS), default="cone512")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--zpt", type=int, default=0, help="backprojection z per thread (0 = default)")
+    ap.add_argument("--mixed-filter", choices=["gemm", "fft"], default="gemm",
+                    help="ramp filter of the mixed path: BF16x3 Toeplitz GEMM on tcgen05, or the FFT")
     ap.add_argument("--no-error", action="store_true", help="skip the FP64 oracle error check")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -340,9 +342,12 @@ def run_gct(args, cfg, rank, world, local_rank):
     updates = nx * ny * nz * cg.num_views
     proj = make_projections(cg, cfg, args.seed + rank, device)
     stream = torch.cuda.current_stream()
+    mixed_filter = g.FILTER_TOEPLITZ_BF16X3 if args.mixed_filter == "gemm" else g.FILTER_FFT
     plans = {
-        "mixed": g.FdkPlan(cg, vg, opts=g.FdkOptions(storage=g.STORAGE_F16, z_per_thread=args.zpt)),
-        "fp32": g.FdkPlan(cg, vg, opts=g.FdkOptions(storage=g.STORAGE_F32, z_per_thread=args.zpt)),
+        "mixed": g.FdkPlan(cg, vg, opts=g.FdkOptions(filter=mixed_filter, storage=g.STORAGE_F16,
+                                                     z_per_thread=args.zpt)),
+        "fp32": g.FdkPlan(cg, vg, opts=g.FdkOptions(filter=g.FILTER_FFT, storage=g.STORAGE_F32,
+                                                    z_per_thread=args.zpt)),
     }
     vols = {k: torch.empty(vg.shape, dtype=torch.float32, device=device) for k in plans}
     for k, p in plans.items():
@@ -424,7 +429,9 @@ def run_gct(args, cfg, rank, world, local_rank):
         "cpu_baseline": cpu,
         "e2e": e2e,
         "clocks": clocks,
-        "gpu_launches": 4 * args.steps,
+        # per mixed step: view max, view scale, (split, GEMM, quads | FFT filter), backprojection
+        "gpu_launches": (6 if args.mixed_filter == "gemm" else 4) * args.steps,
+        "mixed_filter": ("BF16x3 Toeplitz GEMM (tcgen05)" if args.mixed_filter == "gemm" else "shared-memory FFT"),
     }
     print(json.dumps(line), flush=True)
 

@@ -124,7 +124,6 @@ struct gct_fdk_plan {
     DevBuf<float> parker;
     DevBuf<float2> H, tw;
     DevBuf<float> coefs;
-    DevBuf<float> vscale, vinv, amax;
     DevBuf<unsigned char> work;
     // Toeplitz-GEMM filter: B = T^T split into BF16 hi/lo [Np][Kp], A rows [nv*nr][Kp], FP32 rows
     int Kp = 0, Np = 0;
@@ -143,11 +142,38 @@ struct gct_fdk_plan {
     }
 
     size_t quad_bytes() const { return opts.storage == GCT_STORAGE_F16 ? 8 : 16; }
-    size_t workspace_bytes() const
+    // Workspace layout: the quads of view v at v * view_bytes(), then (FP16 storage) the per-view
+    // maxima, scales and inverse scales, nv floats each, from quad_region() on.
+    size_t view_bytes() const
     {
-        return static_cast<size_t>(nv) * (nr + 2 * gct::kQuadPad) * (nc + 2 * gct::kQuadPad) * quad_bytes();
+        return static_cast<size_t>(nr + 2 * gct::kQuadPad) * (nc + 2 * gct::kQuadPad) * quad_bytes();
     }
+    size_t quad_region() const { return (static_cast<size_t>(nv) * view_bytes() + 255) & ~static_cast<size_t>(255); }
+    size_t scale_bytes() const { return opts.storage == GCT_STORAGE_F16 ? 3 * sizeof(float) * nv : 0; }
+    size_t workspace_bytes() const { return quad_region() + scale_bytes(); }
 };
+
+namespace {
+// One filtered stack: the quads of view v at quads + v * view_bytes() and, for FP16 storage, the
+// view's maximum, scale and inverse scale at amax[v], vscale[v], vinv[v]. All four are view-0
+// addresses, so a chunk of views may live at a shifted base.
+struct StackRef {
+    unsigned char *quads = nullptr;
+    float *amax = nullptr, *vscale = nullptr, *vinv = nullptr;
+};
+
+StackRef stack_of(const gct_fdk_plan *p, void *workspace)
+{
+    StackRef r;
+    r.quads = static_cast<unsigned char *>(workspace);
+    if (p->opts.storage == GCT_STORAGE_F16) {
+        r.amax = reinterpret_cast<float *>(r.quads + p->quad_region());
+        r.vscale = r.amax + p->nv;
+        r.vinv = r.vscale + p->nv;
+    }
+    return r;
+}
+}  // namespace
 
 namespace {
 
@@ -257,11 +283,6 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
         p->gemm_err.alloc(1, "GEMM status");
         cuda_check(cudaMemset(p->gemm_err.p, 0, sizeof(int)), "GEMM status reset");
     }
-    if (p->opts.storage == GCT_STORAGE_F16) {
-        p->vscale.alloc(p->nv, "plan view scales");
-        p->vinv.alloc(p->nv, "plan view scales");
-        p->amax.alloc(p->nv, "plan view maxima");
-    }
     // backprojection launch shape
     const bool vol3d = gct::is_2d_detector(kind);
     p->zpt = p->opts.z_per_thread > 0 ? p->opts.z_per_thread : (vol3d ? 8 : 1);
@@ -276,7 +297,8 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
 
 // Toeplitz-GEMM form of run_filter: split, tcgen05 GEMM into FP32 rows, then quads (or the rows
 // themselves for the plain output).
-void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, int mode, int vb, int vc, cudaStream_t s)
+void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float *vscale, int mode, int vb, int vc,
+                     cudaStream_t s)
 {
     const long long row0 = static_cast<long long>(vb) * p->nr, rows = static_cast<long long>(vc) * p->nr;
     gct::SplitArgs sa;
@@ -318,17 +340,19 @@ void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, int mode, in
     qa.nv = vc;
     qa.nr = p->nr;
     qa.nc = p->nc;
-    qa.vscale = (mode == gct::kOutQuadF16) ? p->vscale.p : nullptr;
+    qa.vscale = (mode == gct::kOutQuadF16) ? vscale : nullptr;
     qa.out = out;
     gct::launch_quads_from_rows(qa, mode, p->num_sms, s);
     cuda_check(cudaGetLastError(), "quad kernel launch");
 }
 
-void run_filter(gct_fdk_plan *p, const float *proj, void *out, int mode, int vb, int vc, cudaStream_t s)
+// `out` is the view-0 address of the output; `vscale` (FP16 quads only) the view-0 scales.
+void run_filter(gct_fdk_plan *p, const float *proj, void *out, const float *vscale, int mode, int vb, int vc,
+                cudaStream_t s)
 {
     if (vc <= 0) return;
     if (p->opts.filter == GCT_FILTER_TOEPLITZ_BF16X3) {
-        run_filter_gemm(p, proj, out, mode, vb, vc, s);
+        run_filter_gemm(p, proj, out, vscale, mode, vb, vc, s);
         return;
     }
     const long long pix = static_cast<long long>(p->nr) * p->nc;
@@ -351,20 +375,20 @@ void run_filter(gct_fdk_plan *p, const float *proj, void *out, int mode, int vb,
         const long long qview = static_cast<long long>(p->nr + 2 * gct::kQuadPad) * (p->nc + 2 * gct::kQuadPad);
         fa.out = static_cast<unsigned char *>(out) + vb * qview * static_cast<long long>(p->quad_bytes());
     }
-    fa.vscale = (mode == gct::kOutQuadF16) ? p->vscale.p + vb : nullptr;
+    fa.vscale = (mode == gct::kOutQuadF16) ? vscale + vb : nullptr;
     gct::launch_filter_fft(fa, static_cast<int>(p->L), p->num_sms, s);
     cuda_check(cudaGetLastError(), "filter kernel launch");
 }
 
-void run_backproject(gct_fdk_plan *p, const void *quads, float *vol, int v_begin, int v_count,
+void run_backproject(gct_fdk_plan *p, const StackRef &st, float *vol, int v_begin, int v_count,
                      bool accumulate, cudaStream_t s)
 {
     gct::BpArgs ba;
-    ba.quads = quads;
+    ba.quads = st.quads;
     ba.qpitch = p->nc + 2 * gct::kQuadPad;
     ba.qview = static_cast<long long>(p->nr + 2 * gct::kQuadPad) * ba.qpitch;
     ba.coefs = p->coefs.p;
-    ba.vinv = (p->opts.storage == GCT_STORAGE_F16) ? p->vinv.p : nullptr;
+    ba.vinv = st.vinv;
     ba.v_begin = v_begin;
     ba.v_count = v_count;
     ba.vol = vol;
@@ -392,27 +416,27 @@ void *plan_workspace(gct_fdk_plan *p, void *workspace)
     return p->work.p;
 }
 
-void prepare(gct_fdk_plan *p, const float *proj, void *ws, int vb, int vc, cudaStream_t s)
+void prepare(gct_fdk_plan *p, const float *proj, const StackRef &st, int vb, int vc, cudaStream_t s)
 {
     if (!proj) gct::fail(GCT_ERR_INVALID_ARG, "NULL projection pointer");
     if (vc <= 0) return;
     const bool f16 = p->opts.storage == GCT_STORAGE_F16;
     if (f16) {
         const long long pix = static_cast<long long>(p->nr) * p->nc;
-        cuda_check(cudaMemsetAsync(p->amax.p + vb, 0, sizeof(float) * vc, s), "view maxima reset");
-        gct::launch_view_absmax(proj + vb * pix, vc, pix, p->amax.p + vb, s);
-        gct::launch_view_scales(p->amax.p + vb, vc, p->l1, p->vscale.p + vb, p->vinv.p + vb, s);
+        cuda_check(cudaMemsetAsync(st.amax + vb, 0, sizeof(float) * vc, s), "view maxima reset");
+        gct::launch_view_absmax(proj + vb * pix, vc, pix, st.amax + vb, s);
+        gct::launch_view_scales(st.amax + vb, vc, p->l1, st.vscale + vb, st.vinv + vb, s);
         cuda_check(cudaGetLastError(), "view scale kernels");
     }
-    run_filter(p, proj, ws, f16 ? gct::kOutQuadF16 : gct::kOutQuadF32, vb, vc, s);
+    run_filter(p, proj, st.quads, st.vscale, f16 ? gct::kOutQuadF16 : gct::kOutQuadF32, vb, vc, s);
 }
 
 void execute(gct_fdk_plan *p, const float *proj, float *vol, void *workspace, cudaStream_t s)
 {
     if (!proj || !vol) gct::fail(GCT_ERR_INVALID_ARG, "NULL projection or volume pointer");
-    void *ws = plan_workspace(p, workspace);
-    prepare(p, proj, ws, 0, p->nv, s);
-    run_backproject(p, ws, vol, 0, p->nv, false, s);
+    const StackRef st = stack_of(p, plan_workspace(p, workspace));
+    prepare(p, proj, st, 0, p->nv, s);
+    run_backproject(p, st, vol, 0, p->nv, false, s);
 }
 
 void execute_host(gct_fdk_plan *p, const float *proj_host, float *vol_host, cudaStream_t s)
@@ -422,7 +446,7 @@ void execute_host(gct_fdk_plan *p, const float *proj_host, float *vol_host, cuda
     const size_t vol_n = static_cast<size_t>(p->vol.nx) * p->vol.ny * p->vol.nz;
     if (!p->host_proj.p) p->host_proj.alloc(pix * p->nv, "staging projections");
     if (!p->host_vol.p) p->host_vol.alloc(vol_n, "staging volume");
-    void *ws = plan_workspace(p, nullptr);
+    const StackRef st = stack_of(p, plan_workspace(p, nullptr));
     if (!p->copy_stream) cuda_check(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking), "copy stream");
     // about 8 chunks, at least 16 views each
     const int chunk = std::max(16, (p->nv + 7) / 8);
@@ -442,8 +466,8 @@ void execute_host(gct_fdk_plan *p, const float *proj_host, float *vol_host, cuda
                    "projection upload");
         cuda_check(cudaEventRecord(p->chunk_events[c], p->copy_stream), "event record");
         cuda_check(cudaStreamWaitEvent(s, p->chunk_events[c], 0), "stream wait");
-        prepare(p, p->host_proj.p, ws, vb, vc, s);
-        run_backproject(p, ws, p->host_vol.p, vb, vc, c > 0, s);
+        prepare(p, p->host_proj.p, st, vb, vc, s);
+        run_backproject(p, st, p->host_vol.p, vb, vc, c > 0, s);
     }
     cuda_check(cudaMemcpyAsync(vol_host, p->host_vol.p, sizeof(float) * vol_n, cudaMemcpyDeviceToHost, s),
                "volume download");
@@ -672,7 +696,8 @@ gct_status gct_fdk_filter(gct_fdk_plan *plan, const float *proj_dev, float *filt
     return guarded([&] {
         if (!plan || !proj_dev || !filtered_dev) gct::fail(GCT_ERR_INVALID_ARG, "NULL argument");
         DeviceGuard dg(plan->device);
-        run_filter(plan, proj_dev, filtered_dev, gct::kOutPlainF32, 0, plan->nv, static_cast<cudaStream_t>(stream));
+        run_filter(plan, proj_dev, filtered_dev, nullptr, gct::kOutPlainF32, 0, plan->nv,
+                   static_cast<cudaStream_t>(stream));
     });
 }
 
@@ -683,7 +708,7 @@ gct_status gct_fdk_prepare(gct_fdk_plan *plan, const float *proj_dev, void *work
         if (!plan) gct::fail(GCT_ERR_INVALID_ARG, "NULL plan");
         check_range(plan, view_begin, view_count);
         DeviceGuard dg(plan->device);
-        prepare(plan, proj_dev, plan_workspace(plan, workspace), static_cast<int>(view_begin),
+        prepare(plan, proj_dev, stack_of(plan, plan_workspace(plan, workspace)), static_cast<int>(view_begin),
                 static_cast<int>(view_count), static_cast<cudaStream_t>(stream));
     });
 }
@@ -695,9 +720,9 @@ gct_status gct_fdk_backproject(gct_fdk_plan *plan, const void *workspace, float 
         if (!plan || !vol_dev) gct::fail(GCT_ERR_INVALID_ARG, "NULL argument");
         check_range(plan, view_begin, view_count);
         DeviceGuard dg(plan->device);
-        const void *ws = workspace ? workspace : plan->work.p;
+        void *ws = workspace ? const_cast<void *>(workspace) : plan->work.p;
         if (!ws) gct::fail(GCT_ERR_INVALID_ARG, "no workspace: run gct_fdk_prepare first or pass one");
-        run_backproject(plan, ws, vol_dev, static_cast<int>(view_begin), static_cast<int>(view_count),
+        run_backproject(plan, stack_of(plan, ws), vol_dev, static_cast<int>(view_begin), static_cast<int>(view_count),
                         accumulate != 0, static_cast<cudaStream_t>(stream));
     });
 }
@@ -740,21 +765,34 @@ unsigned char *noalloc_scratch(int dev)
 void execute_noalloc(gct_fdk_plan *p, const float *proj, float *vol, cudaStream_t s)
 {
     if (!proj || !vol) gct::fail(GCT_ERR_INVALID_ARG, "NULL projection or volume pointer");
-    const size_t per_view =
-        static_cast<size_t>(p->nr + 2 * gct::kQuadPad) * (p->nc + 2 * gct::kQuadPad) * p->quad_bytes();
-    if (per_view > GCT_NOALLOC_SCRATCH_BYTES)
+    // per view: its quads and, for FP16 storage, three floats (maximum, scale, inverse scale)
+    const size_t quads_per_view = p->view_bytes();
+    const size_t scales_per_view = p->opts.storage == GCT_STORAGE_F16 ? 3 * sizeof(float) : 0;
+    const size_t per_view = quads_per_view + scales_per_view;
+    if (per_view + 256 > GCT_NOALLOC_SCRATCH_BYTES)
         gct::fail(GCT_ERR_BUDGET, "one view needs " + std::to_string(per_view) +
                                       " bytes of filtered-projection scratch; the allocation-free path holds " +
                                       std::to_string(GCT_NOALLOC_SCRATCH_BYTES) + " bytes");
-    const int chunk = static_cast<int>(std::min<size_t>(static_cast<size_t>(p->nv), GCT_NOALLOC_SCRATCH_BYTES / per_view));
+    const int chunk =
+        static_cast<int>(std::min<size_t>(static_cast<size_t>(p->nv), (GCT_NOALLOC_SCRATCH_BYTES - 256) / per_view));
     unsigned char *scratch = noalloc_scratch(p->device);
+    // the chunk's scales follow its quads, 256-byte aligned
+    float *scales = reinterpret_cast<float *>(
+        scratch + ((static_cast<size_t>(chunk) * quads_per_view + 255) & ~static_cast<size_t>(255)));
     for (int vb = 0; vb < p->nv; vb += chunk) {
         const int vc = std::min(chunk, p->nv - vb);
-        // prepare() and run_backproject() place view v at workspace + v * per_view; shifting the
-        // base by vb views puts this chunk at the start of the scratch.
-        void *ws = reinterpret_cast<void *>(reinterpret_cast<uintptr_t>(scratch) - static_cast<uintptr_t>(vb) * per_view);
-        prepare(p, proj, ws, vb, vc, s);
-        run_backproject(p, ws, vol, vb, vc, vb > 0, s);
+        // prepare() and run_backproject() address view v at view-0 bases; shifting every base by
+        // vb views puts this chunk at the start of its scratch region.
+        StackRef st;
+        st.quads = reinterpret_cast<unsigned char *>(reinterpret_cast<uintptr_t>(scratch) -
+                                                     static_cast<uintptr_t>(vb) * quads_per_view);
+        if (scales_per_view) {
+            st.amax = scales - vb;
+            st.vscale = scales + chunk - vb;
+            st.vinv = scales + 2 * chunk - vb;
+        }
+        prepare(p, proj, st, vb, vc, s);
+        run_backproject(p, st, vol, vb, vc, vb > 0, s);
     }
 }
 }  // namespace

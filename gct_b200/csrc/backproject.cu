@@ -25,7 +25,7 @@
 namespace gct {
 namespace {
 
-constexpr int kViewsPerChunk = 128;
+constexpr int kViewsPerChunk = 32;  // 2.5 KB of coefficients per block leaves L1 to the gathers
 constexpr int kC = kCoefPerView;
 constexpr float kShift = 12582912.0f;  // 1.5 * 2^23
 constexpr int kShiftBits = 0x4B400000;  // bit pattern of kShift
@@ -141,27 +141,26 @@ __device__ __forceinline__ float sample(const typename L::S *view, int qpitch, f
     return L::lerp(__ldg(view + (iv + kQuadPad) * qpitch + iu + kQuadPad), L::ucol(fu), fvc);
 }
 
+// Backprojects views [a.v_begin, a.v_begin + a.v_count) into the column segment (i, j, k0 ..
+// k0 + ZPT - 1) of the calling thread, staging VPS views of coefficients at a time in s_coef.
+// Every thread of the block calls it (it holds block barriers); inactive threads only help to
+// stage. mode: kStore writes the sums, kAccumulate adds them to the volume, kAtomic adds them
+// with atomics (several blocks share the voxels).
 template <int FAMILY, class Q, int ZPT, bool ZAFFINE>
-__global__ void __launch_bounds__(256) bp_kernel(BpArgs a)
+__device__ __forceinline__ void bp_column(const BpArgs &a, int i, int j, int k0, bool active, int vps,
+                                          float4 *s_coef, int tid, int nthr, int mode)
 {
     using L = typename LerpOf<Q>::type;
     using S = typename L::S;
-    __shared__ float4 s_coef[kViewsPerChunk * kC / 4];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k0 = blockIdx.z * ZPT;
-    const bool active = i < a.nx && j < a.ny;
     const float fi = static_cast<float>(i), fj = static_cast<float>(j), fk0 = static_cast<float>(k0);
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    const int nthr = blockDim.x * blockDim.y;
     const S *quads = static_cast<const S *>(a.quads);
 
     float acc[ZPT];
 #pragma unroll
     for (int z = 0; z < ZPT; ++z) acc[z] = 0.f;
 
-    for (int vc = 0; vc < a.v_count; vc += kViewsPerChunk) {
-        const int nvc = min(kViewsPerChunk, a.v_count - vc);
+    for (int vc = 0; vc < a.v_count; vc += vps) {
+        const int nvc = min(vps, a.v_count - vc);
         __syncthreads();
         const float4 *g = reinterpret_cast<const float4 *>(a.coefs + static_cast<long long>(a.v_begin + vc) * kC);
         for (int t = tid; t < nvc * kC / 4; t += nthr) s_coef[t] = __ldg(g + t);
@@ -231,10 +230,22 @@ __global__ void __launch_bounds__(256) bp_kernel(BpArgs a)
     for (int z = 0; z < ZPT; ++z) {
         const int k = k0 + z;
         if (k < a.nz) {
-            const long long idx = (static_cast<long long>(k) * a.ny + j) * a.nx + i;
-            a.vol[idx] = a.accumulate ? a.vol[idx] + acc[z] : acc[z];
+            float *dst = a.vol + (static_cast<long long>(k) * a.ny + j) * a.nx + i;
+            if (mode == kBpAtomic) atomicAdd(dst, acc[z]);
+            else *dst = mode == kBpAccumulate ? *dst + acc[z] : acc[z];
         }
     }
+}
+
+template <int FAMILY, class Q, int ZPT, bool ZAFFINE>
+__global__ void __launch_bounds__(256) bp_kernel(BpArgs a)
+{
+    __shared__ float4 s_coef[kViewsPerChunk * kC / 4];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    bp_column<FAMILY, Q, ZPT, ZAFFINE>(a, i, j, blockIdx.z * ZPT, i < a.nx && j < a.ny, kViewsPerChunk, s_coef,
+                                       threadIdx.y * blockDim.x + threadIdx.x, blockDim.x * blockDim.y,
+                                       a.accumulate ? kBpAccumulate : kBpStore);
 }
 
 template <int FAMILY, class Q, int ZPT>
@@ -260,7 +271,88 @@ void launch_q(const BpArgs &a, bool z_affine, int zpt, int bx, int by, cudaStrea
     }
 }
 
+// ---- work-queue backprojection -----------------------------------------------------------
+
+template <int FAMILY, class Q, int ZPT>
+__device__ __forceinline__ void queue_tile_z(const BpItem &it, const BpArgs &a, int i, int j, int k0, bool active,
+                                             int vps, float4 *s_coef, int tid, int mode)
+{
+    if (FAMILY == 0 || it.z_affine)
+        bp_column<FAMILY, Q, ZPT, true>(a, i, j, k0, active, vps, s_coef, tid, kQueueThreads, mode);
+    else
+        bp_column<FAMILY, Q, ZPT, false>(a, i, j, k0, active, vps, s_coef, tid, kQueueThreads, mode);
+}
+
+template <int FAMILY, class Q>
+__device__ __forceinline__ void queue_tile(const BpItem &it, const BpArgs &a, int i, int j, int tz, bool active,
+                                           int vps, float4 *s_coef, int tid, int mode)
+{
+    switch (it.zpt) {
+        case 1: queue_tile_z<FAMILY, Q, 1>(it, a, i, j, tz, active, vps, s_coef, tid, mode); break;
+        case 4: queue_tile_z<FAMILY, Q, 4>(it, a, i, j, tz * 4, active, vps, s_coef, tid, mode); break;
+        case 8: queue_tile_z<FAMILY, Q, 8>(it, a, i, j, tz * 8, active, vps, s_coef, tid, mode); break;
+        default: queue_tile_z<FAMILY, Q, 16>(it, a, i, j, tz * 16, active, vps, s_coef, tid, mode); break;
+    }
+}
+
+// Persistent blocks take work entries in queue order from a global counter; each entry is one
+// tile of one reconstruction over a range of views. The item descriptor is read once per entry
+// into shared memory; all control flow below depends only on it, so it is uniform per block.
+template <class Q>
+__global__ void __launch_bounds__(kQueueThreads) bp_queue_kernel(const BpItem *__restrict__ items,
+                                                                 const BpWork *__restrict__ work, int n_work,
+                                                                 int *counter, int vps)
+{
+    __shared__ float4 s_coef[kQueueMaxVps * kC / 4];
+    __shared__ BpItem s_item;
+    __shared__ BpWork s_work;
+    __shared__ int s_next;
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) s_next = atomicAdd(counter, 1);
+        __syncthreads();
+        const int w = s_next;
+        if (w >= n_work) return;
+        if (tid == 0) {
+            s_work = work[w];
+            s_item = items[s_work.item];
+        }
+        __syncthreads();
+        const BpItem &it = s_item;
+        BpArgs a = it.a;
+        a.v_begin = s_work.v_begin;
+        a.v_count = s_work.v_count;
+        const int mode = s_work.mode;
+        const int t = s_work.tile;
+        const int tx = t % it.tiles_x, ty = (t / it.tiles_x) % it.tiles_y, tz = t / (it.tiles_x * it.tiles_y);
+        const int i = tx * it.bx + tid % it.bx, j = ty * it.by + tid / it.bx;
+        const bool active = i < a.nx && j < a.ny;
+        if (it.family == 0) queue_tile<0, Q>(it, a, i, j, tz, active, vps, s_coef, tid, mode);
+        else if (it.family == 1) queue_tile<1, Q>(it, a, i, j, tz, active, vps, s_coef, tid, mode);
+        else queue_tile<2, Q>(it, a, i, j, tz, active, vps, s_coef, tid, mode);
+        __syncthreads();  // s_item / s_work / s_next are rewritten for the next entry
+    }
+}
+
 }  // namespace
+
+int queue_blocks_per_sm(int storage)
+{
+    int n = 0;
+    const cudaError_t e = storage == 0
+        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bp_queue_kernel<QuadF32>, kQueueThreads, 0)
+        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bp_queue_kernel<QuadF16>, kQueueThreads, 0);
+    return e == cudaSuccess ? n : 0;
+}
+
+void launch_backproject_queue(const BpItem *items, const BpWork *work, int n_work, int *counter, int storage,
+                              int vps, int grid, cudaStream_t s)
+{
+    if (storage == 0)
+        bp_queue_kernel<QuadF32><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter, vps);
+    else
+        bp_queue_kernel<QuadF16><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter, vps);
+}
 
 void launch_backproject(const BpArgs &a, int family, int storage, bool z_affine, int zpt, int bx,
                         int by, cudaStream_t s)

@@ -284,58 +284,68 @@ __global__ void __launch_bounds__(192, 1)
 }
 
 // Cosine x Parker weighting and BF16 hi/lo split of rows [row0, row0 + rows) into [rows][Kp].
+// One warp per row (per-row view/row indices and geometry), two columns per lane step stored as
+// one bf16x2 word.
 __global__ void split_kernel(SplitArgs a)
 {
-    const long long total = static_cast<long long>(a.rows) * a.Kp;
-    for (long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
-         idx += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const int k = static_cast<int>(idx % a.Kp);
-        const long long rl = idx / a.Kp;
+    const int lane = threadIdx.x & 31;
+    const long long warp0 = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
+    for (long long rl = warp0; rl < a.rows; rl += nwarps) {
         const long long row = a.row0 + rl;
-        float x = 0.f;
-        if (k < a.nc) {
-            const int v = static_cast<int>(row / a.nr), r = static_cast<int>(row - static_cast<long long>(v) * a.nr);
-            const float4 gv = __ldg(&a.fview[v]);
-            x = __ldg(a.proj + row * a.nc + k) * __ldg(a.parker + static_cast<long long>(v) * a.nc + k) *
-                cos_weight_dev(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k, r);
+        const int v = static_cast<int>(row / a.nr), r = static_cast<int>(row - static_cast<long long>(v) * a.nr);
+        const float4 gv = __ldg(&a.fview[v]);
+        const float *src = a.proj + row * a.nc;
+        const float *pk = a.parker + static_cast<long long>(v) * a.nc;
+        __nv_bfloat162 *dh = reinterpret_cast<__nv_bfloat162 *>(a.xh + row * a.Kp);
+        __nv_bfloat162 *dl = reinterpret_cast<__nv_bfloat162 *>(a.xl + row * a.Kp);
+        for (int k2 = lane; k2 < a.Kp / 2; k2 += 32) {
+            float x[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int k = 2 * k2 + h;
+                x[h] = (k < a.nc) ? __ldg(src + k) * __ldg(pk + k) * cos_weight_dev(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k, r)
+                                  : 0.f;
+            }
+            const __nv_bfloat162 hi = __floats2bfloat162_rn(x[0], x[1]);
+            const float2 hf = __bfloat1622float2(hi);
+            dh[k2] = hi;
+            dl[k2] = __floats2bfloat162_rn(x[0] - hf.x, x[1] - hf.y);
         }
-        const __nv_bfloat16 h = __float2bfloat16_rn(x);
-        const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
-        a.xh[row * a.Kp + k] = h;
-        a.xl[row * a.Kp + k] = l;
     }
 }
 
-// Filtered rows Y (row stride ldy) of views [v0, v0 + nv) -> bilinear-coefficient quads.
+// Filtered rows Y (row stride ldy) of views [v0, v0 + nv) -> bilinear-coefficient quads. One
+// block per quad row (view, padded row), threads along the columns.
 template <int MODE>
 __global__ void quads_from_rows_kernel(QuadArgs a)
 {
     const int qpitch = a.nc + 2 * kQuadPad, qrows = a.nr + 2 * kQuadPad;
-    const long long per_view = static_cast<long long>(qpitch) * qrows;
-    const long long total = per_view * a.nv;
-    for (long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
-         idx += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const int vl = static_cast<int>(idx / per_view);
-        const long long rem = idx - static_cast<long long>(vl) * per_view;
-        const int r = static_cast<int>(rem / qpitch) - kQuadPad, c = static_cast<int>(rem % qpitch) - kQuadPad;
+    const long long nrows = static_cast<long long>(a.nv) * qrows;
+    for (long long qr = blockIdx.x; qr < nrows; qr += gridDim.x) {
+        const int vl = static_cast<int>(qr / qrows);
+        const int r = static_cast<int>(qr - static_cast<long long>(vl) * qrows) - kQuadPad;
         const int v = a.v0 + vl;
         const float sc = a.vscale ? a.vscale[v] : 1.0f;
-        auto y = [&](int rr, int cc) -> float {
-            if (rr < 0 || rr >= a.nr || cc < 0 || cc >= a.nc) return 0.f;
-            return sc * a.Y[(static_cast<long long>(vl) * a.nr + rr) * a.ldy + cc];
-        };
-        const float p00 = y(r, c), p01 = y(r, c + 1), p10 = y(r + 1, c), p11 = y(r + 1, c + 1);
-        const float l = p00 + p10, rt = p01 + p11;
-        const float A = 0.5f * l, B = 0.5f * (rt - l), Cc = p10 - p00, D = (p11 - p01) - (p10 - p00);
-        const long long qidx = static_cast<long long>(v) * per_view + rem;
-        if (MODE == kOutQuadF32) {
-            static_cast<float4 *>(a.out)[qidx] = make_float4(A, B, Cc, D);
-        } else {
-            const __half2 lo = __floats2half2_rn(A, Cc), hi = __floats2half2_rn(B, D);
-            uint2 u;
-            u.x = *reinterpret_cast<const unsigned *>(&lo);
-            u.y = *reinterpret_cast<const unsigned *>(&hi);
-            static_cast<uint2 *>(a.out)[qidx] = u;
+        const float *top = (r >= 0 && r < a.nr) ? a.Y + (static_cast<long long>(vl) * a.nr + r) * a.ldy : nullptr;
+        const float *bot = (r + 1 >= 0 && r + 1 < a.nr) ? a.Y + (static_cast<long long>(vl) * a.nr + r + 1) * a.ldy : nullptr;
+        const long long qbase = (static_cast<long long>(v) * qrows + (r + kQuadPad)) * qpitch;
+        for (int cq = threadIdx.x; cq < qpitch; cq += blockDim.x) {
+            const int c = cq - kQuadPad;
+            const bool c0 = c >= 0 && c < a.nc, c1 = c + 1 >= 0 && c + 1 < a.nc;
+            const float p00 = (top && c0) ? sc * __ldg(top + c) : 0.f, p01 = (top && c1) ? sc * __ldg(top + c + 1) : 0.f;
+            const float p10 = (bot && c0) ? sc * __ldg(bot + c) : 0.f, p11 = (bot && c1) ? sc * __ldg(bot + c + 1) : 0.f;
+            const float l = p00 + p10, rt = p01 + p11;
+            const float A = 0.5f * l, B = 0.5f * (rt - l), Cc = p10 - p00, D = (p11 - p01) - (p10 - p00);
+            if (MODE == kOutQuadF32) {
+                static_cast<float4 *>(a.out)[qbase + cq] = make_float4(A, B, Cc, D);
+            } else {
+                const __half2 lo = __floats2half2_rn(A, Cc), hi = __floats2half2_rn(B, D);
+                uint2 u;
+                u.x = *reinterpret_cast<const unsigned *>(&lo);
+                u.y = *reinterpret_cast<const unsigned *>(&hi);
+                static_cast<uint2 *>(a.out)[qbase + cq] = u;
+            }
         }
     }
 }
@@ -375,16 +385,14 @@ size_t toeplitz_gemm_smem_bytes() { return STAGES * STAGE_BYTES + 1024 + 256; }
 
 void launch_split(const SplitArgs &a, int num_sms, cudaStream_t s)
 {
-    long long total = static_cast<long long>(a.rows) * a.Kp;
-    long long grid = (total + 255) / 256;
-    if (grid > static_cast<long long>(num_sms) * 32) grid = static_cast<long long>(num_sms) * 32;
+    long long grid = (a.rows + 7) / 8;  // 8 warps (rows) per block
+    if (grid > static_cast<long long>(num_sms) * 16) grid = static_cast<long long>(num_sms) * 16;
     split_kernel<<<static_cast<unsigned>(grid < 1 ? 1 : grid), 256, 0, s>>>(a);
 }
 
 void launch_quads_from_rows(const QuadArgs &a, int mode, int num_sms, cudaStream_t s)
 {
-    const long long total = static_cast<long long>(a.nv) * (a.nr + 2 * kQuadPad) * (a.nc + 2 * kQuadPad);
-    long long grid = (total + 255) / 256;
+    long long grid = static_cast<long long>(a.nv) * (a.nr + 2 * kQuadPad);
     if (grid > static_cast<long long>(num_sms) * 32) grid = static_cast<long long>(num_sms) * 32;
     if (mode == kOutQuadF32)
         quads_from_rows_kernel<kOutQuadF32><<<static_cast<unsigned>(grid < 1 ? 1 : grid), 256, 0, s>>>(a);

@@ -55,4 +55,32 @@ struct BpArgs {
 void launch_backproject(const BpArgs &a, int family, int storage, bool z_affine, int zpt,
                         int bx, int by, cudaStream_t s);
 
+// How a block writes its sums: overwrite, add (views processed in order by successive launches)
+// or add atomically (several blocks of one launch share the voxels; the volume starts at zero).
+enum BpMode : int { kBpStore = 0, kBpAccumulate = 1, kBpAtomic = 2 };
+
+// Work-queue backprojection: one persistent launch over the tiles of many reconstructions.
+// A tile is the bx x by x zpt voxel box of one block (bx * by = 256 threads).
+struct BpItem {
+    BpArgs a;                  // v_begin / v_count / accumulate are taken from the work entry
+    int family = 0, z_affine = 1, zpt = 8, bx = 8, by = 32;
+    int tiles_x = 0, tiles_y = 0, tiles_z = 0;
+};
+struct BpWork {
+    int item = 0;              // index into the item array
+    int tile = 0;              // x fastest, then y, then z
+    int v_begin = 0, v_count = 0;
+    int mode = kBpStore;
+};
+constexpr int kQueueThreads = 256;
+constexpr int kQueueMaxVps = 64;   // views of coefficients staged per block barrier, at most
+// Supported z-per-thread values of the queue kernel.
+inline bool queue_zpt_ok(int zpt) { return zpt == 1 || zpt == 4 || zpt == 8 || zpt == 16; }
+// Blocks of the queue kernel resident per SM for the storage type (0 f32, 1 f16).
+int queue_blocks_per_sm(int storage);
+// Launches grid blocks that take work entries [0, n_work) in order from *counter (zeroed by the
+// caller before the launch) until none are left.
+void launch_backproject_queue(const BpItem *items, const BpWork *work, int n_work, int *counter, int storage,
+                              int vps, int grid, cudaStream_t s);
+
 }  // namespace gct

@@ -226,7 +226,10 @@ gct_status gct_fdk_plan_destroy(gct_fdk_plan *plan);
  * GCT_ERR_TIMEOUT if a bounded pipeline wait of the Toeplitz-GEMM filter ran out. */
 gct_status gct_fdk_plan_check(gct_fdk_plan *plan);
 
-/* Device bytes of scratch that gct_fdk_execute needs (the filtered-projection stack). */
+/* Device bytes of scratch that gct_fdk_execute needs: the filtered-projection stack and, for
+ * FP16 storage, its per-view scales. A workspace carries everything the backprojection of one
+ * prepared stack reads, so several stacks prepared with one plan into separate workspaces stay
+ * independent. */
 gct_status gct_fdk_plan_workspace_bytes(const gct_fdk_plan *plan, uint64_t *bytes);
 
 /* Full FDK on device buffers, asynchronous on `stream`: fused cosine + Parker weighting and
