@@ -11,9 +11,10 @@
 // column u, its bilinear split, the weight (projective and parallel kinds) and the row coordinate
 // v(z) = v0 + z * vs are set up once. Each voxel then costs one FMA for v, a magic-number floor
 // split, one IMAD.WIDE address, one 8- or 16-byte load of a bilinear-coefficient quad, two FMAs
-// (one HFMA2 plus one FMA for FP16 storage) and the accumulate. A column segment whose rows all fall outside
-// the detector contributes exactly zero (the reference's texture border) and is skipped; one that
-// lies fully on the detector runs without per-voxel clamps.
+// (one HFMA2 plus one FMA for FP16 storage) and the accumulate; pairs of voxels share packed
+// FP32x2 instructions for the row split and the accumulate. A column segment whose rows all fall
+// outside the detector contributes exactly zero (the reference's texture border) and is skipped;
+// one that lies fully on the detector runs without per-voxel clamps.
 //
 // Mappings follow projMapping (src/cuda/geom/coord_trans_proj.cuh:157-345) through per-view
 // coefficients in voxel-index space that the host derives in FP64.
@@ -91,15 +92,41 @@ template <class L, int ZPT, bool CLAMP, class W>
 __device__ __forceinline__ void column(unsigned long long base, int stride, typename L::U fu, float vm0, float vs,
                                        float vmax, const W &wt, float (&acc)[ZPT])
 {
+    if constexpr (ZPT % 2 == 0) {
+        // voxel pairs (z, z + 1): the row split and the accumulate run as packed FP32x2
+        // operations (sm_100 FFMA2 / FADD2), element for element the same roundings as below
+        const float2 shift = make_float2(kShift, kShift), mshift = make_float2(-kShift, -kShift);
+        const float2 vs2 = make_float2(vs, vs), vm02 = make_float2(vm0, vm0);
 #pragma unroll
-    for (int z = 0; z < ZPT; ++z) {
-        float vm = fmaf(vs, static_cast<float>(z), vm0);
-        if (CLAMP) vm = fminf(fmaxf(vm, -1.5f), vmax - 0.5f);
-        const float t = vm + kShift;
-        const float fvc = vm - (t - kShift);
-        const auto *p = reinterpret_cast<const typename L::S *>(
-            base + static_cast<unsigned long long>(static_cast<long long>(__float_as_int(t)) * stride));
-        acc[z] = fmaf(wt.at(z), L::lerp(__ldg(p), fu, fvc), acc[z]);
+        for (int z = 0; z < ZPT; z += 2) {
+            float2 vm = __ffma2_rn(vs2, make_float2(static_cast<float>(z), static_cast<float>(z + 1)), vm02);
+            if (CLAMP) {
+                vm.x = fminf(fmaxf(vm.x, -1.5f), vmax - 0.5f);
+                vm.y = fminf(fmaxf(vm.y, -1.5f), vmax - 0.5f);
+            }
+            const float2 t = __fadd2_rn(vm, shift);
+            const float2 fl = __fadd2_rn(t, mshift);
+            const float2 fvc = __ffma2_rn(fl, make_float2(-1.0f, -1.0f), vm);  // vm - fl, exact
+            const auto *p0 = reinterpret_cast<const typename L::S *>(
+                base + static_cast<unsigned long long>(static_cast<long long>(__float_as_int(t.x)) * stride));
+            const auto *p1 = reinterpret_cast<const typename L::S *>(
+                base + static_cast<unsigned long long>(static_cast<long long>(__float_as_int(t.y)) * stride));
+            const float2 val = make_float2(L::lerp(__ldg(p0), fu, fvc.x), L::lerp(__ldg(p1), fu, fvc.y));
+            const float2 r = __ffma2_rn(make_float2(wt.at(z), wt.at(z + 1)), val, make_float2(acc[z], acc[z + 1]));
+            acc[z] = r.x;
+            acc[z + 1] = r.y;
+        }
+    } else {
+#pragma unroll
+        for (int z = 0; z < ZPT; ++z) {
+            float vm = fmaf(vs, static_cast<float>(z), vm0);
+            if (CLAMP) vm = fminf(fmaxf(vm, -1.5f), vmax - 0.5f);
+            const float t = vm + kShift;
+            const float fvc = vm - (t - kShift);
+            const auto *p = reinterpret_cast<const typename L::S *>(
+                base + static_cast<unsigned long long>(static_cast<long long>(__float_as_int(t)) * stride));
+            acc[z] = fmaf(wt.at(z), L::lerp(__ldg(p), fu, fvc), acc[z]);
+        }
     }
 }
 
@@ -290,8 +317,7 @@ __device__ __forceinline__ void queue_tile(const BpItem &it, const BpArgs &a, in
     switch (it.zpt) {
         case 1: queue_tile_z<FAMILY, Q, 1>(it, a, i, j, tz, active, vps, s_coef, tid, mode); break;
         case 4: queue_tile_z<FAMILY, Q, 4>(it, a, i, j, tz * 4, active, vps, s_coef, tid, mode); break;
-        case 8: queue_tile_z<FAMILY, Q, 8>(it, a, i, j, tz * 8, active, vps, s_coef, tid, mode); break;
-        default: queue_tile_z<FAMILY, Q, 16>(it, a, i, j, tz * 16, active, vps, s_coef, tid, mode); break;
+        default: queue_tile_z<FAMILY, Q, 8>(it, a, i, j, tz * 8, active, vps, s_coef, tid, mode); break;
     }
 }
 
@@ -299,9 +325,9 @@ __device__ __forceinline__ void queue_tile(const BpItem &it, const BpArgs &a, in
 // tile of one reconstruction over a range of views. The item descriptor is read once per entry
 // into shared memory; all control flow below depends only on it, so it is uniform per block.
 template <class Q>
-__global__ void __launch_bounds__(kQueueThreads) bp_queue_kernel(const BpItem *__restrict__ items,
+__global__ void __launch_bounds__(kQueueThreads, kQueueMinBlocks) bp_queue_kernel(const BpItem *__restrict__ items,
                                                                  const BpWork *__restrict__ work, int n_work,
-                                                                 int *counter, int vps)
+                                                                 int *counter)
 {
     __shared__ float4 s_coef[kQueueMaxVps * kC / 4];
     __shared__ BpItem s_item;
@@ -323,6 +349,7 @@ __global__ void __launch_bounds__(kQueueThreads) bp_queue_kernel(const BpItem *_
         a.v_begin = s_work.v_begin;
         a.v_count = s_work.v_count;
         const int mode = s_work.mode;
+        const int vps = it.vps;
         const int t = s_work.tile;
         const int tx = t % it.tiles_x, ty = (t / it.tiles_x) % it.tiles_y, tz = t / (it.tiles_x * it.tiles_y);
         const int i = tx * it.bx + tid % it.bx, j = ty * it.by + tid / it.bx;
@@ -346,12 +373,12 @@ int queue_blocks_per_sm(int storage)
 }
 
 void launch_backproject_queue(const BpItem *items, const BpWork *work, int n_work, int *counter, int storage,
-                              int vps, int grid, cudaStream_t s)
+                              int grid, cudaStream_t s)
 {
     if (storage == 0)
-        bp_queue_kernel<QuadF32><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter, vps);
+        bp_queue_kernel<QuadF32><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter);
     else
-        bp_queue_kernel<QuadF16><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter, vps);
+        bp_queue_kernel<QuadF16><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter);
 }
 
 void launch_backproject(const BpArgs &a, int family, int storage, bool z_affine, int zpt, int bx,

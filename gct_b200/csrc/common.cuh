@@ -17,23 +17,35 @@ namespace gct {
 // border-0 texture addressing (src/cuda/data/nd_array_texture.cuh:33-56) without branches.
 // The padding width is kQuadPad (kernels.hpp).
 
+// Storage tags of the backprojector: FP32 quads (float4, quad_f32) and FP16 quads (uint2, quad_f16).
 struct QuadF32 {
     using storage = float4;
-    static __device__ __forceinline__ float4 load(const float4 *p) { return __ldg(p); }
-    static __device__ __forceinline__ float4 unpack(float4 q) { return q; }
+};
+struct QuadF16 {
+    using storage = uint2;
 };
 
-struct QuadF16 {
-    using storage = uint2;  // four halves: (p00, p01) in .x, (p10, p11) in .y
-    static __device__ __forceinline__ uint2 load(const uint2 *p) { return __ldg(p); }
-    static __device__ __forceinline__ float4 unpack(uint2 q)
-    {
-        __half2 lo = *reinterpret_cast<__half2 *>(&q.x);
-        __half2 hi = *reinterpret_cast<__half2 *>(&q.y);
-        const float2 a = __half22float2(lo), b = __half22float2(hi);
-        return make_float4(a.x, a.y, b.x, b.y);
-    }
-};
+// Quad of taps p00 = p[r][c], p01 = p[r][c+1], p10 = p[r+1][c], p11 = p[r+1][c+1] in the centred
+// form: value = (A + fu B) + fc (C + fu D) with fu in [0, 1] and fc = f - 1/2 in [-1/2, 1/2]:
+//   A = (p00 + p10) / 2, B = (p01 + p11 - p00 - p10) / 2, C = p10 - p00, D = p11 - p01 - p10 + p00.
+// The centred fraction keeps the FP16 products small: emulated on ramp-filtered noisy rows, an
+// offset form (fraction in [1, 2), one operation fewer per sample) had three times the FP16 error.
+__device__ __forceinline__ float4 quad_f32(float p00, float p01, float p10, float p11)
+{
+    const float l = p00 + p10, r = p01 + p11;
+    return make_float4(0.5f * l, 0.5f * (r - l), p10 - p00, (p11 - p01) - (p10 - p00));
+}
+
+// FP16 storage of the same quad: half2 (A, C) in .x and half2 (B, D) in .y.
+__device__ __forceinline__ uint2 quad_f16(float p00, float p01, float p10, float p11)
+{
+    const float4 q = quad_f32(p00, p01, p10, p11);
+    const __half2 lo = __floats2half2_rn(q.x, q.z), hi = __floats2half2_rn(q.y, q.w);
+    uint2 u;
+    u.x = *reinterpret_cast<const unsigned *>(&lo);
+    u.y = *reinterpret_cast<const unsigned *>(&hi);
+    return u;
+}
 
 // floor(x) and x - floor(x) for |x| < 2^22 with three FP32 adds and one integer subtract:
 // round-half-even of (x - 0.5) via the 1.5 * 2^23 shifter. For an integer x the split may

@@ -133,29 +133,14 @@ __device__ __forceinline__ void first_stage_smem(const float2 *src, float2 *dst,
     stage_r4<L, NT, false>(src, dst, nullptr, nullptr, 1, tid);
 }
 
-// Bilinear-coefficient quad of rows (top, bot) at column c: with fu in [0, 1] and the centred row
-// fraction fv' in [-0.5, 0.5], the bilinear value is (A + fu B) + fv' (C + fu D).
-struct QuadCoef {
-    float A, B, C, D;
-};
-__device__ __forceinline__ QuadCoef quad_coef(float p00, float p01, float p10, float p11)
-{
-    const float l = p00 + p10, r = p01 + p11;
-    return {0.5f * l, 0.5f * (r - l), p10 - p00, (p11 - p01) - (p10 - p00)};
-}
-
+// Quad of rows (top, bot) at column c in the storage form of MODE (quad_f32 / quad_f16).
 template <int MODE>
-__device__ __forceinline__ void store_quad(void *out, long long qidx, QuadCoef q)
+__device__ __forceinline__ void store_quad(void *out, long long qidx, float p00, float p01, float p10, float p11)
 {
-    if (MODE == kOutQuadF32) {
-        static_cast<float4 *>(out)[qidx] = make_float4(q.A, q.B, q.C, q.D);
-    } else {
-        const __half2 lo = __floats2half2_rn(q.A, q.C), hi = __floats2half2_rn(q.B, q.D);
-        uint2 u;
-        u.x = *reinterpret_cast<const unsigned *>(&lo);
-        u.y = *reinterpret_cast<const unsigned *>(&hi);
-        static_cast<uint2 *>(out)[qidx] = u;
-    }
+    if (MODE == kOutQuadF32)
+        static_cast<float4 *>(out)[qidx] = quad_f32(p00, p01, p10, p11);
+    else
+        static_cast<uint2 *>(out)[qidx] = quad_f16(p00, p01, p10, p11);
 }
 
 // Writes quad row `r` (detector row r, padded index r + kQuadPad) of view v from the filtered
@@ -176,7 +161,7 @@ __device__ __forceinline__ void write_quad_row(const FilterArgs &a, int v, int r
     };
     for (int cq = tid; cq < qpitch; cq += nthr) {
         const int c = cq - kQuadPad;
-        store_quad<MODE>(a.out, row0 + cq, quad_coef(tv(c), tv(c + 1), bv(c), bv(c + 1)));
+        store_quad<MODE>(a.out, row0 + cq, tv(c), tv(c + 1), bv(c), bv(c + 1));
     }
 }
 

@@ -335,17 +335,10 @@ __global__ void quads_from_rows_kernel(QuadArgs a)
             const bool c0 = c >= 0 && c < a.nc, c1 = c + 1 >= 0 && c + 1 < a.nc;
             const float p00 = (top && c0) ? sc * __ldg(top + c) : 0.f, p01 = (top && c1) ? sc * __ldg(top + c + 1) : 0.f;
             const float p10 = (bot && c0) ? sc * __ldg(bot + c) : 0.f, p11 = (bot && c1) ? sc * __ldg(bot + c + 1) : 0.f;
-            const float l = p00 + p10, rt = p01 + p11;
-            const float A = 0.5f * l, B = 0.5f * (rt - l), Cc = p10 - p00, D = (p11 - p01) - (p10 - p00);
-            if (MODE == kOutQuadF32) {
-                static_cast<float4 *>(a.out)[qbase + cq] = make_float4(A, B, Cc, D);
-            } else {
-                const __half2 lo = __floats2half2_rn(A, Cc), hi = __floats2half2_rn(B, D);
-                uint2 u;
-                u.x = *reinterpret_cast<const unsigned *>(&lo);
-                u.y = *reinterpret_cast<const unsigned *>(&hi);
-                static_cast<uint2 *>(a.out)[qbase + cq] = u;
-            }
+            if (MODE == kOutQuadF32)
+                static_cast<float4 *>(a.out)[qbase + cq] = quad_f32(p00, p01, p10, p11);
+            else
+                static_cast<uint2 *>(a.out)[qbase + cq] = quad_f16(p00, p01, p10, p11);
         }
     }
 }

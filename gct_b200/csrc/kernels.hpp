@@ -64,6 +64,7 @@ enum BpMode : int { kBpStore = 0, kBpAccumulate = 1, kBpAtomic = 2 };
 struct BpItem {
     BpArgs a;                  // v_begin / v_count / accumulate are taken from the work entry
     int family = 0, z_affine = 1, zpt = 8, bx = 8, by = 32;
+    int vps = 32;              // views of coefficients staged per block barrier (<= kQueueMaxVps)
     int tiles_x = 0, tiles_y = 0, tiles_z = 0;
 };
 struct BpWork {
@@ -73,14 +74,15 @@ struct BpWork {
     int mode = kBpStore;
 };
 constexpr int kQueueThreads = 256;
-constexpr int kQueueMaxVps = 64;   // views of coefficients staged per block barrier, at most
+constexpr int kQueueMinBlocks = 3;  // resident blocks per SM the register budget is sized for
+constexpr int kQueueMaxVps = 64;    // views of coefficients staged per block barrier, at most
 // Supported z-per-thread values of the queue kernel.
-inline bool queue_zpt_ok(int zpt) { return zpt == 1 || zpt == 4 || zpt == 8 || zpt == 16; }
+inline bool queue_zpt_ok(int zpt) { return zpt == 1 || zpt == 4 || zpt == 8; }
 // Blocks of the queue kernel resident per SM for the storage type (0 f32, 1 f16).
 int queue_blocks_per_sm(int storage);
 // Launches grid blocks that take work entries [0, n_work) in order from *counter (zeroed by the
 // caller before the launch) until none are left.
 void launch_backproject_queue(const BpItem *items, const BpWork *work, int n_work, int *counter, int storage,
-                              int vps, int grid, cudaStream_t s);
+                              int grid, cudaStream_t s);
 
 }  // namespace gct

@@ -1,0 +1,160 @@
+// Internal host interface of the FDK engine: the plan, device buffers, error plumbing and the
+// stage functions shared by the C ABI (abi.cu), the batch engine (batch.cu) and the serving loop
+// (server.cu). Not part of the public ABI.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/gct_fdk.h"
+#include "geometry.hpp"
+#include "kernels.hpp"
+
+// Records msg as the calling thread's last error and returns s.
+gct_status set_error(gct_status s, const std::string &msg);
+// Throws gct::GctError (GCT_ERR_OUT_OF_MEMORY or GCT_ERR_CUDA) for a failed CUDA call.
+void cuda_check(cudaError_t e, const char *what);
+
+template <class F>
+gct_status guarded(F &&f)
+{
+    try {
+        f();
+        return GCT_OK;
+    } catch (const gct::GctError &e) {
+        return set_error(e.status, e.msg);
+    } catch (const std::bad_alloc &) {
+        return set_error(GCT_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception &e) {
+        return set_error(GCT_ERR_INVALID_ARG, e.what());
+    }
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { reset(); }
+    void reset()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count, const char *what)
+    {
+        reset();
+        if (count == 0) return;
+        cuda_check(cudaMalloc(reinterpret_cast<void **>(&p), count * sizeof(T)), what);
+        n = count;
+    }
+    void upload(const T *host, size_t count, const char *what)
+    {
+        alloc(count, what);
+        if (count) cuda_check(cudaMemcpy(p, host, count * sizeof(T), cudaMemcpyHostToDevice), what);
+    }
+};
+
+struct gct_fdk_plan {
+    int device = 0;
+    int num_sms = 148;
+    gct_geom_kind kind = GCT_GEOM_CONE_FLAT;
+    gct::Family family = gct::Family::Projective;
+    std::vector<gct_view_geom> views;
+    gct_ct_geom geom{};
+    gct_vol_geom vol{};
+    gct_filt_params filt{};
+    gct_fdk_opts opts{};
+    gct::RotationInfo rot;
+    bool z_affine = true;
+    unsigned L = 0;
+    int nv = 0, nr = 0, nc = 0;
+    float l1 = 0.f;
+    int zpt = 8, bx = 32, by = 8;
+    DevBuf<float4> fview;
+    DevBuf<float> parker;
+    DevBuf<float2> H, tw;
+    DevBuf<float> coefs;
+    DevBuf<unsigned char> work;
+    // Toeplitz-GEMM filter: B = T^T split into BF16 hi/lo [Np][Kp], A rows [nv*nr][Kp], FP32 rows
+    int Kp = 0, Np = 0;
+    DevBuf<__nv_bfloat16> th, tl, xh, xl;
+    DevBuf<float> ybuf;
+    DevBuf<int> gemm_err;
+    // staging for gct_fdk_execute_host
+    DevBuf<float> host_proj, host_vol;
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t> chunk_events;
+
+    ~gct_fdk_plan()
+    {
+        for (cudaEvent_t e : chunk_events) cudaEventDestroy(e);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
+    }
+
+    size_t quad_bytes() const { return opts.storage == GCT_STORAGE_F16 ? 8 : 16; }
+    // Workspace layout: the quads of view v at v * view_bytes(), then (FP16 storage) the per-view
+    // maxima, scales and inverse scales, nv floats each, from quad_region() on.
+    size_t view_bytes() const
+    {
+        return static_cast<size_t>(nr + 2 * gct::kQuadPad) * (nc + 2 * gct::kQuadPad) * quad_bytes();
+    }
+    size_t quad_region() const { return (static_cast<size_t>(nv) * view_bytes() + 255) & ~static_cast<size_t>(255); }
+    size_t scale_bytes() const { return opts.storage == GCT_STORAGE_F16 ? 3 * sizeof(float) * nv : 0; }
+    size_t workspace_bytes() const { return quad_region() + scale_bytes(); }
+};
+
+// One filtered stack: the quads of view v at quads + v * view_bytes() and, for FP16 storage, the
+// view's maximum, scale and inverse scale at amax[v], vscale[v], vinv[v]. All four are view-0
+// addresses, so a chunk of views may live at a shifted base.
+struct StackRef {
+    unsigned char *quads = nullptr;
+    float *amax = nullptr, *vscale = nullptr, *vinv = nullptr;
+};
+
+inline StackRef stack_of(const gct_fdk_plan *p, void *workspace)
+{
+    StackRef r;
+    r.quads = static_cast<unsigned char *>(workspace);
+    if (p->opts.storage == GCT_STORAGE_F16) {
+        r.amax = reinterpret_cast<float *>(r.quads + p->quad_region());
+        r.vscale = r.amax + p->nv;
+        r.vinv = r.vscale + p->nv;
+    }
+    return r;
+}
+
+// Stage functions (abi.cu). `out` / StackRef bases are view-0 addresses; [vb, vb + vc) is the
+// view range worked on.
+void run_filter(gct_fdk_plan *p, const float *proj, void *out, const float *vscale, int mode, int vb, int vc,
+                cudaStream_t s);
+void prepare(gct_fdk_plan *p, const float *proj, const StackRef &st, int vb, int vc, cudaStream_t s);
+gct::BpArgs bp_args(const gct_fdk_plan *p, const StackRef &st, float *vol, int v_begin, int v_count);
+void run_backproject(gct_fdk_plan *p, const StackRef &st, float *vol, int v_begin, int v_count, bool accumulate,
+                     cudaStream_t s);
+void check_range(const gct_fdk_plan *p, uint32_t vb, uint32_t vc);
+void *plan_workspace(gct_fdk_plan *p, void *workspace);
