@@ -66,8 +66,9 @@ def parse_args():
     ap.add_argument("--config", choices=sorted(CONFIGS), default="cone512")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--zpt", type=int, default=0, help="backprojection z per thread (0 = default)")
-    ap.add_argument("--mixed-filter", choices=["gemm", "fft"], default="gemm",
-                    help="ramp filter of the mixed path: BF16x3 Toeplitz GEMM on tcgen05, or the FFT")
+    ap.add_argument("--mixed-filter", choices=["gemm4", "gemm3", "fft"], default="gemm4",
+                    help="ramp filter of the mixed path: split-BF16 Toeplitz GEMM on tcgen05 in the four-term "
+                         "form (three pieces of rows and central taps) or three terms, or the FFT")
     ap.add_argument("--no-error", action="store_true", help="skip the FP64 oracle error check")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -342,7 +343,8 @@ def run_gct(args, cfg, rank, world, local_rank):
     updates = nx * ny * nz * cg.num_views
     proj = make_projections(cg, cfg, args.seed + rank, device)
     stream = torch.cuda.current_stream()
-    mixed_filter = g.FILTER_TOEPLITZ_BF16X3 if args.mixed_filter == "gemm" else g.FILTER_FFT
+    mixed_filter = {"gemm4": g.FILTER_TOEPLITZ_BF16X4, "gemm3": g.FILTER_TOEPLITZ_BF16X3,
+                    "fft": g.FILTER_FFT}[args.mixed_filter]
     plans = {
         "mixed": g.FdkPlan(cg, vg, opts=g.FdkOptions(filter=mixed_filter, storage=g.STORAGE_F16,
                                                      z_per_thread=args.zpt)),
@@ -430,8 +432,12 @@ def run_gct(args, cfg, rank, world, local_rank):
         "e2e": e2e,
         "clocks": clocks,
         # per mixed step: view max, view scale, (split, GEMM, quads | FFT filter), backprojection
-        "gpu_launches": (6 if args.mixed_filter == "gemm" else 4) * args.steps,
-        "mixed_filter": ("BF16x3 Toeplitz GEMM (tcgen05)" if args.mixed_filter == "gemm" else "shared-memory FFT"),
+        # per mixed step: view max, view scale, (split, GEMM, quads | FFT filter), backprojection
+        "gpu_launches": (4 if args.mixed_filter == "fft" else 6) * args.steps,
+        "mixed_filter": {"gemm4": "split-BF16 Toeplitz GEMM on tcgen05, 4 terms + banded 5th (rows and central "
+                                  "taps in three BF16 pieces)",
+                         "gemm3": "split-BF16 Toeplitz GEMM on tcgen05, 3 terms",
+                         "fft": "shared-memory FFT"}[args.mixed_filter],
     }
     print(json.dumps(line), flush=True)
 

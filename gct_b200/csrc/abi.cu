@@ -62,7 +62,8 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
     p->vol = *vol;
     p->filt = filt ? *filt : gct_filt_params{1.0, GCT_APOD_NONE};
     if (opts) p->opts = *opts;
-    if (p->opts.filter != GCT_FILTER_FFT && p->opts.filter != GCT_FILTER_TOEPLITZ_BF16X3)
+    if (p->opts.filter != GCT_FILTER_FFT && p->opts.filter != GCT_FILTER_TOEPLITZ_BF16X3 &&
+        p->opts.filter != GCT_FILTER_TOEPLITZ_BF16X4)
         gct::fail(GCT_ERR_INVALID_ARG, "unknown filter option");
     if (p->opts.storage != GCT_STORAGE_F32 && p->opts.storage != GCT_STORAGE_F16)
         gct::fail(GCT_ERR_INVALID_ARG, "unknown storage option");
@@ -130,25 +131,34 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
     p->H.upload(H.data(), H.size(), "plan filter spectrum");
     p->tw.upload(tw.data(), tw.size(), "plan twiddles");
     p->coefs.upload(coefs.data(), coefs.size(), "plan backprojection coefficients");
-    if (p->opts.filter == GCT_FILTER_TOEPLITZ_BF16X3) {
+    if (p->opts.filter != GCT_FILTER_FFT) {
         // B = T^T with T[k][c] = g(c - k): row n holds g(n - k); taps g(m) = taps[m + nc/2]
         p->Kp = gct::gemm_pad_k(p->nc);
         p->Np = gct::gemm_pad_n(p->nc);
-        std::vector<__nv_bfloat16> bh(static_cast<size_t>(p->Np) * p->Kp, __float2bfloat16(0.f)), bl(bh);
+        const bool four = p->opts.filter == GCT_FILTER_TOEPLITZ_BF16X4;
+        std::vector<__nv_bfloat16> bh(static_cast<size_t>(p->Np) * p->Kp, __float2bfloat16(0.f)), bl(bh), bll;
+        if (four) bll = bh;
         for (int n = 0; n < p->nc; ++n)
             for (int k = 0; k < p->nc; ++k) {
                 const int m = n - k + p->nc / 2;
                 if (m < 0 || m >= p->nc) continue;
                 const double t = taps[m];
                 const __nv_bfloat16 hi = __float2bfloat16(static_cast<float>(t));
-                bh[static_cast<size_t>(n) * p->Kp + k] = hi;
-                bl[static_cast<size_t>(n) * p->Kp + k] = __float2bfloat16(static_cast<float>(t - static_cast<double>(__bfloat162float(hi))));
+                const double r1 = t - static_cast<double>(__bfloat162float(hi));
+                const __nv_bfloat16 lo = __float2bfloat16(static_cast<float>(r1));
+                const size_t at = static_cast<size_t>(n) * p->Kp + k;
+                bh[at] = hi;
+                bl[at] = lo;
+                if (four && std::abs(n - k) <= gct::kGemmBand)
+                    bll[at] = __float2bfloat16(static_cast<float>(r1 - static_cast<double>(__bfloat162float(lo))));
             }
         p->th.upload(bh.data(), bh.size(), "Toeplitz matrix (hi)");
         p->tl.upload(bl.data(), bl.size(), "Toeplitz matrix (lo)");
+        if (four) p->tll.upload(bll.data(), bll.size(), "Toeplitz matrix (third piece, central band)");
         const size_t rows = static_cast<size_t>(p->nv) * p->nr;
         p->xh.alloc(rows * p->Kp, "GEMM rows (hi)");
         p->xl.alloc(rows * p->Kp, "GEMM rows (lo)");
+        if (four) p->xll.alloc(rows * p->Kp, "GEMM rows (third piece)");
         p->ybuf.alloc(rows * p->nc, "GEMM filtered rows");
         p->gemm_err.alloc(1, "GEMM status");
         cuda_check(cudaMemset(p->gemm_err.p, 0, sizeof(int)), "GEMM status reset");
@@ -186,11 +196,15 @@ void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float 
     sa.parker = p->parker.p;
     sa.xh = p->xh.p;
     sa.xl = p->xl.p;
+    sa.xll = p->xll.p;
     gct::launch_split(sa, p->num_sms, s);
     cuda_check(cudaGetLastError(), "split kernel launch");
     gct::GemmLaunch gl;
     gl.xh = p->xh.p;
     gl.xl = p->xl.p;
+    gl.xll = p->xll.p;
+    gl.tll = p->tll.p;
+    gl.terms = p->opts.filter == GCT_FILTER_TOEPLITZ_BF16X4 ? 4 : 3;
     gl.a_rows = static_cast<long long>(p->nv) * p->nr;
     gl.th = p->th.p;
     gl.tl = p->tl.p;
@@ -224,7 +238,7 @@ void run_filter(gct_fdk_plan *p, const float *proj, void *out, const float *vsca
                 cudaStream_t s)
 {
     if (vc <= 0) return;
-    if (p->opts.filter == GCT_FILTER_TOEPLITZ_BF16X3) {
+    if (p->opts.filter != GCT_FILTER_FFT) {
         run_filter_gemm(p, proj, out, vscale, mode, vb, vc, s);
         return;
     }

@@ -8,6 +8,7 @@ namespace gct {
 
 int gemm_pad_k(int n);  // K padded to the 64-column tile
 int gemm_pad_n(int n);  // N padded to the 256-column tile
+constexpr int kGemmBand = 64;  // |c - k| of the taps with a third BF16 piece (four-term form)
 size_t toeplitz_gemm_smem_bytes();
 
 struct SplitArgs {
@@ -20,13 +21,17 @@ struct SplitArgs {
     const float4 *fview = nullptr;
     const float *parker = nullptr;
     __nv_bfloat16 *xh = nullptr, *xl = nullptr;  // [all rows][Kp]
+    __nv_bfloat16 *xll = nullptr;                // third piece (four-term GEMM), or NULL
 };
 void launch_split(const SplitArgs &a, int num_sms, cudaStream_t s);
 
 struct GemmLaunch {
     const __nv_bfloat16 *xh = nullptr, *xl = nullptr;  // A: [a_rows][Kp]
+    const __nv_bfloat16 *xll = nullptr;                // third piece of A (terms == 4)
+    int terms = 3;                                     // 3: Xh Th + Xh Tl + Xl Th; 4: + Xll Th + Xh Tll
     long long a_rows = 0;
     const __nv_bfloat16 *th = nullptr, *tl = nullptr;  // B = T^T: [Np][Kp]
+    const __nv_bfloat16 *tll = nullptr;                // third piece of B, central band (terms == 4)
     int Np = 0, Kp = 0;
     int m_begin = 0, M = 0, N = 0;
     float *Y = nullptr;  // row m_begin + i at Y + i * ldy

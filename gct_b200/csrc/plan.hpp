@@ -103,6 +103,7 @@ struct gct_fdk_plan {
     // Toeplitz-GEMM filter: B = T^T split into BF16 hi/lo [Np][Kp], A rows [nv*nr][Kp], FP32 rows
     int Kp = 0, Np = 0;
     DevBuf<__nv_bfloat16> th, tl, xh, xl;
+    DevBuf<__nv_bfloat16> xll, tll;  // four-term filter: third piece of the rows and of the central taps
     DevBuf<float> ybuf;
     DevBuf<int> gemm_err;
     // staging for gct_fdk_execute_host

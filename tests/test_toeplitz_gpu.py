@@ -3,7 +3,9 @@ oracle and against the FFT filter.
 
 Tolerances (relative RMS): filtered rows vs the FP64 oracle <= 3e-4 (the dropped lo x lo term and
 BF16 rounding of the split give ~1e-4 on small detectors, where the alternating ramp taps cancel
-most of the products); full FDK with FP32 quads <= 1e-4, with FP16 quads <= 1e-3.
+most of the products); full FDK with FP32 quads <= 1e-4, with FP16 quads <= 1e-3. The four-term
+form (three BF16 pieces of the rows and of the central taps) is held to the same bounds and must
+be at least as accurate as the three-term form on noisy rows.
 """
 import numpy as np
 import pytest
@@ -16,6 +18,7 @@ from oracle import oracle as orc
 pytestmark = pytest.mark.gpu
 
 TOEPLITZ = g.FILTER_TOEPLITZ_BF16X3
+BOTH = [g.FILTER_TOEPLITZ_BF16X3, g.FILTER_TOEPLITZ_BF16X4]
 
 
 def _filter(case, proj, filt=TOEPLITZ):
@@ -38,32 +41,50 @@ def _fdk(case, proj, storage, filt=TOEPLITZ):
     return vol.cpu().numpy()
 
 
+@pytest.mark.parametrize("filt", BOTH)
 @pytest.mark.parametrize("kind", ["cone_flat", "fan_arc"])
-def test_toeplitz_filter_matches_oracle(kind):
+def test_toeplitz_filter_matches_oracle(kind, filt):
     case = make_case(kind)
     proj = oracle_projections(case)
-    got = _filter(case, proj)
+    got = _filter(case, proj, filt)
     ref = orc.filter_stack(case.og, proj).reshape(got.shape)
     assert rel_rms(got, ref) <= 3e-4
 
 
+@pytest.mark.parametrize("filt", BOTH)
 @pytest.mark.parametrize("nc,nr,nv", [(75, 13, 37), (300, 40, 20), (1024, 8, 6)])
-def test_toeplitz_odd_sizes(nc, nr, nv):
+def test_toeplitz_odd_sizes(nc, nr, nv, filt):
     # K and N not multiples of the 64 / 256 tiles, M not a multiple of 128
     case = make_case("cone_flat", nv=nv, nc=nc, nr=nr)
     proj = oracle_projections(case)
-    got = _filter(case, proj)
+    got = _filter(case, proj, filt)
     ref = orc.filter_stack(case.og, proj).reshape(got.shape)
     assert rel_rms(got, ref) <= 3e-4
 
 
+@pytest.mark.parametrize("filt", BOTH)
 @pytest.mark.parametrize("kind", KINDS)
-def test_toeplitz_fdk_matches_oracle(kind):
+def test_toeplitz_fdk_matches_oracle(kind, filt):
     case = make_case(kind)
     proj = oracle_projections(case)
     ref = orc.fdk(case.og, case.ov, proj).reshape(case.vg.shape)
-    assert rel_rms(_fdk(case, proj, g.STORAGE_F32), ref) <= 1e-4
-    assert rel_rms(_fdk(case, proj, g.STORAGE_F16), ref) <= 1e-3
+    assert rel_rms(_fdk(case, proj, g.STORAGE_F32, filt), ref) <= 1e-4
+    assert rel_rms(_fdk(case, proj, g.STORAGE_F16, filt), ref) <= 1e-3
+
+
+def test_four_terms_at_least_as_accurate_on_noisy_rows():
+    # Poisson-noisy line integrals of a large object: two BF16 pieces of the rows and of the taps
+    # leave residuals of the smooth part that the ramp filter does not cancel
+    case = make_case("cone_flat", nc=512, nr=16, nv=24)
+    rng = np.random.default_rng(5)
+    proj = oracle_projections(case, scale=3.0) * np.float32(4.0)
+    counts = rng.poisson(1e5 * np.exp(-proj.astype(np.float64)))
+    proj = (-np.log(np.maximum(counts, 1) / 1e5)).astype(np.float32)
+    ref = orc.filter_stack(case.og, proj).reshape(proj.shape)
+    e3 = rel_rms(_filter(case, proj, g.FILTER_TOEPLITZ_BF16X3), ref)
+    e4 = rel_rms(_filter(case, proj, g.FILTER_TOEPLITZ_BF16X4), ref)
+    assert e4 <= e3
+    assert e4 <= 2e-4
 
 
 def test_toeplitz_and_fft_agree():
