@@ -13,6 +13,7 @@ from pathlib import Path
 from . import _build
 
 GCT_OK = 0
+GCT_ERR_NOT_READY = 7
 STATUS_NAMES = {
     0: "GCT_OK", 1: "GCT_ERR_INVALID_ARG", 2: "GCT_ERR_OUT_OF_MEMORY", 3: "GCT_ERR_BUDGET",
     4: "GCT_ERR_TIMEOUT", 5: "GCT_ERR_CUDA", 6: "GCT_ERR_NOT_SUPPORTED", 7: "GCT_ERR_NOT_READY",
@@ -70,6 +71,20 @@ class gct_fdk_opts(C.Structure):
                 ("block_x", C.c_int32), ("block_y", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
+class gct_batch_item(C.Structure):
+    _fields_ = [("plan", C.c_void_p), ("proj_dev", C.c_void_p), ("vol_dev", C.c_void_p)]
+
+
+class gct_batch_opts(C.Structure):
+    _fields_ = [("autotune", C.c_int32), ("use_graph", C.c_int32), ("blocks_per_sm", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
+
+
+class gct_batch_item_config(C.Structure):
+    _fields_ = [("z_per_thread", C.c_int32), ("block_x", C.c_int32), ("block_y", C.c_int32),
+                ("views_per_stage", C.c_int32), ("view_split", C.c_int32), ("tuned_gups", C.c_double)]
+
+
 class gct_ellipsoid(C.Structure):
     _fields_ = [("center", C.c_double * 3), ("semi_axes", C.c_double * 3), ("phi", C.c_double),
                 ("mu", C.c_double)]
@@ -103,6 +118,11 @@ SIGNATURES = {
     "gct_reconstruct": [P(gct_ct_geom), P(gct_vol_geom), P(C.c_float), P(C.c_float)],
     "gct_reconstruct_ex": [P(gct_ct_geom), P(gct_vol_geom), P(gct_filt_params), P(gct_fdk_opts),
                            P(C.c_float), P(C.c_float)],
+    "gct_fdk_batch_create": [P(gct_batch_item), C.c_uint32, P(gct_batch_opts), P(VP)],
+    "gct_fdk_batch_launch": [VP, VP],
+    "gct_fdk_batch_item_config": [VP, C.c_uint32, P(gct_batch_item_config)],
+    "gct_fdk_batch_work": [VP, P(C.c_uint64), P(C.c_uint64)],
+    "gct_fdk_batch_destroy": [VP],
     "gct_phantom_project": [P(gct_ct_geom), P(gct_ellipsoid), C.c_uint32, VP, VP],
     "gct_forward_project": [P(gct_ct_geom), P(gct_vol_geom), VP, C.c_float, VP, VP],
 }

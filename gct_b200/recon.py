@@ -181,6 +181,60 @@ class FdkPlan:
         self.close()
 
 
+class FdkBatch:
+    """Many reconstructions in one persistent backprojection launch, replayed as a CUDA graph.
+
+    ``items`` is a sequence of ``(plan, proj, vol)`` with device buffers (torch CUDA tensors or
+    addresses); every ``launch`` overwrites each ``vol`` with its reconstruction. The plans and
+    buffers must outlive the batch. No counterpart in the reference (one stack per call).
+    """
+
+    def __init__(self, items, autotune: bool = True, use_graph: bool = True, blocks_per_sm: int = 0):
+        self._lib = _lib.load()
+        self._handle = C.c_void_p()
+        self._keep = list(items)
+        arr = (_lib.gct_batch_item * len(self._keep))()
+        for i, (plan, proj, vol) in enumerate(self._keep):
+            arr[i].plan = plan._handle
+            arr[i].proj_dev = _ptr(proj)
+            arr[i].vol_dev = _ptr(vol)
+        opts = _lib.gct_batch_opts()
+        opts.autotune, opts.use_graph, opts.blocks_per_sm = int(autotune), int(use_graph), int(blocks_per_sm)
+        _lib.check(self._lib.gct_fdk_batch_create(arr, len(self._keep), C.byref(opts), C.byref(self._handle)))
+
+    def launch(self, stream=None) -> None:
+        _lib.check(self._lib.gct_fdk_batch_launch(self._handle, C.c_void_p(_stream(stream))))
+
+    def item_config(self, i: int) -> dict:
+        c = _lib.gct_batch_item_config()
+        _lib.check(self._lib.gct_fdk_batch_item_config(self._handle, i, C.byref(c)))
+        return {"z_per_thread": c.z_per_thread, "block": (c.block_x, c.block_y),
+                "views_per_stage": c.views_per_stage, "view_split": c.view_split, "tuned_gups": c.tuned_gups}
+
+    def work(self) -> tuple[int, int]:
+        """(work entries, voxel-view updates) of one launch."""
+        n, u = C.c_uint64(), C.c_uint64()
+        _lib.check(self._lib.gct_fdk_batch_work(self._handle, C.byref(n), C.byref(u)))
+        return n.value, u.value
+
+    def close(self) -> None:
+        if self._handle:
+            _lib.check(self._lib.gct_fdk_batch_destroy(self._handle))
+            self._handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 def ellipsoid_array(ellipsoids) -> "C.Array":
     """ellipsoids: iterable of (cx, cy, cz, ax, ay, az, phi, mu)."""
     ell = list(ellipsoids)

@@ -300,6 +300,54 @@ gct_status gct_reconstruct_ex(const gct_ct_geom *geom, const gct_vol_geom *vol,
                               const gct_filt_params *filt, const gct_fdk_opts *opts,
                               const float *proj_host, float *vol_host);
 
+/* ---- batches (device) -------------------------------------------------------------------- */
+
+/* Many reconstructions of uneven sizes and geometries in one persistent backprojection launch.
+ * No counterpart in the reference, which reconstructs one stack per call
+ * (src/cuda/recon/recon_wrappers.cuh:15-43) with one backprojection launch per view
+ * (src/cuda/recon/fdk_axial.cuh:189-193).
+ *
+ * gct_fdk_batch_create takes the items (each: a plan, its device projections and its device
+ * volume), allocates a workspace per item, picks each item's tile shape (z-voxels per thread,
+ * block footprint, views per coefficient stage) with an on-device autotuner whose results are
+ * cached per process, device and item shape, builds one work queue of (volume tile, view chunk)
+ * entries per storage type, and captures the filter stages of all items (on up to four forked
+ * streams) plus the queue launches as one CUDA graph. gct_fdk_batch_launch replays it on
+ * `stream`: every item's volume is overwritten with its reconstruction, the values
+ * gct_fdk_execute gives up to the order of the floating-point sums. The buffers and plans must
+ * stay alive while the batch exists; items that share a plan run their filter stages one after
+ * another. The batch uses the plans' filter scratch: do not run those plans elsewhere while a
+ * launch is in flight. */
+typedef struct gct_fdk_batch gct_fdk_batch;
+
+typedef struct {
+    gct_fdk_plan *plan;
+    const float *proj_dev;    /* [view][row][col] */
+    float *vol_dev;           /* [z][y][x], overwritten */
+} gct_batch_item;
+
+typedef struct {
+    int32_t autotune;         /* 1: time tile shapes on the device (default); 0: fixed defaults */
+    int32_t use_graph;        /* 1: replay a captured CUDA graph (default); 0: issue stage by stage */
+    int32_t blocks_per_sm;    /* resident blocks of the queue kernel per SM; 0: its occupancy */
+    int32_t reserved[5];
+} gct_batch_opts;
+
+typedef struct {
+    int32_t z_per_thread, block_x, block_y, views_per_stage;
+    int32_t view_split;       /* view chunks of the item's tiles (> 1: atomic accumulation) */
+    double tuned_gups;        /* autotuner's measured rate of the chosen shape; 0 if untuned */
+} gct_batch_item_config;
+
+/* opts may be NULL (autotune, graph). */
+gct_status gct_fdk_batch_create(const gct_batch_item *items, uint32_t count, const gct_batch_opts *opts,
+                                gct_fdk_batch **out);
+gct_status gct_fdk_batch_launch(gct_fdk_batch *batch, void *stream);
+gct_status gct_fdk_batch_item_config(const gct_fdk_batch *batch, uint32_t item, gct_batch_item_config *out);
+/* Work entries in the queues and voxel-view updates of one launch. */
+gct_status gct_fdk_batch_work(const gct_fdk_batch *batch, uint64_t *work_entries, uint64_t *updates);
+gct_status gct_fdk_batch_destroy(gct_fdk_batch *batch);
+
 /* ---- projection (device) ---------------------------------------------------------------- */
 
 /* Analytic phantom: an ellipsoid with centre c (mm), semi-axes a (mm), rotation angle

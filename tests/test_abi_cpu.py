@@ -131,3 +131,11 @@ def test_no_cpu_fallback_without_a_device():
     vol = g.ReconImg(vg)
     with pytest.raises(g.GctError):
         g.reconstruct(cg, g.ProjectionStack(16, 8, 8), vol)
+
+
+def test_empty_batch_rejected():
+    lib = _lib.load()
+    out = C.c_void_p()
+    assert lib.gct_fdk_batch_create(None, 0, None, C.byref(out)) == 1
+    assert not out.value
+    assert b"empty batch" in lib.gct_last_error_string()
