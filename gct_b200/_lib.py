@@ -85,6 +85,23 @@ class gct_batch_item_config(C.Structure):
                 ("views_per_stage", C.c_int32), ("view_split", C.c_int32), ("tuned_gups", C.c_double)]
 
 
+class gct_server_opts(C.Structure):
+    _fields_ = [("memory_budget_bytes", C.c_uint64), ("max_active", C.c_uint32), ("autotune", C.c_uint32),
+                ("round_updates", C.c_double), ("reserved", C.c_int32 * 4)]
+
+
+class gct_request_info(C.Structure):
+    _fields_ = [("state", C.c_int32), ("status", C.c_int32), ("queued_ms", C.c_double), ("latency_ms", C.c_double),
+                ("rounds", C.c_uint32), ("views_per_round", C.c_uint32)]
+
+
+class gct_server_stats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("cancelled", C.c_uint64), ("rejected", C.c_uint64), ("rounds", C.c_uint64),
+                ("peak_bytes", C.c_uint64), ("peak_active", C.c_uint32), ("p50_ms", C.c_double),
+                ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("recons_per_s", C.c_double)]
+
+
 class gct_ellipsoid(C.Structure):
     _fields_ = [("center", C.c_double * 3), ("semi_axes", C.c_double * 3), ("phi", C.c_double),
                 ("mu", C.c_double)]
@@ -123,6 +140,13 @@ SIGNATURES = {
     "gct_fdk_batch_item_config": [VP, C.c_uint32, P(gct_batch_item_config)],
     "gct_fdk_batch_work": [VP, P(C.c_uint64), P(C.c_uint64)],
     "gct_fdk_batch_destroy": [VP],
+    "gct_fdk_server_create": [P(gct_server_opts), P(VP)],
+    "gct_fdk_server_submit": [VP, VP, P(C.c_float), P(C.c_float), P(C.c_uint64)],
+    "gct_fdk_server_info": [VP, C.c_uint64, P(gct_request_info)],
+    "gct_fdk_server_wait": [VP, C.c_uint64, C.c_double],
+    "gct_fdk_server_cancel": [VP, C.c_uint64],
+    "gct_fdk_server_stats": [VP, P(gct_server_stats)],
+    "gct_fdk_server_destroy": [VP],
     "gct_phantom_project": [P(gct_ct_geom), P(gct_ellipsoid), C.c_uint32, VP, VP],
     "gct_forward_project": [P(gct_ct_geom), P(gct_vol_geom), VP, C.c_float, VP, VP],
 }

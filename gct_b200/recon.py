@@ -235,6 +235,80 @@ class FdkBatch:
         self.close()
 
 
+REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
+
+
+class FdkServer:
+    """Request loop with continuous batching over a device-memory budget (gct_fdk_server_*).
+
+    ``submit(plan, proj, vol)`` takes host float32 arrays ([view][row][col] in, [z][y][x] out),
+    keeps references to them until the request finishes and returns a ticket. Pinned arrays
+    (e.g. from ``torch.empty(..., pin_memory=True).numpy()``) let the copies overlap.
+    No counterpart in the reference (one synchronous reconstruction per call).
+    """
+
+    def __init__(self, memory_budget_bytes: int, max_active: int = 0, autotune: bool = False,
+                 round_updates: float = 0.0):
+        self._lib = _lib.load()
+        self._handle = C.c_void_p()
+        self._keep = {}
+        o = _lib.gct_server_opts()
+        o.memory_budget_bytes, o.max_active, o.autotune = int(memory_budget_bytes), int(max_active), int(autotune)
+        o.round_updates = float(round_updates)
+        _lib.check(self._lib.gct_fdk_server_create(C.byref(o), C.byref(self._handle)))
+
+    def submit(self, plan, proj: np.ndarray, vol: np.ndarray) -> int:
+        fp = C.POINTER(C.c_float)
+        for a in (proj, vol):
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags.c_contiguous):
+                raise TypeError("expected contiguous float32 numpy arrays")
+        t = C.c_uint64()
+        _lib.check(self._lib.gct_fdk_server_submit(self._handle, plan._handle, proj.ctypes.data_as(fp),
+                                                   vol.ctypes.data_as(fp), C.byref(t)))
+        self._keep[t.value] = (plan, proj, vol)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: float = -1.0) -> None:
+        """Blocks until the request finishes; raises GctError if it failed, was cancelled or timed out."""
+        st = self._lib.gct_fdk_server_wait(self._handle, ticket, float(timeout_ms))
+        if st != _lib.GCT_ERR_NOT_READY:
+            self._keep.pop(ticket, None)
+        _lib.check(st)
+
+    def info(self, ticket: int) -> dict:
+        i = _lib.gct_request_info()
+        _lib.check(self._lib.gct_fdk_server_info(self._handle, ticket, C.byref(i)))
+        return {"state": REQ_STATES.get(i.state, i.state), "status": i.status, "queued_ms": i.queued_ms,
+                "latency_ms": i.latency_ms, "rounds": i.rounds, "views_per_round": i.views_per_round}
+
+    def cancel(self, ticket: int) -> None:
+        _lib.check(self._lib.gct_fdk_server_cancel(self._handle, ticket))
+        self._keep.pop(ticket, None)
+
+    def stats(self) -> dict:
+        s = _lib.gct_server_stats()
+        _lib.check(self._lib.gct_fdk_server_stats(self._handle, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in _lib.gct_server_stats._fields_}
+
+    def close(self) -> None:
+        if self._handle:
+            _lib.check(self._lib.gct_fdk_server_destroy(self._handle))
+            self._handle = C.c_void_p()
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 def ellipsoid_array(ellipsoids) -> "C.Array":
     """ellipsoids: iterable of (cx, cy, cz, ax, ay, az, phi, mu)."""
     ell = list(ellipsoids)

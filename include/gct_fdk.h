@@ -348,6 +348,77 @@ gct_status gct_fdk_batch_item_config(const gct_fdk_batch *batch, uint32_t item, 
 gct_status gct_fdk_batch_work(const gct_fdk_batch *batch, uint64_t *work_entries, uint64_t *updates);
 gct_status gct_fdk_batch_destroy(gct_fdk_batch *batch);
 
+/* ---- serving (device) -------------------------------------------------------------------- */
+
+/* A request loop with continuous batching. No counterpart in the reference (one synchronous
+ * reconstruction per call, src/cuda/recon/recon_wrappers.cuh:15-43).
+ *
+ * gct_fdk_server_create reserves `memory_budget_bytes` of device memory once and starts a worker
+ * thread on the current device. gct_fdk_server_submit queues a request (a plan, host projections
+ * [view][row][col], a host volume [z][y][x] to fill) and returns a ticket; requests are admitted
+ * in arrival order as soon as their projections, workspace and volume fit in the free part of the
+ * budget and fewer than max_active are on the device. An admitted request is uploaded and
+ * filtered on its own streams while others backproject; the backprojection runs in rounds, each
+ * one persistent work-queue launch over the tiles of every active request, each request
+ * contributing its next chunk of views (sized from its own shape only: about round_updates
+ * voxel-view updates, at least 16 views). Requests arriving meanwhile join the next round. A
+ * finished volume is copied back and its memory returned to the budget.
+ *
+ * Because a request's chunks and tile shape depend only on the request (and the process-wide
+ * autotuner cache), its result is bit-identical whether it runs alone or among others. Host
+ * buffers must stay valid until the request completes; pinned memory lets copies overlap. The
+ * plan's filter scratch is used by the worker: do not run a plan elsewhere while the server holds
+ * requests for it. */
+typedef struct gct_fdk_server gct_fdk_server;
+
+typedef struct {
+    uint64_t memory_budget_bytes;   /* device bytes for admitted requests (required) */
+    uint32_t max_active;            /* requests admitted at once; 0 = 64 */
+    uint32_t autotune;              /* 1 = tile shapes from the autotuner (default 0 = fixed) */
+    double round_updates;           /* voxel-view updates per request per round; 0 = 2e9 */
+    int32_t reserved[4];
+} gct_server_opts;
+
+typedef enum {
+    GCT_REQ_QUEUED = 0,
+    GCT_REQ_RUNNING = 1,
+    GCT_REQ_DONE = 2,
+    GCT_REQ_FAILED = 3,
+    GCT_REQ_CANCELLED = 4
+} gct_req_state;
+
+typedef struct {
+    int32_t state;                  /* gct_req_state */
+    int32_t status;                 /* gct_status of a failed request, else GCT_OK */
+    double queued_ms;               /* submit -> admission */
+    double latency_ms;              /* submit -> volume on the host */
+    uint32_t rounds;                /* backprojection rounds the request took part in */
+    uint32_t views_per_round;
+} gct_request_info;
+
+typedef struct {
+    uint64_t submitted, completed, failed, cancelled, rejected;
+    uint64_t rounds;                /* backprojection rounds launched */
+    uint64_t peak_bytes;            /* most budget bytes in use at once */
+    uint32_t peak_active;           /* most requests admitted at once */
+    double p50_ms, p99_ms, mean_ms; /* latency of completed requests */
+    double recons_per_s;            /* completed / (last completion - first submission) */
+} gct_server_stats;
+
+gct_status gct_fdk_server_create(const gct_server_opts *opts, gct_fdk_server **out);
+/* GCT_ERR_BUDGET if the request alone exceeds the budget. */
+gct_status gct_fdk_server_submit(gct_fdk_server *server, gct_fdk_plan *plan, const float *proj_host,
+                                 float *vol_host, uint64_t *ticket);
+gct_status gct_fdk_server_info(gct_fdk_server *server, uint64_t ticket, gct_request_info *info);
+/* Blocks until the request is done, failed or cancelled (its status is returned) or timeout_ms
+ * passes (GCT_ERR_NOT_READY); timeout_ms < 0 waits without limit. */
+gct_status gct_fdk_server_wait(gct_fdk_server *server, uint64_t ticket, double timeout_ms);
+/* Cancels a request that is still queued; GCT_ERR_NOT_READY if it was already admitted. */
+gct_status gct_fdk_server_cancel(gct_fdk_server *server, uint64_t ticket);
+gct_status gct_fdk_server_stats(gct_fdk_server *server, gct_server_stats *stats);
+/* Finishes every request, stops the worker and releases the budget. */
+gct_status gct_fdk_server_destroy(gct_fdk_server *server);
+
 /* ---- projection (device) ---------------------------------------------------------------- */
 
 /* Analytic phantom: an ellipsoid with centre c (mm), semi-axes a (mm), rotation angle
