@@ -57,13 +57,34 @@ CONFIGS = {
 }
 
 
+# Batched mix (C4, 48 reconstructions). Choices the mix leaves open are fixed here and echoed in
+# the JSON line: 2D parallel N x N with 1.42 N cells (FOV 250 mm); fan arc 672 channels over a
+# 0.907 rad fan (SOD 570, SDD 1040) into 512^2 at 0.9 mm; cylindrical cone 64 x 896 (arc 0.0011
+# rad, rows 1.0 mm, SOD 600, SDD 1100) and cone-parallel (rebinned) 64 x 736 at 0.65 mm, both into
+# 512 x 512 x 64 at 0.9 x 0.9 x 0.55 mm, 1152 views each.
+BATCH48_2D = [(256, 180), (512, 360), (1024, 900), (2048, 1800)]
+BATCH48_LABEL = ("48 uneven reconstructions in one persistent launch: 24 x 2D parallel (256-2048 px, 180-1800 "
+                 "views), 8 x fan arc 672 ch x 1152 views -> 512^2, 8 x cylindrical cone 64x896 x 1152 views -> "
+                 "512x512x64, 8 x cone-parallel 64x736 x 1152 views -> 512x512x64")
+# Serving mix (C5): 70 % 2D fan (line detector, 768 cells at 1.0 mm, SOD 570, SDD 1040, 720 views ->
+# 512^2 at 0.8 mm), 25 % cylindrical cone (the C4 geometry -> 512 x 512 x 64), 5 % flat cone 512^3
+# (the cone512 workload); 80 GB budget, mixed precision (FP16 quads; the flat cone with the
+# four-term Toeplitz filter, the others with the FFT filter).
+SERVE_LABEL = ("Poisson arrivals, mix 70/25/5: 2D fan 512^2 x 720 views / cylindrical cone 512x512x64 x 1152 "
+               "views / flat cone 512^3 x 720 views, 80 GB budget, mixed precision")
+EXTRA_CONFIGS = ["batch48", "serve"]
+
+
 def parse_args():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["gct", "reference"], default="gct")
-    ap.add_argument("--config", choices=sorted(CONFIGS), default="cone512")
+    ap.add_argument("--config", choices=sorted(CONFIGS) + EXTRA_CONFIGS, default="cone512")
+    ap.add_argument("--serve-requests", type=int, default=160, help="requests per arrival rate (serve)")
+    ap.add_argument("--serve-loads", type=str, default="0.3,0.6,0.9",
+                    help="arrival rates as fractions of the measured capacity (serve)")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--zpt", type=int, default=0, help="backprojection z per thread (0 = default)")
     ap.add_argument("--mixed-filter", choices=["gemm4", "gemm3", "fft"], default="gemm4",
@@ -442,8 +463,277 @@ def run_gct(args, cfg, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def batch48_items():
+    items = []
+    for i in range(24):
+        n, nv = BATCH48_2D[i % 4]
+        items.append(dict(kind="parallel_1d", nv=nv, nc=int(math.ceil(1.42 * n)), nr=1, du=250.0 / n, dv=1.0,
+                          n=(n, n, 1), vox=250.0 / n, voxz=1.0, n_ell=10))
+    for _ in range(8):
+        items.append(dict(kind="fan_arc", nv=1152, nc=672, nr=1, du=0.907 / 672, dv=1.0, sod=570.0, sdd=1040.0,
+                          n=(512, 512, 1), vox=0.9, voxz=1.0, n_ell=10))
+    for _ in range(8):
+        items.append(cyl_item())
+    for _ in range(8):
+        items.append(dict(kind="cone_parallel", nv=1152, nc=736, nr=64, du=0.65, dv=1.0, sod=600.0, sdd=1100.0,
+                          n=(512, 512, 64), vox=0.9, voxz=0.55, n_ell=16))
+    return items
+
+
+def cyl_item():
+    return dict(kind="cone_cyl", nv=1152, nc=896, nr=64, du=0.0011, dv=1.0, sod=600.0, sdd=1100.0,
+                n=(512, 512, 64), vox=0.9, voxz=0.55, n_ell=16)
+
+
+def make_geometry2(c):
+    """Full-scan geometry of a batch or serving item, any of the seven kinds' factories."""
+    import gct_b200 as g
+    nv, nc, nr = c["nv"], c["nc"], c["nr"]
+    rot = g.RotationParams(g.RotDir.CW, 0.0, 2 * math.pi / nv, nv)
+    c0, r0 = (nc - 1) / 2.0, (nr - 1) / 2.0
+    k = c["kind"]
+    if k == "parallel_1d":
+        det, params = (g.DetParallel(nc, c["du"]),), g.Parallel1DProjGeomParams(c0, rot)
+    elif k == "fan_arc":
+        det, params = (g.DetFanArc(nc, c["du"]),), g.FanBeamProjGeomParams(c0, rot, c["sdd"], c["sod"])
+    elif k == "fan_line":
+        det, params = (g.DetFanLine(nc, c["du"]),), g.FanBeamProjGeomParams(c0, rot, c["sdd"], c["sod"])
+    elif k == "cone_cyl":
+        det = (g.DetFanArc(nc, c["du"]), g.DetFanLine(nr, c["dv"]))
+        params = g.ConeBeamProjGeomParams(c0, rot, c["sdd"], c["sod"], r0)
+    elif k == "cone_parallel":
+        det = (g.DetParallel(nc, c["du"]), g.DetFanLine(nr, c["dv"]))
+        params = g.ConeBeamProjGeomParams(c0, rot, c["sdd"], c["sod"], r0)
+    elif k == "cone_flat":
+        det = (g.DetFanLine(nc, c["du"]), g.DetFanLine(nr, c["dv"]))
+        params = g.ConeBeamProjGeomParams(c0, rot, c["sdd"], c["sod"], r0)
+    else:
+        raise KeyError(k)
+    cg = g.AxialCTGeom.from_params(det, params)
+    nx, ny, nz = c["n"]
+    if nr > 1:
+        vg = g.ReconImgGeom(g.EqDistSampler(nx, c["vox"]), g.EqDistSampler(ny, c["vox"]),
+                            g.EqDistSampler(nz, c["voxz"]), (0.0, 0.0, 0.0))
+    else:
+        vg = g.ReconImgGeom(g.EqDistSampler(nx, c["vox"]), g.EqDistSampler(ny, c["vox"]), None, (0.0, 0.0))
+    return cg, vg
+
+
+def item_projections(cg, c, seed, device):
+    import torch
+    import gct_b200 as g
+    proj = torch.empty((cg.num_views, cg.num_rows, cg.num_cols), dtype=torch.float32, device=device)
+    g.phantom_project(cg, make_ellipsoids(dict(n=c["n"], vox=c["vox"], n_ell=c["n_ell"]), seed), proj)
+    return proj
+
+
+def device_timed(fn, steps, warmup, stream, dist, device):
+    import torch
+    for _ in range(warmup):
+        fn()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    start.record(stream)
+    for _ in range(steps):
+        fn()
+    stop.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    total = start.elapsed_time(stop) / 1000.0
+    if dist:
+        t = torch.tensor([total], device=device, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total = float(t.item())
+    return total
+
+
+def run_batch(args, rank, world, local_rank):
+    """C4: 48 uneven reconstructions as one batch (filters on forked streams + one persistent
+    work-queue backprojection, replayed as a CUDA graph), against the same 48 plans run one after
+    another through gct_fdk_execute."""
+    import torch
+    import gct_b200 as g
+    dist = world > 1
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream()
+    specs = batch48_items()
+    plans, projs, vols = [], [], []
+    updates = 0
+    for i, c in enumerate(specs):
+        cg, vg = make_geometry2(c)
+        projs.append(item_projections(cg, c, args.seed + 17 * i + rank, device))
+        plans.append(g.FdkPlan(cg, vg, opts=g.FdkOptions(filter=g.FILTER_FFT, storage=g.STORAGE_F16)))
+        vols.append(torch.empty(vg.shape, dtype=torch.float32, device=device))
+        updates += int(np.prod(c["n"])) * c["nv"]
+    torch.cuda.synchronize()
+    t_build = time.perf_counter()
+    batch = g.FdkBatch(list(zip(plans, projs, vols)))
+    t_build = time.perf_counter() - t_build
+    n_work, upd = batch.work()
+    assert upd == updates
+    sampler = ClockSampler(local_rank)
+    t_batch = device_timed(lambda: batch.launch(stream=stream), args.steps, args.warmup, stream, dist, device)
+    clocks = sampler.stop()
+    batch_vols = [v.clone() for v in vols]
+
+    def sequential():
+        for p, pr, v in zip(plans, projs, vols):
+            p.execute(pr, v, stream=stream)
+    t_seq = device_timed(sequential, args.steps, args.warmup, stream, dist, device)
+    diff = max(float(((a - b).norm() / b.norm().clamp_min(1e-30)).item()) for a, b in zip(batch_vols, vols))
+    configs = {}
+    for i, c in enumerate(specs):
+        configs[f"{c['kind']} {c['n'][0]}x{c['n'][1]}x{c['n'][2]} nv={c['nv']}"] = batch.item_config(i)
+    batch.close()
+    for p in plans:
+        p.close()
+    if rank != 0:
+        return
+    line = {
+        "metric": "FDK batched backprojection GUPS (voxel x view updates / s), 48 mixed reconstructions",
+        "value": updates * world * args.steps / t_batch / 1e9, "unit": "GUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_batch / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32-accumulate/f16-storage", "data": "synthetic",
+        "config": {"workload": "batch48", "description": BATCH48_LABEL, "items": len(specs),
+                   "filter": "shared-memory FFT", "l2": "inputs larger than L2, no flush",
+                   "parallelism": f"replicas x{world}"},
+        "recons_per_s": world * len(specs) * args.steps / t_batch,
+        "sequential": {"value": updates * world * args.steps / t_seq / 1e9, "unit": "GUPS",
+                       "ms_per_step": 1000.0 * t_seq / args.steps,
+                       "path": "the same 48 plans through gct_fdk_execute one after another"},
+        "speedup_batch_vs_sequential": t_seq / t_batch,
+        "max_rel_diff_batch_vs_sequential": diff,
+        "work_entries": n_work, "batch_build_s": t_build, "tile_configs": configs,
+        "clocks": clocks, "gpu_launches": (3 * len(specs) + 1) * args.steps,
+        "cpu_baseline": None, "e2e": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args, rank, world, local_rank):
+    """C5: Poisson arrivals of the 70/25/5 mix into the serving loop (80 GB budget) at several
+    arrival rates, host buffers in and out; p50/p99 latency and recons/s per rate."""
+    import threading
+    import torch
+    import gct_b200 as g
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    kinds = [
+        ("fan2d", 0.70, dict(kind="fan_line", nv=720, nc=768, nr=1, du=1.0, dv=1.0, sod=570.0, sdd=1040.0,
+                             n=(512, 512, 1), vox=0.8, voxz=1.0, n_ell=10), g.FILTER_FFT, 64),
+        ("cyl", 0.25, cyl_item(), g.FILTER_FFT, 24),
+        ("flat", 0.05, dict(kind="cone_flat", nv=720, nc=1024, nr=768, du=0.4, dv=0.4, sod=750.0, sdd=1200.0,
+                            n=(512, 512, 512), vox=0.5, voxz=0.5, n_ell=16), g.FILTER_TOEPLITZ_BF16X4, 6),
+    ]
+    cls = []
+    for i, (name, frac, c, filt, nbuf) in enumerate(kinds):
+        cg, vg = make_geometry2(c)
+        proj = item_projections(cg, c, args.seed + i, device)
+        hp = torch.empty(proj.shape, dtype=torch.float32, pin_memory=True)
+        hp.copy_(proj)
+        del proj
+        plan = g.FdkPlan(cg, vg, opts=g.FdkOptions(filter=filt, storage=g.STORAGE_F16))
+        outs = [torch.empty(vg.shape, dtype=torch.float32, pin_memory=True).numpy() for _ in range(nbuf)]
+        cls.append(dict(name=name, frac=frac, plan=plan, proj=hp.numpy(), outs=outs,
+                        updates=int(np.prod(c["n"])) * c["nv"]))
+    torch.cuda.empty_cache()
+    srv = g.FdkServer(80 << 30)
+
+    def run_load(rate, nreq, seed):
+        rng = np.random.default_rng(seed)
+        picks = rng.choice(len(cls), size=nreq, p=[k["frac"] for k in cls])
+        gaps = rng.exponential(1.0 / rate, size=nreq) if rate > 0 else np.zeros(nreq)
+        owner = {}   # (class, buffer) -> ticket still using it
+        nxt = [0] * len(cls)
+        tickets = []
+        t0 = time.perf_counter()
+        due = t0
+        for k, gap in zip(picks, gaps):
+            due += gap
+            now = time.perf_counter()
+            if due > now:
+                time.sleep(due - now)
+            b = nxt[k]
+            nxt[k] = (b + 1) % len(cls[k]["outs"])
+            prev = owner.get((k, b))
+            if prev is not None:
+                srv.wait(prev)
+            t = srv.submit(cls[k]["plan"], cls[k]["proj"], cls[k]["outs"][b])
+            owner[(k, b)] = t
+            tickets.append((k, t))
+        for _, t in tickets:
+            srv.wait(t)
+        span = time.perf_counter() - t0
+        lat = {}
+        for k, t in tickets:
+            lat.setdefault(cls[k]["name"], []).append(srv.info(t)["latency_ms"])
+        allv = np.concatenate([np.array(v) for v in lat.values()])
+        upd = sum(cls[k]["updates"] for k, _ in tickets)
+        return {"offered_per_s": rate, "requests": nreq, "recons_per_s": nreq / span, "gups": upd / span / 1e9,
+                "p50_ms": float(np.percentile(allv, 50)), "p99_ms": float(np.percentile(allv, 99)),
+                "per_class": {n: {"n": len(v), "p50_ms": float(np.percentile(v, 50)),
+                                  "p99_ms": float(np.percentile(v, 99))} for n, v in lat.items()}}
+
+    # capacity: everything submitted at once (closed loop), after a warm-up pass
+    run_load(0, 24, args.seed + 99)
+    sat = run_load(0, args.serve_requests, args.seed + 100)
+    cap = sat["recons_per_s"]
+    sampler = ClockSampler(local_rank)
+    loads = []
+    for j, f in enumerate(float(x) for x in args.serve_loads.split(",")):
+        loads.append(dict(load=f, **run_load(f * cap, args.serve_requests, args.seed + 200 + j)))
+    clocks = sampler.stop()
+    st = srv.stats()
+    srv.close()
+    for k in cls:
+        k["plan"].close()
+    if rank != 0:
+        return
+    mid = loads[len(loads) // 2]
+    line = {
+        "metric": "FDK serving recons/s with p50/p99 latency (continuous batching, 1 GPU)",
+        "value": mid["recons_per_s"], "unit": "recons/s", "n_gpus": world, "steps": args.serve_requests,
+        "warmup": 24, "ms_per_step": 1000.0 / mid["recons_per_s"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32-accumulate/f16-storage", "data": "synthetic",
+        "config": {"workload": "serve", "description": SERVE_LABEL, "budget_bytes": 80 << 30,
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2, no flush"},
+        "p50_ms": mid["p50_ms"], "p99_ms": mid["p99_ms"], "capacity": sat, "loads": loads,
+        "server": {"rounds": st["rounds"], "peak_active": st["peak_active"], "peak_bytes": st["peak_bytes"]},
+        "e2e": {"value": mid["recons_per_s"], "unit": "recons/s", "path": "host buffers in and out through the server"},
+        "clocks": clocks, "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.config in EXTRA_CONFIGS:
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": f"the {args.config} workload has no CPU leg; "
+                                  "the reference arm runs on the cone512 workload"}), flush=True)
+            return
+        if world > 1:
+            import datetime
+            import torch
+            torch.cuda.set_device(local_rank)
+            torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                                 device_id=torch.device("cuda", local_rank))
+        try:
+            (run_batch if args.config == "batch48" else run_serve)(args, rank, world, local_rank)
+        finally:
+            if world > 1:
+                import torch
+                torch.distributed.destroy_process_group()
+        return
     cfg = CONFIGS[args.config]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -27,6 +27,8 @@ bool vol3d(const gct_fdk_plan *p) { return p->vol.nz > 1 || is_2d_detector(p->ki
 
 BpItem make_item(const gct_fdk_plan *p, const StackRef &st, float *vol, const TileConfig &c)
 {
+    if (c.bx * c.by != kQueueThreads || c.bx < 1 || !queue_zpt_ok(c.zpt) || c.vps < 1 || c.vps > kQueueMaxVps)
+        fail(GCT_ERR_INVALID_ARG, "queue tile shape must cover 256 threads with z per thread 1, 4 or 8");
     BpItem it;
     it.a = bp_args(p, st, vol, 0, p->nv);
     it.family = static_cast<int>(p->family);

@@ -13,7 +13,7 @@ namespace gct {
 // Tile of one block of the queue kernel: zpt voxels along z per thread, bx x by threads
 // (bx * by = kQueueThreads) over x and y, vps views of coefficients staged per block barrier.
 struct TileConfig {
-    int zpt = 8, bx = 8, by = 16, vps = 32;
+    int zpt = 8, bx = 8, by = 32, vps = 32;
 };
 
 struct Tuned {
@@ -23,11 +23,13 @@ struct Tuned {
 
 bool vol3d(const gct_fdk_plan *p);
 // Queue item of a prepared stack (all views; work entries pick the view range and write mode).
+// Fails unless bx * by == kQueueThreads and zpt is a queue shape: every thread of a block owns
+// one column of its tile, and tiles must not overlap (accumulating entries would add twice).
 BpItem make_item(const gct_fdk_plan *p, const StackRef &st, float *vol, const TileConfig &c);
 long long item_tiles(const BpItem &it);
 // Work entries for every tile of queue item `item` over views [vb, vb + vc).
 std::vector<BpWork> tile_entries(int item, long long tiles, int vb, int vc, int mode);
-// The fixed shape used when autotuning is off: 8 x 16 x 8 voxels (3D) or 32 x 8 pixels (2D).
+// The fixed shape used when autotuning is off: 8 x 32 x 8 voxels (3D) or 32 x 8 pixels (2D).
 TileConfig default_config(const gct_fdk_plan *p);
 // Best tile shape for the plan's kind, storage, grid and detector sizes: every candidate is timed
 // with the queue kernel over all tiles and the first 64 views (writing into `vol`), once per

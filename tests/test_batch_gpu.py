@@ -105,6 +105,8 @@ def test_batch_graph_and_direct_issue_agree():
             outs.append([v.cpu().numpy() for _, _, v, _ in items])
     for a, b in zip(*outs):
         assert rel_rms(a, b) <= 1e-6
+    for case, (plan, dproj, _, _), got in zip(cases, items, outs[0]):
+        assert rel_rms(got, _alone(plan, dproj, case.vg.shape)) <= 1e-5, case.name
     for p, *_ in items:
         p.close()
 
