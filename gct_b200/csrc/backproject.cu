@@ -130,26 +130,70 @@ __device__ __forceinline__ void column(unsigned long long base, int stride, type
     }
 }
 
+// Block classes of one view (box_class): the block's voxels all project off the detector, all
+// well inside it, or some of each.
+constexpr int kBoxOff = 0, kBoxInside = 1, kBoxMixed = 2;
+
+// cls == kBoxInside skips the per-column range tests: box_class has shown, with a margin, that
+// every column of the block passes them, so the result is the same as with the tests.
 template <class L, int ZPT, class W>
 __device__ __forceinline__ void column_dispatch(const typename L::S *view, int qpitch, float u, float v0, float vs,
-                                                float umax, float vmax, const W &wt, float (&acc)[ZPT])
+                                                float umax, float vmax, const W &wt, float (&acc)[ZPT],
+                                                int cls = kBoxMixed)
 {
-    if (!(u >= -1.0f && u <= umax)) return;  // the column's rays miss the detector: zero
+    if (cls != kBoxInside && !(u >= -1.0f && u <= umax)) return;  // the column's rays miss the detector: zero
     int iu;
     float fu;
     split_coord(u, iu, fu);
     const float va = v0, vb = fmaf(vs, static_cast<float>(ZPT - 1), v0);
     const float lo = fminf(va, vb), hi = fmaxf(va, vb);
-    if (hi < -1.0f || lo > vmax) return;  // every voxel of the segment projects off the detector
+    if (cls != kBoxInside && (hi < -1.0f || lo > vmax)) return;  // the whole segment is off the detector
     const int stride = qpitch * static_cast<int>(sizeof(typename L::S));
     const unsigned long long base =
         reinterpret_cast<unsigned long long>(view + iu + kQuadPad) -
         static_cast<unsigned long long>(static_cast<long long>(kShiftBits - kQuadPad) * stride);
     const typename L::U fuc = L::ucol(fu);
-    if (lo >= -1.0f && hi <= vmax)
+    if (cls == kBoxInside || (lo >= -1.0f && hi <= vmax))
         column<L, ZPT, false>(base, stride, fuc, v0 - 0.5f, vs, vmax, wt, acc);
     else
         column<L, ZPT, true>(base, stride, fuc, v0 - 0.5f, vs, vmax, wt, acc);
+}
+
+// Classifies the block's voxel box [i0, i1] x [j0, j1] x [k0, k1] for one view of the affine or
+// projective (z-affine) family. u and v are linear or linear-fractional in each index with a
+// positive denominator over the box, so their extremes are at the corners; the tests keep a
+// margin of 1/64 pixel so that the per-column values, computed with the same formulas, agree.
+template <int FAMILY>
+__device__ __forceinline__ int box_class(const float *c, float i0, float i1, float j0, float j1, float k0, float k1,
+                                         float umax, float vmax)
+{
+    float ulo = 3.0e38f, uhi = -3.0e38f, vlo = 3.0e38f, vhi = -3.0e38f;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float fi = (q & 1) ? i1 : i0, fj = (q & 2) ? j1 : j0;
+        float u, va, vb;
+        if (FAMILY == 0) {
+            u = fmaf(c[2], fj, fmaf(c[1], fi, c[0]));
+            va = fmaf(c[4], k0, c[3]);
+            vb = fmaf(c[4], k1, c[3]);
+        } else {
+            const float D = fmaf(c[10], fj, fmaf(c[9], fi, c[8]));
+            if (!(D > 0.0f)) return kBoxMixed;
+            const float inv = rcp_approx(D);
+            u = fmaf(c[2], fj, fmaf(c[1], fi, c[0])) * inv;
+            const float V = fmaf(c[6], fj, fmaf(c[5], fi, c[4]));
+            va = fmaf(c[7], k0, V) * inv;
+            vb = fmaf(c[7], k1, V) * inv;
+        }
+        ulo = fminf(ulo, u);
+        uhi = fmaxf(uhi, u);
+        vlo = fminf(vlo, fminf(va, vb));
+        vhi = fmaxf(vhi, fmaxf(va, vb));
+    }
+    const float m = 1.0f / 64.0f;
+    if (uhi < -1.0f - m || ulo > umax + m || vhi < -1.0f - m || vlo > vmax + m) return kBoxOff;
+    if (ulo >= -1.0f + m && uhi <= umax - m && vlo >= -1.0f + m && vhi <= vmax - m) return kBoxInside;
+    return kBoxMixed;
 }
 
 // Clamped bilinear sample at (u, v) for the per-voxel (non-z-affine) kernels.
@@ -173,10 +217,18 @@ __device__ __forceinline__ float sample(const typename L::S *view, int qpitch, f
 // Every thread of the block calls it (it holds block barriers); inactive threads only help to
 // stage. mode: kStore writes the sums, kAccumulate adds them to the volume, kAtomic adds them
 // with atomics (several blocks share the voxels).
+// Voxel box of the calling block (active columns only; the full ZPT segment along z), used to
+// classify each view for the whole block.
+struct BlockBox {
+    float i0, i1, j0, j1, k0, k1;
+};
+
 template <int FAMILY, class Q, int ZPT, bool ZAFFINE>
 __device__ __forceinline__ void bp_column(const BpArgs &a, int i, int j, int k0, bool active, int vps,
-                                          float4 *s_coef, int tid, int nthr, int mode)
+                                          float4 *s_coef, int *s_cls, const BlockBox *s_box, int tid, int nthr,
+                                          int mode)
 {
+    constexpr bool kClassify = ZAFFINE && FAMILY != 2;
     using L = typename LerpOf<Q>::type;
     using S = typename L::S;
     const float fi = static_cast<float>(i), fj = static_cast<float>(j), fk0 = static_cast<float>(k0);
@@ -192,20 +244,27 @@ __device__ __forceinline__ void bp_column(const BpArgs &a, int i, int j, int k0,
         const float4 *g = reinterpret_cast<const float4 *>(a.coefs + static_cast<long long>(a.v_begin + vc) * kC);
         for (int t = tid; t < nvc * kC / 4; t += nthr) s_coef[t] = __ldg(g + t);
         __syncthreads();
-        if (a.vinv) {
-            for (int t = tid; t < nvc; t += nthr)
-                reinterpret_cast<float *>(s_coef)[t * kC + wscale_slot(FAMILY)] *= __ldg(a.vinv + a.v_begin + vc + t);
+        if (a.vinv || kClassify) {
+            for (int t = tid; t < nvc; t += nthr) {
+                float *ct = reinterpret_cast<float *>(s_coef) + t * kC;
+                if (a.vinv) ct[wscale_slot(FAMILY)] *= __ldg(a.vinv + a.v_begin + vc + t);
+                if (kClassify)
+                    s_cls[t] = box_class<FAMILY>(ct, s_box->i0, s_box->i1, s_box->j0, s_box->j1, s_box->k0, s_box->k1,
+                                                 a.umax, a.vmax);
+            }
             __syncthreads();
         }
         if (!active) continue;
         for (int vv = 0; vv < nvc; ++vv) {
+            const int cls = kClassify ? s_cls[vv] : kBoxMixed;
+            if (cls == kBoxOff) continue;  // exact: every column of the block would add zero
             const float *c = reinterpret_cast<const float *>(s_coef) + vv * kC;
             const S *view = quads + static_cast<long long>(a.v_begin + vc + vv) * a.qview;
             if (FAMILY == 0) {
                 // parallel kinds: u = u0 + ui i + uj j, v = v0 + vk k, constant weight
                 const float u = fmaf(c[2], fj, fmaf(c[1], fi, c[0]));
                 column_dispatch<L, ZPT>(view, a.qpitch, u, fmaf(c[4], fk0, c[3]), c[4], a.umax, a.vmax,
-                                        ConstWeight{c[5]}, acc);
+                                        ConstWeight{c[5]}, acc, cls);
             } else if (FAMILY == 1) {
                 if (ZAFFINE) {
                     const float D = fmaf(c[10], fj, fmaf(c[9], fi, c[8]));
@@ -213,7 +272,7 @@ __device__ __forceinline__ void bp_column(const BpArgs &a, int i, int j, int k0,
                     const float u = fmaf(c[2], fj, fmaf(c[1], fi, c[0])) * inv;
                     const float v0 = fmaf(c[7], fk0, fmaf(c[6], fj, fmaf(c[5], fi, c[4]))) * inv;
                     column_dispatch<L, ZPT>(view, a.qpitch, u, v0, c[7] * inv, a.umax, a.vmax,
-                                            ConstWeight{c[12] * inv * inv}, acc);
+                                            ConstWeight{c[12] * inv * inv}, acc, cls);
                 } else {
 #pragma unroll
                     for (int z = 0; z < ZPT; ++z) {
@@ -264,13 +323,26 @@ __device__ __forceinline__ void bp_column(const BpArgs &a, int i, int j, int k0,
     }
 }
 
+__device__ __forceinline__ BlockBox block_box(const BpArgs &a, int i0, int j0, int bx, int by, int k0, int zpt)
+{
+    return BlockBox{static_cast<float>(i0), static_cast<float>(min(i0 + bx, a.nx) - 1), static_cast<float>(j0),
+                    static_cast<float>(min(j0 + by, a.ny) - 1), static_cast<float>(k0),
+                    static_cast<float>(k0 + zpt - 1)};
+}
+
 template <int FAMILY, class Q, int ZPT, bool ZAFFINE>
 __global__ void __launch_bounds__(256) bp_kernel(BpArgs a)
 {
     __shared__ float4 s_coef[kViewsPerChunk * kC / 4];
+    __shared__ int s_cls[kViewsPerChunk];
+    __shared__ BlockBox s_box;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    bp_column<FAMILY, Q, ZPT, ZAFFINE>(a, i, j, blockIdx.z * ZPT, i < a.nx && j < a.ny, kViewsPerChunk, s_coef,
+    const int k0 = blockIdx.z * ZPT;
+    if (threadIdx.x == 0 && threadIdx.y == 0)
+        s_box = block_box(a, blockIdx.x * blockDim.x, blockIdx.y * blockDim.y, blockDim.x, blockDim.y, k0, ZPT);
+    // the first barrier of bp_column orders this store before any read
+    bp_column<FAMILY, Q, ZPT, ZAFFINE>(a, i, j, k0, i < a.nx && j < a.ny, kViewsPerChunk, s_coef, s_cls, &s_box,
                                        threadIdx.y * blockDim.x + threadIdx.x, blockDim.x * blockDim.y,
                                        a.accumulate ? kBpAccumulate : kBpStore);
 }
@@ -301,23 +373,27 @@ void launch_q(const BpArgs &a, bool z_affine, int zpt, int bx, int by, cudaStrea
 // ---- work-queue backprojection -----------------------------------------------------------
 
 template <int FAMILY, class Q, int ZPT>
-__device__ __forceinline__ void queue_tile_z(const BpItem &it, const BpArgs &a, int i, int j, int k0, bool active,
-                                             int vps, float4 *s_coef, int tid, int mode)
+__device__ __forceinline__ void queue_tile_z(const BpItem &it, const BpArgs &a, int tx, int ty, int tz, int tid,
+                                             int mode, float4 *s_coef, int *s_cls, BlockBox *s_box)
 {
+    const int i0 = tx * it.bx, j0 = ty * it.by, k0 = tz * ZPT;
+    const int i = i0 + tid % it.bx, j = j0 + tid / it.bx;
+    const bool active = i < a.nx && j < a.ny;
+    if (tid == 0) *s_box = block_box(a, i0, j0, it.bx, it.by, k0, ZPT);  // ordered by bp_column's first barrier
     if (FAMILY == 0 || it.z_affine)
-        bp_column<FAMILY, Q, ZPT, true>(a, i, j, k0, active, vps, s_coef, tid, kQueueThreads, mode);
+        bp_column<FAMILY, Q, ZPT, true>(a, i, j, k0, active, it.vps, s_coef, s_cls, s_box, tid, kQueueThreads, mode);
     else
-        bp_column<FAMILY, Q, ZPT, false>(a, i, j, k0, active, vps, s_coef, tid, kQueueThreads, mode);
+        bp_column<FAMILY, Q, ZPT, false>(a, i, j, k0, active, it.vps, s_coef, s_cls, s_box, tid, kQueueThreads, mode);
 }
 
 template <int FAMILY, class Q>
-__device__ __forceinline__ void queue_tile(const BpItem &it, const BpArgs &a, int i, int j, int tz, bool active,
-                                           int vps, float4 *s_coef, int tid, int mode)
+__device__ __forceinline__ void queue_tile(const BpItem &it, const BpArgs &a, int tx, int ty, int tz, int tid,
+                                           int mode, float4 *s_coef, int *s_cls, BlockBox *s_box)
 {
     switch (it.zpt) {
-        case 1: queue_tile_z<FAMILY, Q, 1>(it, a, i, j, tz, active, vps, s_coef, tid, mode); break;
-        case 4: queue_tile_z<FAMILY, Q, 4>(it, a, i, j, tz * 4, active, vps, s_coef, tid, mode); break;
-        default: queue_tile_z<FAMILY, Q, 8>(it, a, i, j, tz * 8, active, vps, s_coef, tid, mode); break;
+        case 1: queue_tile_z<FAMILY, Q, 1>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, s_box); break;
+        case 4: queue_tile_z<FAMILY, Q, 4>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, s_box); break;
+        default: queue_tile_z<FAMILY, Q, 8>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, s_box); break;
     }
 }
 
@@ -330,6 +406,8 @@ __global__ void __launch_bounds__(kQueueThreads, kQueueMinBlocks) bp_queue_kerne
                                                                  int *counter)
 {
     __shared__ float4 s_coef[kQueueMaxVps * kC / 4];
+    __shared__ int s_cls[kQueueMaxVps];
+    __shared__ BlockBox s_box;
     __shared__ BpItem s_item;
     __shared__ BpWork s_work;
     __shared__ int s_next;
@@ -349,14 +427,11 @@ __global__ void __launch_bounds__(kQueueThreads, kQueueMinBlocks) bp_queue_kerne
         a.v_begin = s_work.v_begin;
         a.v_count = s_work.v_count;
         const int mode = s_work.mode;
-        const int vps = it.vps;
         const int t = s_work.tile;
         const int tx = t % it.tiles_x, ty = (t / it.tiles_x) % it.tiles_y, tz = t / (it.tiles_x * it.tiles_y);
-        const int i = tx * it.bx + tid % it.bx, j = ty * it.by + tid / it.bx;
-        const bool active = i < a.nx && j < a.ny;
-        if (it.family == 0) queue_tile<0, Q>(it, a, i, j, tz, active, vps, s_coef, tid, mode);
-        else if (it.family == 1) queue_tile<1, Q>(it, a, i, j, tz, active, vps, s_coef, tid, mode);
-        else queue_tile<2, Q>(it, a, i, j, tz, active, vps, s_coef, tid, mode);
+        if (it.family == 0) queue_tile<0, Q>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, &s_box);
+        else if (it.family == 1) queue_tile<1, Q>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, &s_box);
+        else queue_tile<2, Q>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, &s_box);
         __syncthreads();  // s_item / s_work / s_next are rewritten for the next entry
     }
 }
