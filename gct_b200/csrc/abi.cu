@@ -165,15 +165,15 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
     }
     // backprojection launch shape
     const bool vol3d = gct::is_2d_detector(kind);
-    // measured on B200 (512^3, 720 views): 8 voxels per thread for FP16 quads (1758 GUPS; 16: 1338),
-    // 16 for FP32 quads (1274 GUPS; 8: 1196)
-    const int zpt3d = p->opts.storage == GCT_STORAGE_F16 ? 8 : 16;
+    // measured on B200 (512^3, 720 views, with the per-block view classes): 16 voxels per thread
+    // with 8 x 16 blocks for FP16 quads (2047 GUPS; 8 voxels: 1855, 32: 1543) and with 4 x 16 blocks
+    // for FP32 quads (1466 GUPS; 8 voxels on 4 x 32: 1425)
+    const bool f16 = p->opts.storage == GCT_STORAGE_F16;
+    const int zpt3d = 16;
     p->zpt = p->opts.z_per_thread > 0 ? p->opts.z_per_thread : (vol3d ? zpt3d : 1);
     if (p->zpt != 1 && p->zpt != 2 && p->zpt != 4 && p->zpt != 8 && p->zpt != 16)
         gct::fail(GCT_ERR_INVALID_ARG, "z_per_thread must be 1, 2, 4, 8 or 16");
-    // measured on B200 (512^3, 720 views): 8 x 16 threads per block with 8 voxels per thread was
-    // fastest for both storages (FP16 1753 GUPS, FP32 1188 GUPS; 8 x 32: 1723 / 1156)
-    p->bx = p->opts.block_x > 0 ? p->opts.block_x : (vol3d ? 8 : 32);
+    p->bx = p->opts.block_x > 0 ? p->opts.block_x : (vol3d ? (f16 ? 8 : 4) : 32);
     p->by = p->opts.block_y > 0 ? p->opts.block_y : (vol3d ? 16 : 8);
     if (p->bx * p->by > 256 || p->bx * p->by < 32)
         gct::fail(GCT_ERR_INVALID_ARG, "backprojection block must hold 32..256 threads");

@@ -372,8 +372,10 @@ void launch_q(const BpArgs &a, bool z_affine, int zpt, int bx, int by, cudaStrea
 
 // ---- work-queue backprojection -----------------------------------------------------------
 
+// Not inlined: each (family, storage, z depth) path gets its own register allocation instead of
+// the union of all paths; the call happens once per work entry.
 template <int FAMILY, class Q, int ZPT>
-__device__ __forceinline__ void queue_tile_z(const BpItem &it, const BpArgs &a, int tx, int ty, int tz, int tid,
+__device__ __noinline__ void queue_tile_z(const BpItem &it, const BpArgs &a, int tx, int ty, int tz, int tid,
                                              int mode, float4 *s_coef, int *s_cls, BlockBox *s_box)
 {
     const int i0 = tx * it.bx, j0 = ty * it.by, k0 = tz * ZPT;
@@ -386,24 +388,28 @@ __device__ __forceinline__ void queue_tile_z(const BpItem &it, const BpArgs &a, 
         bp_column<FAMILY, Q, ZPT, false>(a, i, j, k0, active, it.vps, s_coef, s_cls, s_box, tid, kQueueThreads, mode);
 }
 
-template <int FAMILY, class Q>
+template <int FAMILY, class Q, int ZC>
 __device__ __forceinline__ void queue_tile(const BpItem &it, const BpArgs &a, int tx, int ty, int tz, int tid,
                                            int mode, float4 *s_coef, int *s_cls, BlockBox *s_box)
 {
+    if constexpr (ZC == 0) {
+        queue_tile_z<FAMILY, Q, 1>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, s_box);
+        return;
+    }
     switch (it.zpt) {
         case 1: queue_tile_z<FAMILY, Q, 1>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, s_box); break;
         case 4: queue_tile_z<FAMILY, Q, 4>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, s_box); break;
-        default: queue_tile_z<FAMILY, Q, 8>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, s_box); break;
+        case 8: queue_tile_z<FAMILY, Q, 8>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, s_box); break;
+        default: queue_tile_z<FAMILY, Q, 16>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, s_box); break;
     }
 }
 
 // Persistent blocks take work entries in queue order from a global counter; each entry is one
 // tile of one reconstruction over a range of views. The item descriptor is read once per entry
 // into shared memory; all control flow below depends only on it, so it is uniform per block.
-template <class Q>
-__global__ void __launch_bounds__(kQueueThreads, kQueueMinBlocks) bp_queue_kernel(const BpItem *__restrict__ items,
-                                                                 const BpWork *__restrict__ work, int n_work,
-                                                                 int *counter)
+template <class Q, int ZC>
+__global__ void __launch_bounds__(kQueueThreads, ZC == 0 ? 4 : 2)
+    bp_queue_kernel(const BpItem *__restrict__ items, const BpWork *__restrict__ work, int n_work, int *counter)
 {
     __shared__ float4 s_coef[kQueueMaxVps * kC / 4];
     __shared__ int s_cls[kQueueMaxVps];
@@ -429,31 +435,38 @@ __global__ void __launch_bounds__(kQueueThreads, kQueueMinBlocks) bp_queue_kerne
         const int mode = s_work.mode;
         const int t = s_work.tile;
         const int tx = t % it.tiles_x, ty = (t / it.tiles_x) % it.tiles_y, tz = t / (it.tiles_x * it.tiles_y);
-        if (it.family == 0) queue_tile<0, Q>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, &s_box);
-        else if (it.family == 1) queue_tile<1, Q>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, &s_box);
-        else queue_tile<2, Q>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, &s_box);
+        if (it.family == 0) queue_tile<0, Q, ZC>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, &s_box);
+        else if (it.family == 1) queue_tile<1, Q, ZC>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, &s_box);
+        else queue_tile<2, Q, ZC>(it, a, tx, ty, tz, tid, mode, s_coef, s_cls, &s_box);
         __syncthreads();  // s_item / s_work / s_next are rewritten for the next entry
     }
 }
 
 }  // namespace
 
-int queue_blocks_per_sm(int storage)
+int queue_blocks_per_sm(int storage, int zclass)
 {
     int n = 0;
-    const cudaError_t e = storage == 0
-        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bp_queue_kernel<QuadF32>, kQueueThreads, 0)
-        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bp_queue_kernel<QuadF16>, kQueueThreads, 0);
+    cudaError_t e;
+    if (storage == 0)
+        e = zclass == 0 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bp_queue_kernel<QuadF32, 0>, kQueueThreads, 0)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bp_queue_kernel<QuadF32, 1>, kQueueThreads, 0);
+    else
+        e = zclass == 0 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bp_queue_kernel<QuadF16, 0>, kQueueThreads, 0)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bp_queue_kernel<QuadF16, 1>, kQueueThreads, 0);
     return e == cudaSuccess ? n : 0;
 }
 
 void launch_backproject_queue(const BpItem *items, const BpWork *work, int n_work, int *counter, int storage,
-                              int grid, cudaStream_t s)
+                              int zclass, int grid, cudaStream_t s)
 {
-    if (storage == 0)
-        bp_queue_kernel<QuadF32><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter);
-    else
-        bp_queue_kernel<QuadF16><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter);
+    if (storage == 0) {
+        if (zclass == 0) bp_queue_kernel<QuadF32, 0><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter);
+        else bp_queue_kernel<QuadF32, 1><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter);
+    } else {
+        if (zclass == 0) bp_queue_kernel<QuadF16, 0><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter);
+        else bp_queue_kernel<QuadF16, 1><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter);
+    }
 }
 
 void launch_backproject(const BpArgs &a, int family, int storage, bool z_affine, int zpt, int bx,

@@ -28,7 +28,7 @@ bool vol3d(const gct_fdk_plan *p) { return p->vol.nz > 1 || is_2d_detector(p->ki
 BpItem make_item(const gct_fdk_plan *p, const StackRef &st, float *vol, const TileConfig &c)
 {
     if (c.bx * c.by != kQueueThreads || c.bx < 1 || !queue_zpt_ok(c.zpt) || c.vps < 1 || c.vps > kQueueMaxVps)
-        fail(GCT_ERR_INVALID_ARG, "queue tile shape must cover 256 threads with z per thread 1, 4 or 8");
+        fail(GCT_ERR_INVALID_ARG, "queue tile shape must cover 256 threads with z per thread 1, 4, 8 or 16");
     BpItem it;
     it.a = bp_args(p, st, vol, 0, p->nv);
     it.family = static_cast<int>(p->family);
@@ -70,7 +70,7 @@ std::vector<TileConfig> shape_candidates(bool three_d)
 {
     std::vector<TileConfig> c;
     if (three_d) {
-        for (int zpt : {4, 8})
+        for (int zpt : {8, 16})
             for (auto b : {std::make_pair(8, 32), std::make_pair(16, 16), std::make_pair(32, 8)})
                 c.push_back({zpt, b.first, b.second, 32});
     } else {
@@ -87,10 +87,13 @@ struct QueueScratch {
     DevBuf<int> counter;
 };
 
-// Updates per second of one configuration: all tiles of the item over its first views.
-double time_config(const gct_fdk_plan *p, const StackRef &st, float *vol, const TileConfig &c, int grid,
+// Updates per second of one configuration: all tiles of the item over its first views, on the
+// grid of the configuration's queue kernel.
+double time_config(const gct_fdk_plan *p, const StackRef &st, float *vol, const TileConfig &c, int num_sms,
                    QueueScratch &sc, cudaStream_t s)
 {
+    const int zc = queue_class(c.zpt);
+    const int grid = std::max(1, queue_blocks_per_sm(p->opts.storage, zc)) * num_sms;
     const BpItem it = make_item(p, st, vol, c);
     const int nvt = std::min(p->nv, 64);
     const std::vector<BpWork> w = tile_entries(0, item_tiles(it), 0, nvt, kBpStore);
@@ -104,7 +107,7 @@ double time_config(const gct_fdk_plan *p, const StackRef &st, float *vol, const 
     for (int rep = 0; rep < 3; ++rep) {  // the first run warms up
         cuda_check(cudaMemsetAsync(sc.counter.p, 0, sizeof(int), s), "counter reset");
         cuda_check(cudaEventRecord(e0, s), "event record");
-        launch_backproject_queue(sc.item.p, sc.work.p, static_cast<int>(w.size()), sc.counter.p, p->opts.storage,
+        launch_backproject_queue(sc.item.p, sc.work.p, static_cast<int>(w.size()), sc.counter.p, p->opts.storage, zc,
                                  grid, s);
         cuda_check(cudaGetLastError(), "autotune launch");
         cuda_check(cudaEventRecord(e1, s), "event record");
@@ -122,19 +125,19 @@ double time_config(const gct_fdk_plan *p, const StackRef &st, float *vol, const 
 std::mutex g_tune_mu;
 std::map<std::string, Tuned> g_tune_cache;
 
-std::string tune_key(const gct_fdk_plan *p, int grid)
+std::string tune_key(const gct_fdk_plan *p, int num_sms)
 {
     return std::to_string(p->device) + "/" + std::to_string(static_cast<int>(p->kind)) + "/" +
            std::to_string(p->opts.storage) + "/" + std::to_string(p->z_affine) + "/" + std::to_string(p->vol.nx) +
            "x" + std::to_string(p->vol.ny) + "x" + std::to_string(p->vol.nz) + "/" + std::to_string(p->nr) + "x" +
-           std::to_string(p->nc) + "/" + std::to_string(grid);
+           std::to_string(p->nc) + "/" + std::to_string(num_sms);
 }
 
 }  // namespace
 
-Tuned autotune(const gct_fdk_plan *p, const StackRef &st, float *vol, int grid, cudaStream_t s)
+Tuned autotune(const gct_fdk_plan *p, const StackRef &st, float *vol, int num_sms, cudaStream_t s)
 {
-    const std::string key = tune_key(p, grid);
+    const std::string key = tune_key(p, num_sms);
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         auto it = g_tune_cache.find(key);
@@ -143,13 +146,13 @@ Tuned autotune(const gct_fdk_plan *p, const StackRef &st, float *vol, int grid, 
     QueueScratch sc;
     Tuned best;
     for (const TileConfig &c : shape_candidates(vol3d(p))) {
-        const double ups = time_config(p, st, vol, c, grid, sc, s);
+        const double ups = time_config(p, st, vol, c, num_sms, sc, s);
         if (ups > best.ups) best = {c, ups};
     }
     for (int vps : {16, 64}) {
         TileConfig c = best.cfg;
         c.vps = vps;
-        const double ups = time_config(p, st, vol, c, grid, sc, s);
+        const double ups = time_config(p, st, vol, c, num_sms, sc, s);
         if (ups > best.ups) best = {c, ups};
     }
     std::lock_guard<std::mutex> lock(g_tune_mu);
@@ -175,14 +178,14 @@ struct gct_fdk_batch {
     int num_sms = 148;
     bool use_graph = true;
     std::vector<std::unique_ptr<Item>> items;
-    // one queue per storage type present: [0] FP32 quads, [1] FP16 quads
+    // one queue per storage type and depth class present: index 2 * storage + class
     struct Queue {
         DevBuf<gct::BpItem> d_items;
         DevBuf<gct::BpWork> d_work;
         int n_work = 0;
         int grid = 0;
         std::vector<int> atomic_items;  // items whose volumes start at zero (view-split)
-    } queue[2];
+    } queue[2 * gct::kQueueClasses];
     DevBuf<int> counters;  // one per queue
     unsigned long long updates = 0;
     std::vector<cudaStream_t> side;
@@ -233,7 +236,7 @@ void issue(gct_fdk_batch *b, cudaStream_t s)
         cuda_check(cudaEventRecord(join, b->side[k]), "event record");
         cuda_check(cudaStreamWaitEvent(s, join, 0), "stream wait");
     }
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < 2 * kQueueClasses; ++q) {
         const auto &Q = b->queue[q];
         if (Q.n_work == 0) continue;
         for (int i : Q.atomic_items) {
@@ -242,7 +245,8 @@ void issue(gct_fdk_batch *b, cudaStream_t s)
                        "volume reset");
         }
         cuda_check(cudaMemsetAsync(b->counters.p + q, 0, sizeof(int), s), "queue counter reset");
-        launch_backproject_queue(Q.d_items.p, Q.d_work.p, Q.n_work, b->counters.p + q, q, Q.grid, s);
+        launch_backproject_queue(Q.d_items.p, Q.d_work.p, Q.n_work, b->counters.p + q, q / kQueueClasses,
+                                 q % kQueueClasses, Q.grid, s);
         cuda_check(cudaGetLastError(), "queue backprojection launch");
     }
 }
@@ -289,15 +293,14 @@ void build_batch(gct_fdk_batch *b, const gct_batch_item *items, uint32_t n, cons
     cuda_check(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking), "capture stream");
 
     // tile configurations
-    for (int q = 0; q < 2; ++q) {
-        int bps = bps_opt > 0 ? bps_opt : queue_blocks_per_sm(q);
+    for (int q = 0; q < 2 * kQueueClasses; ++q) {
+        int bps = bps_opt > 0 ? bps_opt : queue_blocks_per_sm(q / kQueueClasses, q % kQueueClasses);
         if (bps <= 0) bps = 1;
         b->queue[q].grid = bps * b->num_sms;
     }
     for (auto &ip : b->items) {
-        const int q = ip->plan->opts.storage == GCT_STORAGE_F16 ? 1 : 0;
         if (tune) {
-            const Tuned t = autotune(ip->plan, ip->st, ip->vol, b->queue[q].grid, b->cap);
+            const Tuned t = autotune(ip->plan, ip->st, ip->vol, b->num_sms, b->cap);
             ip->cfg = t.cfg;
             ip->tuned_ups = t.ups;
         } else {
@@ -307,11 +310,14 @@ void build_batch(gct_fdk_batch *b, const gct_batch_item *items, uint32_t n, cons
 
     // work queues: items by decreasing cost; an item whose single tile costs more than an even
     // share of the queue over 8 entries per block is split into view chunks (atomic adds)
-    for (int q = 0; q < 2; ++q) {
+    auto queue_of = [&](const gct_fdk_batch::Item &it) {
+        return (it.plan->opts.storage == GCT_STORAGE_F16 ? 1 : 0) * kQueueClasses + queue_class(it.cfg.zpt);
+    };
+    for (int q = 0; q < 2 * kQueueClasses; ++q) {
         auto &Q = b->queue[q];
         std::vector<int> idx;
         for (int i = 0; i < static_cast<int>(b->items.size()); ++i)
-            if ((b->items[i]->plan->opts.storage == GCT_STORAGE_F16 ? 1 : 0) == q) idx.push_back(i);
+            if (queue_of(*b->items[i]) == q) idx.push_back(i);
         if (idx.empty()) continue;
         std::vector<BpItem> qitems;
         std::vector<double> cost;
@@ -353,7 +359,7 @@ void build_batch(gct_fdk_batch *b, const gct_batch_item *items, uint32_t n, cons
         Q.d_work.upload(work.data(), work.size(), "queue work");
         Q.n_work = static_cast<int>(work.size());
     }
-    b->counters.alloc(2, "queue counters");
+    b->counters.alloc(2 * kQueueClasses, "queue counters");
 
     if (b->use_graph) {
         cuda_check(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal), "graph capture begin");
@@ -427,7 +433,9 @@ gct_status gct_fdk_batch_work(const gct_fdk_batch *batch, uint64_t *work_entries
     return guarded([&] {
         if (!batch) gct::fail(GCT_ERR_INVALID_ARG, "NULL batch");
         if (work_entries)
-            *work_entries = static_cast<uint64_t>(batch->queue[0].n_work) + static_cast<uint64_t>(batch->queue[1].n_work);
+            *work_entries = 0;
+        for (const auto &q : batch->queue)
+            if (work_entries) *work_entries += static_cast<uint64_t>(q.n_work);
         if (updates) *updates = batch->updates;
     });
 }

@@ -74,15 +74,19 @@ struct BpWork {
     int mode = kBpStore;
 };
 constexpr int kQueueThreads = 256;
-constexpr int kQueueMinBlocks = 3;  // resident blocks per SM the register budget is sized for
 constexpr int kQueueMaxVps = 64;    // views of coefficients staged per block barrier, at most
-// Supported z-per-thread values of the queue kernel.
-inline bool queue_zpt_ok(int zpt) { return zpt == 1 || zpt == 4 || zpt == 8; }
-// Blocks of the queue kernel resident per SM for the storage type (0 f32, 1 f16).
-int queue_blocks_per_sm(int storage);
+// Supported z-per-thread values of the queue kernels.
+inline bool queue_zpt_ok(int zpt) { return zpt == 1 || zpt == 4 || zpt == 8 || zpt == 16; }
+// Queue kernels by depth class, each compiled with its own register budget: class 0 runs tiles of
+// one voxel per thread along z (2D images; needs many resident warps to hide its gather latency),
+// class 1 tiles of 4, 8 or 16 (volumes; needs registers for its accumulators).
+constexpr int kQueueClasses = 2;
+inline int queue_class(int zpt) { return zpt == 1 ? 0 : 1; }
+// Blocks of a queue kernel resident per SM for the storage type (0 f32, 1 f16) and depth class.
+int queue_blocks_per_sm(int storage, int zclass);
 // Launches grid blocks that take work entries [0, n_work) in order from *counter (zeroed by the
-// caller before the launch) until none are left.
+// caller before the launch) until none are left. Every entry's item must be of the depth class.
 void launch_backproject_queue(const BpItem *items, const BpWork *work, int n_work, int *counter, int storage,
-                              int grid, cudaStream_t s);
+                              int zclass, int grid, cudaStream_t s);
 
 }  // namespace gct

@@ -31,9 +31,9 @@ long long item_tiles(const BpItem &it);
 std::vector<BpWork> tile_entries(int item, long long tiles, int vb, int vc, int mode);
 // The fixed shape used when autotuning is off: 8 x 32 x 8 voxels (3D) or 32 x 8 pixels (2D).
 TileConfig default_config(const gct_fdk_plan *p);
-// Best tile shape for the plan's kind, storage, grid and detector sizes: every candidate is timed
-// with the queue kernel over all tiles and the first 64 views (writing into `vol`), once per
+// Best tile shape for the plan's kind, storage and sizes: every candidate is timed with its depth
+// class's queue kernel over all tiles and the first 64 views (writing into `vol`), once per
 // process, device and shape; later calls return the cached choice.
-Tuned autotune(const gct_fdk_plan *p, const StackRef &st, float *vol, int grid, cudaStream_t s);
+Tuned autotune(const gct_fdk_plan *p, const StackRef &st, float *vol, int num_sms, cudaStream_t s);
 
 }  // namespace gct

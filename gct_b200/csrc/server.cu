@@ -3,7 +3,8 @@
 // One worker thread per server drives four streams: uploads, filter stages, backprojection
 // rounds and downloads. Admission is first-come first-served against a device memory budget
 // reserved once (Arena) and a cap on admitted requests. Each backprojection round is one launch
-// of the work-queue kernel (per storage type) over the tiles of every active request, each
+// of the work-queue kernel (per storage type and depth class) over the tiles of every active
+// request, each
 // request contributing its next chunk of views; chunk 0 overwrites the volume and later chunks
 // add to it in view order, so a result does not depend on which other requests share the rounds.
 // Two rounds are in flight at most (double-buffered work lists in pinned host memory).
@@ -92,7 +93,7 @@ struct gct_fdk_server {
     DevBuf<unsigned char> budget;
     gct::Arena arena;
     cudaStream_t s_in = nullptr, s_prep = nullptr, s_bp = nullptr, s_out = nullptr;
-    int grid[2] = {0, 0};
+    int grid[2 * gct::kQueueClasses] = {};
 
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -210,9 +211,8 @@ void start(gct_fdk_server *s, Request *r)
 
 void activate(gct_fdk_server *s, Request *r)
 {
-    const int q = r->plan->opts.storage == GCT_STORAGE_F16 ? 1 : 0;
     cuda_check(cudaStreamWaitEvent(s->s_bp, r->e_prep, 0), "stream wait");
-    r->cfg = s->autotune ? gct::autotune(r->plan, r->st, r->vol_dev, s->grid[q], s->s_bp).cfg
+    r->cfg = s->autotune ? gct::autotune(r->plan, r->st, r->vol_dev, s->num_sms, s->s_bp).cfg
                          : gct::default_config(r->plan);
     s->active.push_back(r);
 }
@@ -222,11 +222,13 @@ void run_round(gct_fdk_server *s)
 {
     auto &sl = s->slot[s->round % 2];
     if (sl.used) cuda_check(cudaEventSynchronize(sl.done), "round slot");
-    std::vector<gct::BpItem> items[2];
-    std::vector<gct::BpWork> work[2];
+    constexpr int NQ = 2 * gct::kQueueClasses;  // index 2 * storage + depth class
+    std::vector<gct::BpItem> items[NQ];
+    std::vector<gct::BpWork> work[NQ];
     std::vector<std::pair<Request *, int>> advanced;
     for (Request *r : s->active) {
-        const int q = r->plan->opts.storage == GCT_STORAGE_F16 ? 1 : 0;
+        const int q = (r->plan->opts.storage == GCT_STORAGE_F16 ? 1 : 0) * gct::kQueueClasses +
+                      gct::queue_class(r->cfg.zpt);
         const int vb = r->next_view, vc = std::min(r->chunk, r->plan->nv - vb);
         const gct::BpItem it = gct::make_item(r->plan, r->st, r->vol_dev, r->cfg);
         const int idx = static_cast<int>(items[q].size());
@@ -235,28 +237,35 @@ void run_round(gct_fdk_server *s)
         work[q].insert(work[q].end(), w.begin(), w.end());
         advanced.emplace_back(r, vc);
     }
-    const size_t ni = items[0].size() + items[1].size(), nw = work[0].size() + work[1].size();
+    size_t ni = 0, nw = 0;
+    for (int q = 0; q < NQ; ++q) {
+        ni += items[q].size();
+        nw += work[q].size();
+    }
     if (sl.items.n < ni) sl.items.alloc(ni, "round items");
     if (sl.work.n < nw) sl.work.alloc(nw, "round work");
-    if (!sl.counters.p) sl.counters.alloc(2, "round counters");
+    if (!sl.counters.p) sl.counters.alloc(NQ, "round counters");
     sl.h_items.reserve(ni * sizeof(gct::BpItem));
     sl.h_work.reserve(nw * sizeof(gct::BpWork));
     auto *hi = static_cast<gct::BpItem *>(sl.h_items.p);
     auto *hw = static_cast<gct::BpWork *>(sl.h_work.p);
-    std::copy(items[0].begin(), items[0].end(), hi);
-    std::copy(items[1].begin(), items[1].end(), hi + items[0].size());
-    std::copy(work[0].begin(), work[0].end(), hw);
-    std::copy(work[1].begin(), work[1].end(), hw + work[0].size());
+    for (int q = 0, io = 0, wo = 0; q < NQ; ++q) {
+        std::copy(items[q].begin(), items[q].end(), hi + io);
+        std::copy(work[q].begin(), work[q].end(), hw + wo);
+        io += static_cast<int>(items[q].size());
+        wo += static_cast<int>(work[q].size());
+    }
     cuda_check(cudaMemcpyAsync(sl.items.p, hi, ni * sizeof(gct::BpItem), cudaMemcpyHostToDevice, s->s_bp),
                "round items upload");
     cuda_check(cudaMemcpyAsync(sl.work.p, hw, nw * sizeof(gct::BpWork), cudaMemcpyHostToDevice, s->s_bp),
                "round work upload");
-    cuda_check(cudaMemsetAsync(sl.counters.p, 0, 2 * sizeof(int), s->s_bp), "round counters");
+    cuda_check(cudaMemsetAsync(sl.counters.p, 0, NQ * sizeof(int), s->s_bp), "round counters");
     size_t item_off = 0, work_off = 0;
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < NQ; ++q) {
         if (!work[q].empty()) {
             gct::launch_backproject_queue(sl.items.p + item_off, sl.work.p + work_off, static_cast<int>(work[q].size()),
-                                          sl.counters.p + q, q, s->grid[q], s->s_bp);
+                                          sl.counters.p + q, q / gct::kQueueClasses, q % gct::kQueueClasses,
+                                          s->grid[q], s->s_bp);
             cuda_check(cudaGetLastError(), "round launch");
         }
         item_off += items[q].size();
@@ -372,7 +381,8 @@ void create_server(gct_fdk_server *s, const gct_server_opts *o)
     cudaDeviceProp prop{};
     cuda_check(cudaGetDeviceProperties(&prop, s->device), "cudaGetDeviceProperties");
     s->num_sms = prop.multiProcessorCount;
-    for (int q = 0; q < 2; ++q) s->grid[q] = std::max(1, gct::queue_blocks_per_sm(q)) * s->num_sms;
+    for (int q = 0; q < 2 * gct::kQueueClasses; ++q)
+        s->grid[q] = std::max(1, gct::queue_blocks_per_sm(q / gct::kQueueClasses, q % gct::kQueueClasses)) * s->num_sms;
     s->budget.alloc(o->memory_budget_bytes, "server memory budget");
     s->arena.reset(o->memory_budget_bytes);
     for (cudaStream_t *st : {&s->s_in, &s->s_prep, &s->s_bp, &s->s_out})

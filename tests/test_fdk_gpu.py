@@ -64,7 +64,7 @@ def test_filter_stage_matches_oracle(kind):
 
 
 @pytest.mark.parametrize("kind", ["fan_arc", "cone_flat", "cone_cyl", "parallel_2d"])
-@pytest.mark.parametrize("zpt", [1, 4, 16])
+@pytest.mark.parametrize("zpt", [1, 4, 8, 16])
 def test_z_per_thread_variants_agree(kind, zpt):
     case = make_case(kind, nz=10)
     proj = oracle_projections(case)
