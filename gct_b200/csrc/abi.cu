@@ -96,6 +96,24 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
     std::vector<double> wscale(p->nv);
     for (int v = 0; v < p->nv; ++v) wscale[v] = dtheta * vd[v].bp_const;
     std::vector<float> coefs = gct::bp_coefficients(p->geom, p->vol, vd, wscale, &p->z_affine);
+    // 1D parallel kind: transpose, so that the detector coordinate u(x, y) = u0 + ui x + uj y becomes
+    // the row coordinate v(i, k) = v0 + vi i + vk k of a one-column detector and image rows run
+    // along the backprojector's z loop
+    p->t1d = kind == GCT_GEOM_PARALLEL_1D;
+    p->kx = static_cast<int>(vol->nx);
+    p->ky = p->t1d ? 1 : static_cast<int>(vol->ny);
+    p->kz = p->t1d ? static_cast<int>(vol->ny) : static_cast<int>(vol->nz);
+    if (p->t1d) {
+        for (int v = 0; v < static_cast<int>(g->num_views); ++v) {
+            float *c = &coefs[static_cast<size_t>(v) * gct::kCoefPerView];
+            const float u0 = c[0], ui = c[1], uj = c[2];
+            c[0] = c[1] = c[2] = 0.0f;  // the single detector column
+            c[3] = u0;
+            c[6] = ui;
+            c[4] = uj;
+            c[7] = 0.0f;
+        }
+    }
 
     std::vector<float4> fview(p->nv);
     for (int v = 0; v < p->nv; ++v)
@@ -169,12 +187,13 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
     // with 8 x 16 blocks for FP16 quads (2047 GUPS; 8 voxels: 1855, 32: 1543) and with 4 x 16 blocks
     // for FP32 quads (1466 GUPS; 8 voxels on 4 x 32: 1425)
     const bool f16 = p->opts.storage == GCT_STORAGE_F16;
+    // the transposed 1D parallel kind loops over image rows: 16 rows per thread, 128 x 1 blocks
     const int zpt3d = 16;
-    p->zpt = p->opts.z_per_thread > 0 ? p->opts.z_per_thread : (vol3d ? zpt3d : 1);
+    p->zpt = p->opts.z_per_thread > 0 ? p->opts.z_per_thread : ((vol3d || p->t1d) ? zpt3d : 1);
     if (p->zpt != 1 && p->zpt != 2 && p->zpt != 4 && p->zpt != 8 && p->zpt != 16)
         gct::fail(GCT_ERR_INVALID_ARG, "z_per_thread must be 1, 2, 4, 8 or 16");
-    p->bx = p->opts.block_x > 0 ? p->opts.block_x : (vol3d ? (f16 ? 8 : 4) : 32);
-    p->by = p->opts.block_y > 0 ? p->opts.block_y : (vol3d ? 16 : 8);
+    p->bx = p->opts.block_x > 0 ? p->opts.block_x : (p->t1d ? 128 : vol3d ? (f16 ? 8 : 4) : 32);
+    p->by = p->opts.block_y > 0 ? p->opts.block_y : (p->t1d ? 1 : vol3d ? 16 : 8);
     if (p->bx * p->by > 256 || p->bx * p->by < 32)
         gct::fail(GCT_ERR_INVALID_ARG, "backprojection block must hold 32..256 threads");
 }
@@ -228,6 +247,7 @@ void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float 
     qa.nv = vc;
     qa.nr = p->nr;
     qa.nc = p->nc;
+    qa.t1d = p->t1d ? 1 : 0;
     qa.vscale = (mode == gct::kOutQuadF16) ? vscale : nullptr;
     qa.out = out;
     gct::launch_quads_from_rows(qa, mode, p->num_sms, s);
@@ -266,6 +286,7 @@ void run_filter(gct_fdk_plan *p, const float *proj, void *out, const float *vsca
         fa.out = static_cast<unsigned char *>(out) + vb * qview * static_cast<long long>(p->quad_bytes());
     }
     fa.vscale = (mode == gct::kOutQuadF16) ? vscale + vb : nullptr;
+    fa.t1d = (p->t1d && mode != gct::kOutPlainF32) ? 1 : 0;
     gct::launch_filter_fft(fa, static_cast<int>(p->L), p->num_sms, s);
     cuda_check(cudaGetLastError(), "filter kernel launch");
 }
@@ -274,18 +295,19 @@ gct::BpArgs bp_args(const gct_fdk_plan *p, const StackRef &st, float *vol, int v
 {
     gct::BpArgs ba;
     ba.quads = st.quads;
-    ba.qpitch = p->nc + 2 * gct::kQuadPad;
-    ba.qview = static_cast<long long>(p->nr + 2 * gct::kQuadPad) * ba.qpitch;
+    // the quad grid per view holds (nr + 4) x (nc + 4) entries in either orientation
+    ba.qpitch = p->t1d ? gct::kT1dPitch : p->nc + 2 * gct::kQuadPad;
+    ba.qview = static_cast<long long>(p->nr + 2 * gct::kQuadPad) * (p->nc + 2 * gct::kQuadPad);
     ba.coefs = p->coefs.p;
     ba.vinv = st.vinv;
     ba.v_begin = v_begin;
     ba.v_count = v_count;
     ba.vol = vol;
-    ba.nx = static_cast<int>(p->vol.nx);
-    ba.ny = static_cast<int>(p->vol.ny);
-    ba.nz = static_cast<int>(p->vol.nz);
-    ba.umax = static_cast<float>(p->nc);
-    ba.vmax = static_cast<float>(p->nr);
+    ba.nx = p->kx;
+    ba.ny = p->ky;
+    ba.nz = p->kz;
+    ba.umax = static_cast<float>(p->t1d ? 1 : p->nc);
+    ba.vmax = static_cast<float>(p->t1d ? p->nc : p->nr);
     return ba;
 }
 

@@ -32,7 +32,8 @@ constexpr float kShift = 12582912.0f;  // 1.5 * 2^23
 constexpr int kShiftBits = 0x4B400000;  // bit pattern of kShift
 
 // Coefficient layouts (per view, kCoefPerView floats):
-//  affine     : [0..2] u0, ui, uj; [3..4] v0, vk; [5] wscale
+//  affine     : [0..2] u0, ui, uj; [3..4] v0, vk; [5] wscale; [6..7] vi, vj (zero except for the
+//               transposed one-row detector, where v is the detector coordinate)
 //  projective : [0..3] U numerator; [4..7] V numerator; [8..11] denominator D; [12] wscale
 //               u = U/D, v = V/D, weight = wscale / D^2
 //  arc        : [0..3] A = e_u.d; [4..7] B = e_w.d; [8..11] T = e_v.d; [12] 1/dgamma; [13] c0;
@@ -174,8 +175,9 @@ __device__ __forceinline__ int box_class(const float *c, float i0, float i1, flo
         float u, va, vb;
         if (FAMILY == 0) {
             u = fmaf(c[2], fj, fmaf(c[1], fi, c[0]));
-            va = fmaf(c[4], k0, c[3]);
-            vb = fmaf(c[4], k1, c[3]);
+            const float V = fmaf(c[7], fj, fmaf(c[6], fi, c[3]));
+            va = fmaf(c[4], k0, V);
+            vb = fmaf(c[4], k1, V);
         } else {
             const float D = fmaf(c[10], fj, fmaf(c[9], fi, c[8]));
             if (!(D > 0.0f)) return kBoxMixed;
@@ -261,10 +263,10 @@ __device__ __forceinline__ void bp_column(const BpArgs &a, int i, int j, int k0,
             const float *c = reinterpret_cast<const float *>(s_coef) + vv * kC;
             const S *view = quads + static_cast<long long>(a.v_begin + vc + vv) * a.qview;
             if (FAMILY == 0) {
-                // parallel kinds: u = u0 + ui i + uj j, v = v0 + vk k, constant weight
+                // parallel kinds: u = u0 + ui i + uj j, v = v0 + vi i + vj j + vk k, constant weight
                 const float u = fmaf(c[2], fj, fmaf(c[1], fi, c[0]));
-                column_dispatch<L, ZPT>(view, a.qpitch, u, fmaf(c[4], fk0, c[3]), c[4], a.umax, a.vmax,
-                                        ConstWeight{c[5]}, acc, cls);
+                const float v0 = fmaf(c[4], fk0, fmaf(c[7], fj, fmaf(c[6], fi, c[3])));
+                column_dispatch<L, ZPT>(view, a.qpitch, u, v0, c[4], a.umax, a.vmax, ConstWeight{c[5]}, acc, cls);
             } else if (FAMILY == 1) {
                 if (ZAFFINE) {
                     const float D = fmaf(c[10], fj, fmaf(c[9], fi, c[8]));

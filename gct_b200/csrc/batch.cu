@@ -23,7 +23,7 @@
 
 namespace gct {
 
-bool vol3d(const gct_fdk_plan *p) { return p->vol.nz > 1 || is_2d_detector(p->kind); }
+bool vol3d(const gct_fdk_plan *p) { return p->kz > 1 || is_2d_detector(p->kind); }
 
 BpItem make_item(const gct_fdk_plan *p, const StackRef &st, float *vol, const TileConfig &c)
 {
@@ -37,9 +37,9 @@ BpItem make_item(const gct_fdk_plan *p, const StackRef &st, float *vol, const Ti
     it.bx = c.bx;
     it.by = c.by;
     it.vps = c.vps;
-    it.tiles_x = (static_cast<int>(p->vol.nx) + c.bx - 1) / c.bx;
-    it.tiles_y = (static_cast<int>(p->vol.ny) + c.by - 1) / c.by;
-    it.tiles_z = (static_cast<int>(p->vol.nz) + c.zpt - 1) / c.zpt;
+    it.tiles_x = (p->kx + c.bx - 1) / c.bx;
+    it.tiles_y = (p->ky + c.by - 1) / c.by;
+    it.tiles_z = (p->kz + c.zpt - 1) / c.zpt;
     return it;
 }
 
@@ -55,7 +55,11 @@ std::vector<BpWork> tile_entries(int item, long long tiles, int vb, int vc, int 
 TileConfig default_config(const gct_fdk_plan *p)
 {
     TileConfig c;
-    if (!vol3d(p)) {
+    if (p->ky == 1 && vol3d(p)) {  // one row of columns (the transposed 1D parallel kind)
+        c.bx = 256;
+        c.by = 1;
+        c.zpt = 16;
+    } else if (!vol3d(p)) {
         c.zpt = 1;
         c.bx = 32;
         c.by = 8;
@@ -66,10 +70,12 @@ TileConfig default_config(const gct_fdk_plan *p)
 namespace {
 
 // Candidate (zpt, block) shapes; views per stage is tuned afterwards for the best shape.
-std::vector<TileConfig> shape_candidates(bool three_d)
+std::vector<TileConfig> shape_candidates(bool three_d, bool one_row)
 {
     std::vector<TileConfig> c;
-    if (three_d) {
+    if (one_row) {
+        for (int zpt : {8, 16}) c.push_back({zpt, 256, 1, 32});
+    } else if (three_d) {
         for (int zpt : {8, 16})
             for (auto b : {std::make_pair(8, 32), std::make_pair(16, 16), std::make_pair(32, 8)})
                 c.push_back({zpt, b.first, b.second, 32});
@@ -128,8 +134,8 @@ std::map<std::string, Tuned> g_tune_cache;
 std::string tune_key(const gct_fdk_plan *p, int num_sms)
 {
     return std::to_string(p->device) + "/" + std::to_string(static_cast<int>(p->kind)) + "/" +
-           std::to_string(p->opts.storage) + "/" + std::to_string(p->z_affine) + "/" + std::to_string(p->vol.nx) +
-           "x" + std::to_string(p->vol.ny) + "x" + std::to_string(p->vol.nz) + "/" + std::to_string(p->nr) + "x" +
+           std::to_string(p->opts.storage) + "/" + std::to_string(p->z_affine) + "/" + std::to_string(p->kx) +
+           "x" + std::to_string(p->ky) + "x" + std::to_string(p->kz) + "/" + std::to_string(p->nr) + "x" +
            std::to_string(p->nc) + "/" + std::to_string(num_sms);
 }
 
@@ -145,7 +151,7 @@ Tuned autotune(const gct_fdk_plan *p, const StackRef &st, float *vol, int num_sm
     }
     QueueScratch sc;
     Tuned best;
-    for (const TileConfig &c : shape_candidates(vol3d(p))) {
+    for (const TileConfig &c : shape_candidates(vol3d(p), p->ky == 1 && vol3d(p))) {
         const double ups = time_config(p, st, vol, c, num_sms, sc, s);
         if (ups > best.ups) best = {c, ups};
     }

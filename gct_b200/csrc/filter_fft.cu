@@ -165,6 +165,25 @@ __device__ __forceinline__ void write_quad_row(const FilterArgs &a, int v, int r
     }
 }
 
+// Transposed quad grid of view v of a one-row detector from its filtered, scaled row y (shared).
+template <int MODE>
+__device__ __forceinline__ void write_quads_t1d(const FilterArgs &a, int v, const float *y, int tid, int nthr)
+{
+    const int nc = a.nc, rows = nc + 2 * kQuadPad;
+    const long long base = static_cast<long long>(v) * rows * kT1dPitch;
+    auto yv = [&](int r) -> float { return (r >= 0 && r < nc) ? y[r] : 0.0f; };
+    for (int e = tid; e < rows * kT1dPitch; e += nthr) {
+        const int r = e / kT1dPitch - kQuadPad, c = e % kT1dPitch - kQuadPad;
+        const float t = yv(r), b = yv(r + 1);
+        if (c == 0)
+            store_quad<MODE>(a.out, base + e, t, 0.0f, b, 0.0f);
+        else if (c == -1)
+            store_quad<MODE>(a.out, base + e, 0.0f, t, 0.0f, b);
+        else
+            store_quad<MODE>(a.out, base + e, 0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
 template <int LOG2L, int MODE>
 __global__ void __launch_bounds__(256) filter_fft_kernel(FilterArgs a, int seg_rows, int nseg)
 {
@@ -188,7 +207,7 @@ __global__ void __launch_bounds__(256) filter_fft_kernel(FilterArgs a, int seg_r
         const float sc = (quads && a.vscale) ? a.vscale[v] : 1.0f;
         int prev_row = r0 - 1;
         bool have_prev = false;
-        if (quads && s == 0) {
+        if (quads && s == 0 && !a.t1d) {
             write_quad_row<MODE>(a, v, -2, nullptr, nullptr, false, sc, tid, NT);
             for (int c = tid; c < nc; c += NT) yprev[c] = 0.0f;  // row -1 is zero
             have_prev = true;
@@ -244,7 +263,9 @@ __global__ void __launch_bounds__(256) filter_fft_kernel(FilterArgs a, int seg_r
             }
             __syncthreads();
         }
-        if (quads && r1 == nr) {  // last segment: rows nr-1 (bottom neighbour zero), nr and nr+1
+        if (quads && a.t1d) {  // one-row detector: the transposed grid from the filtered row
+            write_quads_t1d<MODE>(a, v, yprev, tid, NT);
+        } else if (quads && r1 == nr) {  // last segment: rows nr-1 (bottom neighbour zero), nr and nr+1
             write_quad_row<MODE>(a, v, nr - 1, yprev, nullptr, false, sc, tid, NT);
             write_quad_row<MODE>(a, v, nr, nullptr, nullptr, false, sc, tid, NT);
             write_quad_row<MODE>(a, v, nr + 1, nullptr, nullptr, false, sc, tid, NT);

@@ -355,6 +355,32 @@ __global__ void split_kernel(SplitArgs a)
 
 // Filtered rows Y (row stride ldy) of views [v0, v0 + nv) -> bilinear-coefficient quads. One
 // block per quad row (view, padded row), threads along the columns.
+// One-row detector: each view's filtered row -> its transposed quad grid, one thread per entry.
+template <int MODE>
+__global__ void quads_t1d_kernel(QuadArgs a)
+{
+    const int rows = a.nc + 2 * kQuadPad;
+    const long long n = static_cast<long long>(a.nv) * rows * kT1dPitch;
+    for (long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e < n;
+         e += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int vl = static_cast<int>(e / (rows * kT1dPitch));
+        const int rem = static_cast<int>(e - static_cast<long long>(vl) * rows * kT1dPitch);
+        const int r = rem / kT1dPitch - kQuadPad, c = rem % kT1dPitch - kQuadPad;
+        const int v = a.v0 + vl;
+        const float sc = a.vscale ? a.vscale[v] : 1.0f;
+        const float *y = a.Y + static_cast<long long>(vl) * a.ldy;
+        const float t = (r >= 0 && r < a.nc) ? sc * __ldg(y + r) : 0.f;
+        const float b = (r + 1 >= 0 && r + 1 < a.nc) ? sc * __ldg(y + r + 1) : 0.f;
+        const float p00 = c == 0 ? t : 0.f, p01 = c == -1 ? t : 0.f;
+        const float p10 = c == 0 ? b : 0.f, p11 = c == -1 ? b : 0.f;
+        const long long q = static_cast<long long>(v) * rows * kT1dPitch + rem;
+        if (MODE == kOutQuadF32)
+            static_cast<float4 *>(a.out)[q] = quad_f32(p00, p01, p10, p11);
+        else
+            static_cast<uint2 *>(a.out)[q] = quad_f16(p00, p01, p10, p11);
+    }
+}
+
 template <int MODE>
 __global__ void quads_from_rows_kernel(QuadArgs a)
 {
@@ -423,6 +449,16 @@ void launch_split(const SplitArgs &a, int num_sms, cudaStream_t s)
 
 void launch_quads_from_rows(const QuadArgs &a, int mode, int num_sms, cudaStream_t s)
 {
+    if (a.t1d) {
+        const long long n = static_cast<long long>(a.nv) * (a.nc + 2 * kQuadPad) * kT1dPitch;
+        long long grid = (n + 255) / 256;
+        if (grid > static_cast<long long>(num_sms) * 32) grid = static_cast<long long>(num_sms) * 32;
+        if (mode == kOutQuadF32)
+            quads_t1d_kernel<kOutQuadF32><<<static_cast<unsigned>(grid < 1 ? 1 : grid), 256, 0, s>>>(a);
+        else
+            quads_t1d_kernel<kOutQuadF16><<<static_cast<unsigned>(grid < 1 ? 1 : grid), 256, 0, s>>>(a);
+        return;
+    }
     long long grid = static_cast<long long>(a.nv) * (a.nr + 2 * kQuadPad);
     if (grid > static_cast<long long>(num_sms) * 32) grid = static_cast<long long>(num_sms) * 32;
     if (mode == kOutQuadF32)

@@ -46,6 +46,7 @@ struct QuadArgs {
     int v0 = 0, nv = 0, nr = 0, nc = 0;
     const float *vscale = nullptr;
     void *out = nullptr;       // quads of the full stack
+    int t1d = 0;               // one-row detector: transposed quad grid (kernels.hpp, kT1dPitch)
 };
 void launch_quads_from_rows(const QuadArgs &a, int mode, int num_sms, cudaStream_t s);
 

@@ -23,7 +23,15 @@ struct FilterArgs {
     int mode = kOutPlainF32;
     void *out = nullptr;           // plain: [nv][nr][nc] f32; quads: [nv][nr+4][nc+4]
     const float *vscale = nullptr; // per-view output scale for quads (nullable = 1)
+    int t1d = 0;                   // one-row detectors: write the transposed quad grid (t1d_quad_layout)
 };
+
+// Transposed quads of a one-row detector (1D parallel kind): the nc cells become the rows of a
+// one-column image, so that the backprojector's row coordinate runs along the image's y axis (an
+// affine function of the thread's loop index) and its column coordinate is the constant 0. Grid
+// per view: (nc + 4) rows x 5 columns, entry (r, c) for r in [-2, nc + 2), c in [-2, 3); the quad
+// at column 0 holds (y[r], 0, y[r + 1], 0) and at column -1 (0, y[r], 0, y[r + 1]).
+constexpr int kT1dPitch = 1 + 2 * kQuadPad;
 
 // Fused cosine + Parker weighting, zero padding, FFT convolution with the ramp filter and the
 // epilogue into the requested layout. L is the power-of-two FFT length.

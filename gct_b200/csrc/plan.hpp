@@ -95,6 +95,10 @@ struct gct_fdk_plan {
     int nv = 0, nr = 0, nc = 0;
     float l1 = 0.f;
     int zpt = 8, bx = 32, by = 8;
+    // One-row 1D parallel detectors run transposed (kT1dPitch): the backprojector sees the image
+    // as kx x 1 x kz voxels (z = image y) over a one-column detector of nc rows.
+    bool t1d = false;
+    int kx = 0, ky = 0, kz = 0;  // backprojector grid (the image's [z][y][x] memory either way)
     DevBuf<float4> fview;
     DevBuf<float> parker;
     DevBuf<float2> H, tw;

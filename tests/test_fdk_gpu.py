@@ -63,7 +63,7 @@ def test_filter_stage_matches_oracle(kind):
     assert rel_rms(out.cpu().numpy(), ref) <= 1e-5
 
 
-@pytest.mark.parametrize("kind", ["fan_arc", "cone_flat", "cone_cyl", "parallel_2d"])
+@pytest.mark.parametrize("kind", ["fan_arc", "cone_flat", "cone_cyl", "parallel_2d", "parallel_1d"])
 @pytest.mark.parametrize("zpt", [1, 4, 8, 16])
 def test_z_per_thread_variants_agree(kind, zpt):
     case = make_case(kind, nz=10)
