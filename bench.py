@@ -347,10 +347,24 @@ def time_plan(plan, proj, vol, steps, warmup, stream, dist):
     filt = float(np.mean([e[0].elapsed_time(e[1]) for e in ev]))
     bp = float(np.mean([e[1].elapsed_time(e[2]) for e in ev]))
     if dist:
-        t = torch.tensor([total], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total = float(t.item())
+        total = max_over_ranks(total, "cuda")
     return total, filt, bp
+
+
+def max_over_ranks(value: float, device) -> float:
+    """The job's time for a per-rank time: the maximum over all ranks (every rank calls this)."""
+    import torch
+    if not (torch.distributed.is_available() and torch.distributed.is_initialized()):
+        return float(value)
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(units_per_rank: float, world: int, steps: int, seconds: float) -> float:
+    """Whole-job rate of `world` independent replicas, each processing units_per_rank per step,
+    over the max-over-ranks time."""
+    return units_per_rank * world * steps / seconds
 
 
 def run_gct(args, cfg, rank, world, local_rank):
@@ -389,7 +403,7 @@ def run_gct(args, cfg, rank, world, local_rank):
         if sampler:
             clocks = sampler.stop()
         results[name] = dict(total=total, filt_ms=filt_ms, bp_ms=bp_ms,
-                             gups=updates * world * args.steps / total / 1e9)
+                             gups=replica_rate(updates, world, args.steps, total) / 1e9)
 
     e2e = None
     if not args.no_e2e:
@@ -407,10 +421,8 @@ def run_gct(args, cfg, rank, world, local_rank):
             plan.execute_host(hp, hv, stream=stream)
         te = time.perf_counter() - t0
         if dist:
-            t = torch.tensor([te], device=device, dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            te = float(t.item())
-        e2e = {"value": updates * world * args.steps / te / 1e9, "unit": "GUPS",
+            te = max_over_ranks(te, device)
+        e2e = {"value": replica_rate(updates, world, args.steps, te) / 1e9, "unit": "GUPS",
                "h2d_bytes_per_step": int(proj.numel() * 4), "d2h_bytes_per_step": int(host_vol.numel() * 4),
                "ms_per_step": 1000.0 * te / args.steps, "path": "gct_fdk_execute_host (pinned host buffers)"}
 
@@ -544,9 +556,7 @@ def device_timed(fn, steps, warmup, stream, dist, device):
         torch.distributed.barrier()
     total = start.elapsed_time(stop) / 1000.0
     if dist:
-        t = torch.tensor([total], device=device, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total = float(t.item())
+        total = max_over_ranks(total, device)
     return total
 
 
@@ -595,7 +605,7 @@ def run_batch(args, rank, world, local_rank):
         return
     line = {
         "metric": "FDK batched backprojection GUPS (voxel x view updates / s), 48 mixed reconstructions",
-        "value": updates * world * args.steps / t_batch / 1e9, "unit": "GUPS", "n_gpus": world,
+        "value": replica_rate(updates, world, args.steps, t_batch) / 1e9, "unit": "GUPS", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_batch / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32-accumulate/f16-storage", "data": "synthetic",
@@ -603,7 +613,7 @@ def run_batch(args, rank, world, local_rank):
                    "filter": "shared-memory FFT", "l2": "inputs larger than L2, no flush",
                    "parallelism": f"replicas x{world}"},
         "recons_per_s": world * len(specs) * args.steps / t_batch,
-        "sequential": {"value": updates * world * args.steps / t_seq / 1e9, "unit": "GUPS",
+        "sequential": {"value": replica_rate(updates, world, args.steps, t_seq) / 1e9, "unit": "GUPS",
                        "ms_per_step": 1000.0 * t_seq / args.steps,
                        "path": "the same 48 plans through gct_fdk_execute one after another"},
         "speedup_batch_vs_sequential": t_seq / t_batch,
