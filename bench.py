@@ -90,6 +90,8 @@ def parse_args():
     ap.add_argument("--mixed-filter", choices=["gemm4", "gemm3", "fft"], default="gemm4",
                     help="ramp filter of the mixed path: split-BF16 Toeplitz GEMM on tcgen05 in the four-term "
                          "form (three pieces of rows and central taps) or three terms, or the FFT")
+    ap.add_argument("--symmetry", choices=["auto", "off", "on"], default="auto",
+                    help="quarter-turn backprojection: auto (FP16 storage, when the scan has it), off, on")
     ap.add_argument("--no-error", action="store_true", help="skip the FP64 oracle error check")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -380,12 +382,14 @@ def run_gct(args, cfg, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     mixed_filter = {"gemm4": g.FILTER_TOEPLITZ_BF16X4, "gemm3": g.FILTER_TOEPLITZ_BF16X3,
                     "fft": g.FILTER_FFT}[args.mixed_filter]
+    sym = {"auto": g.SYMMETRY_AUTO, "off": g.SYMMETRY_OFF, "on": g.SYMMETRY_ON}[args.symmetry]
     plans = {
         "mixed": g.FdkPlan(cg, vg, opts=g.FdkOptions(filter=mixed_filter, storage=g.STORAGE_F16,
-                                                     z_per_thread=args.zpt)),
+                                                     z_per_thread=args.zpt, symmetry=sym)),
         "fp32": g.FdkPlan(cg, vg, opts=g.FdkOptions(filter=g.FILTER_FFT, storage=g.STORAGE_F32,
-                                                    z_per_thread=args.zpt)),
+                                                    z_per_thread=args.zpt, symmetry=sym)),
     }
+    mixed_quarter_turn = plans["mixed"].quarter_turn
     vols = {k: torch.empty(vg.shape, dtype=torch.float32, device=device) for k in plans}
     for k, p in plans.items():
         p.execute(proj, vols[k], stream=stream)
@@ -440,7 +444,10 @@ def run_gct(args, cfg, rank, world, local_rank):
     mixed = results["mixed"]
     bytes_per_update = 8  # four FP16 bilinear taps
     achieved = updates * bytes_per_update / (mixed["bp_ms"] / 1000.0) / 1e9
-    traffic = profiled_traffic(f"backproject_{args.config}_f16.md")
+    quarter = mixed_quarter_turn
+    bp_label = ("backproject, quarter-turn partners (FP16 quads, bp_sym_kernel)" if quarter
+                else "backproject (FP16 quads, bp_kernel)")
+    traffic = profiled_traffic(f"backproject_{'sym_' if quarter else ''}{args.config}_f16.md")
     line = {
         "metric": "FDK backprojection GUPS (voxel x view updates / s), mixed precision", "value": mixed["gups"],
         "unit": "GUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -452,19 +459,19 @@ def run_gct(args, cfg, rank, world, local_rank):
                    "parallelism": f"replicas x{world}"},
         "recons_per_s": world * args.steps / mixed["total"],
         "stages_ms": {"filter": mixed["filt_ms"], "backproject": mixed["bp_ms"]},
+        "quarter_turn": {"mixed": mixed_quarter_turn, "fp32": plans["fp32"].quarter_turn},
         "fp32": {"value": results["fp32"]["gups"], "unit": "GUPS",
                  "recons_per_s": world * args.steps / results["fp32"]["total"],
                  "stages_ms": {"filter": results["fp32"]["filt_ms"], "backproject": results["fp32"]["bp_ms"]}},
         "speedup_mixed_vs_fp32": mixed["gups"] / results["fp32"]["gups"],
         "error_vs_fp64_oracle": ({"voxels": nsamp, **errors} if errors else None),
-        "roofline": {"bound": "hbm", "kernel": "backproject (FP16 quads)", "achieved": achieved, "peak": hbm,
+        "roofline": {"bound": "hbm", "kernel": bp_label, "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_kind,
                      "algorithmic_bytes_per_update": bytes_per_update,
                      "traffic": traffic},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "clocks": clocks,
-        # per mixed step: view max, view scale, (split, GEMM, quads | FFT filter), backprojection
         # per mixed step: view max, view scale, (split, GEMM, quads | FFT filter), backprojection
         "gpu_launches": (4 if args.mixed_filter == "fft" else 6) * args.steps,
         "mixed_filter": {"gemm4": "split-BF16 Toeplitz GEMM on tcgen05, 4 terms + banded 5th (rows and central "

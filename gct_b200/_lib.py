@@ -68,7 +68,8 @@ class gct_geom_params(C.Structure):
 
 class gct_fdk_opts(C.Structure):
     _fields_ = [("filter", C.c_int32), ("storage", C.c_int32), ("z_per_thread", C.c_int32),
-                ("block_x", C.c_int32), ("block_y", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("block_x", C.c_int32), ("block_y", C.c_int32), ("symmetry", C.c_int32),
+                ("reserved", C.c_int32 * 2)]
 
 
 class gct_batch_item(C.Structure):
@@ -126,6 +127,7 @@ SIGNATURES = {
     "gct_fdk_plan_destroy": [VP],
     "gct_fdk_plan_check": [VP],
     "gct_fdk_plan_workspace_bytes": [VP, P(C.c_uint64)],
+    "gct_fdk_plan_symmetry": [VP, P(C.c_int32)],
     "gct_fdk_execute": [VP, VP, VP, VP, VP],
     "gct_fdk_filter": [VP, VP, VP, VP],
     "gct_fdk_prepare": [VP, VP, VP, C.c_uint32, C.c_uint32, VP],

@@ -138,8 +138,8 @@ constexpr int kBoxOff = 0, kBoxInside = 1, kBoxMixed = 2;
 // cls == kBoxInside skips the per-column range tests: box_class has shown, with a margin, that
 // every column of the block passes them, so the result is the same as with the tests.
 template <class L, int ZPT, class W>
-__device__ __forceinline__ void column_dispatch(const typename L::S *view, int qpitch, float u, float v0, float vs,
-                                                float umax, float vmax, const W &wt, float (&acc)[ZPT],
+__device__ __forceinline__ void column_dispatch(const typename L::S *view, int es, int qpitch, float u, float v0,
+                                                float vs, float umax, float vmax, const W &wt, float (&acc)[ZPT],
                                                 int cls = kBoxMixed)
 {
     if (cls != kBoxInside && !(u >= -1.0f && u <= umax)) return;  // the column's rays miss the detector: zero
@@ -149,9 +149,9 @@ __device__ __forceinline__ void column_dispatch(const typename L::S *view, int q
     const float va = v0, vb = fmaf(vs, static_cast<float>(ZPT - 1), v0);
     const float lo = fminf(va, vb), hi = fmaxf(va, vb);
     if (cls != kBoxInside && (hi < -1.0f || lo > vmax)) return;  // the whole segment is off the detector
-    const int stride = qpitch * static_cast<int>(sizeof(typename L::S));
+    const int stride = qpitch * es * static_cast<int>(sizeof(typename L::S));
     const unsigned long long base =
-        reinterpret_cast<unsigned long long>(view + iu + kQuadPad) -
+        reinterpret_cast<unsigned long long>(view + (iu + kQuadPad) * es) -
         static_cast<unsigned long long>(static_cast<long long>(kShiftBits - kQuadPad) * stride);
     const typename L::U fuc = L::ucol(fu);
     if (cls == kBoxInside || (lo >= -1.0f && hi <= vmax))
@@ -200,7 +200,7 @@ __device__ __forceinline__ int box_class(const float *c, float i0, float i1, flo
 
 // Clamped bilinear sample at (u, v) for the per-voxel (non-z-affine) kernels.
 template <class L>
-__device__ __forceinline__ float sample(const typename L::S *view, int qpitch, float u, float v, float umax,
+__device__ __forceinline__ float sample(const typename L::S *view, int es, int qpitch, float u, float v, float umax,
                                         float vmax)
 {
     u = fminf(fmaxf(u, -1.0f), umax);
@@ -211,7 +211,8 @@ __device__ __forceinline__ float sample(const typename L::S *view, int qpitch, f
     const float t = vm + kShift;
     const int iv = __float_as_int(t) - kShiftBits;
     const float fvc = vm - (t - kShift);
-    return L::lerp(__ldg(view + (iv + kQuadPad) * qpitch + iu + kQuadPad), L::ucol(fu), fvc);
+    return L::lerp(__ldg(view + static_cast<long long>((iv + kQuadPad) * qpitch + iu + kQuadPad) * es), L::ucol(fu),
+                   fvc);
 }
 
 // Backprojects views [a.v_begin, a.v_begin + a.v_count) into the column segment (i, j, k0 ..
@@ -225,7 +226,8 @@ struct BlockBox {
     float i0, i1, j0, j1, k0, k1;
 };
 
-template <int FAMILY, class Q, int ZPT, bool ZAFFINE>
+// ES is the entry step of the stack's quad_layout: 1 view-major, 4 interleaved partner views.
+template <int FAMILY, class Q, int ZPT, bool ZAFFINE, int ES = 1>
 __device__ __forceinline__ void bp_column(const BpArgs &a, int i, int j, int k0, bool active, int vps,
                                           float4 *s_coef, int *s_cls, const BlockBox *s_box, int tid, int nthr,
                                           int mode)
@@ -261,19 +263,21 @@ __device__ __forceinline__ void bp_column(const BpArgs &a, int i, int j, int k0,
             const int cls = kClassify ? s_cls[vv] : kBoxMixed;
             if (cls == kBoxOff) continue;  // exact: every column of the block would add zero
             const float *c = reinterpret_cast<const float *>(s_coef) + vv * kC;
-            const S *view = quads + static_cast<long long>(a.v_begin + vc + vv) * a.qview;
+            const long long v = a.v_begin + vc + vv;
+            const S *view = ES == 1 ? quads + v * a.qview : quads + ((v % a.quarter) * a.qview * 4 + v / a.quarter);
+            constexpr int es = ES;
             if (FAMILY == 0) {
                 // parallel kinds: u = u0 + ui i + uj j, v = v0 + vi i + vj j + vk k, constant weight
                 const float u = fmaf(c[2], fj, fmaf(c[1], fi, c[0]));
                 const float v0 = fmaf(c[4], fk0, fmaf(c[7], fj, fmaf(c[6], fi, c[3])));
-                column_dispatch<L, ZPT>(view, a.qpitch, u, v0, c[4], a.umax, a.vmax, ConstWeight{c[5]}, acc, cls);
+                column_dispatch<L, ZPT>(view, es, a.qpitch, u, v0, c[4], a.umax, a.vmax, ConstWeight{c[5]}, acc, cls);
             } else if (FAMILY == 1) {
                 if (ZAFFINE) {
                     const float D = fmaf(c[10], fj, fmaf(c[9], fi, c[8]));
                     const float inv = rcp_approx(D);
                     const float u = fmaf(c[2], fj, fmaf(c[1], fi, c[0])) * inv;
                     const float v0 = fmaf(c[7], fk0, fmaf(c[6], fj, fmaf(c[5], fi, c[4]))) * inv;
-                    column_dispatch<L, ZPT>(view, a.qpitch, u, v0, c[7] * inv, a.umax, a.vmax,
+                    column_dispatch<L, ZPT>(view, es, a.qpitch, u, v0, c[7] * inv, a.umax, a.vmax,
                                             ConstWeight{c[12] * inv * inv}, acc, cls);
                 } else {
 #pragma unroll
@@ -283,7 +287,7 @@ __device__ __forceinline__ void bp_column(const BpArgs &a, int i, int j, int k0,
                         const float inv = rcp_approx(D);
                         const float u = fmaf(c[3], fk, fmaf(c[2], fj, fmaf(c[1], fi, c[0]))) * inv;
                         const float v = fmaf(c[7], fk, fmaf(c[6], fj, fmaf(c[5], fi, c[4]))) * inv;
-                        acc[z] = fmaf(c[12] * inv * inv, sample<L>(view, a.qpitch, u, v, a.umax, a.vmax), acc[z]);
+                        acc[z] = fmaf(c[12] * inv * inv, sample<L>(view, es, a.qpitch, u, v, a.umax, a.vmax), acc[z]);
                     }
                 }
             } else {
@@ -294,7 +298,7 @@ __device__ __forceinline__ void bp_column(const BpArgs &a, int i, int j, int k0,
                     const float u = fmaf(atan2f(A, B), c[12], c[13]);
                     const float vsr = c[14] * rsqrtf(rho2);
                     const float T0 = fmaf(c[11], fk0, c[8]);
-                    column_dispatch<L, ZPT>(view, a.qpitch, u, fmaf(vsr, T0, c[15]), vsr * c[11], a.umax, a.vmax,
+                    column_dispatch<L, ZPT>(view, es, a.qpitch, u, fmaf(vsr, T0, c[15]), vsr * c[11], a.umax, a.vmax,
                                             ArcWeight{c[16], rho2, T0, c[11]}, acc);
                 } else {
 #pragma unroll
@@ -307,7 +311,7 @@ __device__ __forceinline__ void bp_column(const BpArgs &a, int i, int j, int k0,
                         const float u = fmaf(atan2f(A, B), c[12], c[13]);
                         const float v = fmaf(c[14] * rsqrtf(rho2), T, c[15]);
                         const float w = c[16] * rcp_approx(fmaf(T, T, rho2));
-                        acc[z] = fmaf(w, sample<L>(view, a.qpitch, u, v, a.umax, a.vmax), acc[z]);
+                        acc[z] = fmaf(w, sample<L>(view, es, a.qpitch, u, v, a.umax, a.vmax), acc[z]);
                     }
                 }
             }
@@ -332,7 +336,7 @@ __device__ __forceinline__ BlockBox block_box(const BpArgs &a, int i0, int j0, i
                     static_cast<float>(k0 + zpt - 1)};
 }
 
-template <int FAMILY, class Q, int ZPT, bool ZAFFINE>
+template <int FAMILY, class Q, int ZPT, bool ZAFFINE, int ES>
 __global__ void __launch_bounds__(256) bp_kernel(BpArgs a)
 {
     __shared__ float4 s_coef[kViewsPerChunk * kC / 4];
@@ -344,7 +348,7 @@ __global__ void __launch_bounds__(256) bp_kernel(BpArgs a)
     if (threadIdx.x == 0 && threadIdx.y == 0)
         s_box = block_box(a, blockIdx.x * blockDim.x, blockIdx.y * blockDim.y, blockDim.x, blockDim.y, k0, ZPT);
     // the first barrier of bp_column orders this store before any read
-    bp_column<FAMILY, Q, ZPT, ZAFFINE>(a, i, j, k0, i < a.nx && j < a.ny, kViewsPerChunk, s_coef, s_cls, &s_box,
+    bp_column<FAMILY, Q, ZPT, ZAFFINE, ES>(a, i, j, k0, i < a.nx && j < a.ny, kViewsPerChunk, s_coef, s_cls, &s_box,
                                        threadIdx.y * blockDim.x + threadIdx.x, blockDim.x * blockDim.y,
                                        a.accumulate ? kBpAccumulate : kBpStore);
 }
@@ -352,10 +356,12 @@ __global__ void __launch_bounds__(256) bp_kernel(BpArgs a)
 template <int FAMILY, class Q, int ZPT>
 void launch_zpt(const BpArgs &a, bool z_affine, dim3 grid, dim3 block, cudaStream_t s)
 {
-    if (z_affine || FAMILY == 0)
-        bp_kernel<FAMILY, Q, ZPT, true><<<grid, block, 0, s>>>(a);
+    if (a.quarter)  // interleaved partner views: quarter-turn plans, which are z-affine
+        bp_kernel<FAMILY, Q, ZPT, true, 4><<<grid, block, 0, s>>>(a);
+    else if (z_affine || FAMILY == 0)
+        bp_kernel<FAMILY, Q, ZPT, true, 1><<<grid, block, 0, s>>>(a);
     else
-        bp_kernel<FAMILY, Q, ZPT, false><<<grid, block, 0, s>>>(a);
+        bp_kernel<FAMILY, Q, ZPT, false, 1><<<grid, block, 0, s>>>(a);
 }
 
 template <int FAMILY, class Q>
@@ -369,6 +375,285 @@ void launch_q(const BpArgs &a, bool z_affine, int zpt, int bx, int by, cudaStrea
         case 4: launch_zpt<FAMILY, Q, 4>(a, z_affine, grid, block, s); break;
         case 8: launch_zpt<FAMILY, Q, 8>(a, z_affine, grid, block, s); break;
         default: launch_zpt<FAMILY, Q, 16>(a, z_affine, grid, block, s); break;
+    }
+}
+
+// ---- quarter-turn backprojection -----------------------------------------------------------
+//
+// On a full circular scan whose views come in quarter-turn partners (view v + q m, m = nv / 4, is
+// view v turned by q quarter turns about the rotation axis) and a square, centred grid of even
+// side n, view v + q m samples voxel column R^q(x) exactly where view v samples column x (R is a
+// quarter turn of the grid, (i, j) -> (n-1-j, i) or (j, n-1-i); the host checks every view in
+// FP64). A thread owns the four columns R^k(c), k = 0..3, of one first-quadrant column c. Per base
+// view v it evaluates the detector coordinates of each of its columns (u, the weight, the row
+// coordinates, their split and the quad offsets), and the evaluation at R^k(c) serves all four
+// partners: partner q samples there for column R^(k+q)(c). The coordinate work is thus done once
+// per four voxel-view updates; the loads, blends and accumulates are per update.
+
+// Weight of partner q at voxel z: the partner's scale times a factor common to the four.
+struct ConstWeight4 {
+    float w[4];
+    __device__ __forceinline__ float at(int q, int) const { return w[q]; }
+};
+struct ArcWeight4 {
+    float ws[4];
+    float rho2, T0, tk;
+    __device__ __forceinline__ float at(int q, int z) const
+    {
+        const float T = fmaf(tk, static_cast<float>(z), T0);
+        return ws[q] * rcp_approx(fmaf(T, T, rho2));
+    }
+};
+
+// The four partner quads of one detector position in the quarter-turn layout (quad_layout): 32
+// bytes (FP16) or 64 bytes (FP32), 32-byte aligned, read through the non-coherent path.
+__device__ __forceinline__ void ldg_partners(unsigned long long p, uint2 (&o)[4])
+{
+    asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(o[0].x), "=r"(o[0].y), "=r"(o[1].x), "=r"(o[1].y), "=r"(o[2].x), "=r"(o[2].y), "=r"(o[3].x),
+          "=r"(o[3].y)
+        : "l"(p));
+}
+__device__ __forceinline__ void ldg_partners(unsigned long long p, float4 (&o)[4])
+{
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(o[0].x), "=f"(o[0].y), "=f"(o[0].z), "=f"(o[0].w), "=f"(o[1].x), "=f"(o[1].y), "=f"(o[1].z),
+          "=f"(o[1].w)
+        : "l"(p));
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8+32];"
+        : "=f"(o[2].x), "=f"(o[2].y), "=f"(o[2].z), "=f"(o[2].w), "=f"(o[3].x), "=f"(o[3].y), "=f"(o[3].z),
+          "=f"(o[3].w)
+        : "l"(p));
+}
+
+// column() for the four partners of one evaluation: `base` addresses the partner groups as in
+// column(), and partner q accumulates into column (K + q) mod 4.
+template <class L, int ZPT, int K, bool CLAMP, class W>
+__device__ __forceinline__ void column4(unsigned long long base, int stride, typename L::U fu, float vm0, float vs,
+                                        float vmax, const W &wt, float (&acc)[4][ZPT])
+{
+    if constexpr (ZPT % 2 == 0) {
+        const float2 shift = make_float2(kShift, kShift), mshift = make_float2(-kShift, -kShift);
+        const float2 vs2 = make_float2(vs, vs), vm02 = make_float2(vm0, vm0);
+#pragma unroll
+        for (int z = 0; z < ZPT; z += 2) {
+            float2 vm = __ffma2_rn(vs2, make_float2(static_cast<float>(z), static_cast<float>(z + 1)), vm02);
+            if (CLAMP) {
+                vm.x = fminf(fmaxf(vm.x, -1.5f), vmax - 0.5f);
+                vm.y = fminf(fmaxf(vm.y, -1.5f), vmax - 0.5f);
+            }
+            const float2 t = __fadd2_rn(vm, shift);
+            const float2 fl = __fadd2_rn(t, mshift);
+            const float2 fvc = __ffma2_rn(fl, make_float2(-1.0f, -1.0f), vm);
+            typename L::S q0[4], q1[4];
+            ldg_partners(base + static_cast<unsigned long long>(static_cast<long long>(__float_as_int(t.x)) * stride), q0);
+            ldg_partners(base + static_cast<unsigned long long>(static_cast<long long>(__float_as_int(t.y)) * stride), q1);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float2 val = make_float2(L::lerp(q0[q], fu, fvc.x), L::lerp(q1[q], fu, fvc.y));
+                float(&dst)[ZPT] = acc[(K + q) & 3];
+                const float2 r =
+                    __ffma2_rn(make_float2(wt.at(q, z), wt.at(q, z + 1)), val, make_float2(dst[z], dst[z + 1]));
+                dst[z] = r.x;
+                dst[z + 1] = r.y;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int z = 0; z < ZPT; ++z) {
+            float vm = fmaf(vs, static_cast<float>(z), vm0);
+            if (CLAMP) vm = fminf(fmaxf(vm, -1.5f), vmax - 0.5f);
+            const float t = vm + kShift;
+            const float fvc = vm - (t - kShift);
+            typename L::S qv[4];
+            ldg_partners(base + static_cast<unsigned long long>(static_cast<long long>(__float_as_int(t)) * stride), qv);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                acc[(K + q) & 3][z] = fmaf(wt.at(q, z), L::lerp(qv[q], fu, fvc), acc[(K + q) & 3][z]);
+        }
+    }
+}
+
+// column_dispatch() for the four partners of one evaluation; group0 is the base view's grid of
+// partner groups (four quads per detector position).
+template <class L, int ZPT, int K, class W>
+__device__ __forceinline__ void column4_dispatch(const typename L::S *group0, int qpitch, float u, float v0, float vs,
+                                                 float umax, float vmax, const W &wt, float (&acc)[4][ZPT], int cls)
+{
+    if (cls != kBoxInside && !(u >= -1.0f && u <= umax)) return;
+    int iu;
+    float fu;
+    split_coord(u, iu, fu);
+    const float va = v0, vb = fmaf(vs, static_cast<float>(ZPT - 1), v0);
+    const float lo = fminf(va, vb), hi = fmaxf(va, vb);
+    if (cls != kBoxInside && (hi < -1.0f || lo > vmax)) return;
+    const int stride = qpitch * 4 * static_cast<int>(sizeof(typename L::S));
+    const unsigned long long base = reinterpret_cast<unsigned long long>(group0 + (iu + kQuadPad) * 4) -
+                                    static_cast<unsigned long long>(static_cast<long long>(kShiftBits - kQuadPad) * stride);
+    const typename L::U fuc = L::ucol(fu);
+    if (cls == kBoxInside || (lo >= -1.0f && hi <= vmax))
+        column4<L, ZPT, K, false>(base, stride, fuc, v0 - 0.5f, vs, vmax, wt, acc);
+    else
+        column4<L, ZPT, K, true>(base, stride, fuc, v0 - 0.5f, vs, vmax, wt, acc);
+}
+
+// One quarter turn of column (i, j) on a grid of side n: (n-1-j, i) for sym = +1, (j, n-1-i)
+// for sym = -1.
+__device__ __forceinline__ void turn(int sym, int n, int &i, int &j)
+{
+    const int ti = sym > 0 ? n - 1 - j : j, tj = sym > 0 ? i : n - 1 - i;
+    i = ti;
+    j = tj;
+}
+// The same turn of the index box [b.x, b.y] x [b.z, b.w].
+__device__ __forceinline__ float4 turn_box(int sym, int n, float4 b)
+{
+    const float m = static_cast<float>(n - 1);
+    return sym > 0 ? make_float4(m - b.w, m - b.z, b.x, b.y) : make_float4(b.z, b.w, m - b.y, m - b.x);
+}
+
+// Base view c (coefficients), evaluated at column (fi, fj) = R^K(c) of the thread; w holds the
+// partners' weight scales.
+template <int FAMILY, class L, int ZPT, int K>
+__device__ __forceinline__ void sym_rotation(const BpArgs &a, const float *c, float4 w, const typename L::S *group0,
+                                             float fi, float fj, float fk0, int cls, float (&acc)[4][ZPT])
+{
+    if (cls == kBoxOff) return;
+    if (FAMILY == 0) {
+        const float u = fmaf(c[2], fj, fmaf(c[1], fi, c[0]));
+        const float v0 = fmaf(c[4], fk0, fmaf(c[7], fj, fmaf(c[6], fi, c[3])));
+        column4_dispatch<L, ZPT, K>(group0, a.qpitch, u, v0, c[4], a.umax, a.vmax,
+                                    ConstWeight4{{w.x, w.y, w.z, w.w}}, acc, cls);
+    } else if (FAMILY == 1) {
+        const float D = fmaf(c[10], fj, fmaf(c[9], fi, c[8]));
+        const float inv = rcp_approx(D);
+        const float u = fmaf(c[2], fj, fmaf(c[1], fi, c[0])) * inv;
+        const float v0 = fmaf(c[7], fk0, fmaf(c[6], fj, fmaf(c[5], fi, c[4]))) * inv;
+        const float i2 = inv * inv;
+        column4_dispatch<L, ZPT, K>(group0, a.qpitch, u, v0, c[7] * inv, a.umax, a.vmax,
+                                    ConstWeight4{{w.x * i2, w.y * i2, w.z * i2, w.w * i2}}, acc, cls);
+    } else {
+        const float A = fmaf(c[2], fj, fmaf(c[1], fi, c[0]));
+        const float B = fmaf(c[6], fj, fmaf(c[5], fi, c[4]));
+        const float rho2 = fmaf(A, A, B * B);
+        const float u = fmaf(atan2f(A, B), c[12], c[13]);
+        const float vsr = c[14] * rsqrtf(rho2);
+        const float T0 = fmaf(c[11], fk0, c[8]);
+        column4_dispatch<L, ZPT, K>(group0, a.qpitch, u, fmaf(vsr, T0, c[15]), vsr * c[11], a.umax, a.vmax,
+                                    ArcWeight4{{w.x, w.y, w.z, w.w}, rho2, T0, c[11]}, acc, cls);
+    }
+}
+
+template <int FAMILY, class Q, int ZPT>
+__global__ void __launch_bounds__(256) bp_sym_kernel(BpArgs a)
+{
+    using L = typename LerpOf<Q>::type;
+    using S = typename L::S;
+    constexpr bool kClassify = FAMILY != 2;
+    __shared__ float4 s_coef[kViewsPerChunk * kC / 4];
+    __shared__ float4 s_w[kViewsPerChunk];  // weight scales of the four partners of each base view
+    __shared__ int s_cls[kViewsPerChunk];   // box class of each of the block's four turned boxes, 2 bits each
+    const int n = a.nx, h = n / 2;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k0 = blockIdx.z * ZPT;
+    const bool active = i < h && j < h;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nthr = blockDim.x * blockDim.y;
+    const float fk0 = static_cast<float>(k0);
+    const S *quads = static_cast<const S *>(a.quads);
+    const int wslot = wscale_slot(FAMILY);
+
+    // the thread's four columns and the block's four boxes (active columns only)
+    float fi[4], fj[4];
+    {
+        int ti = i, tj = j;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            fi[k] = static_cast<float>(ti);
+            fj[k] = static_cast<float>(tj);
+            turn(a.sym, n, ti, tj);
+        }
+    }
+    const int bi0 = blockIdx.x * blockDim.x, bj0 = blockIdx.y * blockDim.y;
+    const float4 box0 = make_float4(static_cast<float>(bi0), static_cast<float>(min(bi0 + static_cast<int>(blockDim.x), h) - 1),
+                                    static_cast<float>(bj0), static_cast<float>(min(bj0 + static_cast<int>(blockDim.y), h) - 1));
+    const float bk0 = fk0, bk1 = static_cast<float>(k0 + ZPT - 1);
+
+    float acc[4][ZPT];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int z = 0; z < ZPT; ++z) acc[q][z] = 0.f;
+
+    for (int vc = 0; vc < a.v_count; vc += kViewsPerChunk) {
+        const int nvc = min(kViewsPerChunk, a.v_count - vc);
+        __syncthreads();
+        const float4 *g = reinterpret_cast<const float4 *>(a.coefs + static_cast<long long>(a.v_begin + vc) * kC);
+        for (int t = tid; t < nvc * kC / 4; t += nthr) s_coef[t] = __ldg(g + t);
+        for (int t = tid; t < nvc; t += nthr) {
+            float w[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const long long v = a.v_begin + vc + t + static_cast<long long>(q) * a.quarter;
+                w[q] = __ldg(a.coefs + v * kC + wslot) * (a.vinv ? __ldg(a.vinv + v) : 1.0f);
+            }
+            s_w[t] = make_float4(w[0], w[1], w[2], w[3]);
+        }
+        __syncthreads();
+        for (int t = tid; t < nvc; t += nthr) {
+            int packed = 0;
+            float4 b = box0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int cls = kClassify ? box_class<FAMILY>(reinterpret_cast<const float *>(s_coef) + t * kC, b.x,
+                                                              b.y, b.z, b.w, bk0, bk1, a.umax, a.vmax)
+                                          : kBoxMixed;
+                packed |= cls << (2 * k);
+                b = turn_box(a.sym, n, b);
+            }
+            s_cls[t] = packed;
+        }
+        __syncthreads();
+        if (!active) continue;
+        for (int vv = 0; vv < nvc; ++vv) {
+            const int packed = s_cls[vv];
+            if (packed == 0) continue;  // every turned box off the detector (kBoxOff == 0)
+            const float *c = reinterpret_cast<const float *>(s_coef) + vv * kC;
+            const float4 w = s_w[vv];
+            // base views are below quarter, so their partner groups start at 4 qview per view
+            const S *group0 = quads + static_cast<long long>(a.v_begin + vc + vv) * a.qview * 4;
+            sym_rotation<FAMILY, L, ZPT, 0>(a, c, w, group0, fi[0], fj[0], fk0, packed & 3, acc);
+            sym_rotation<FAMILY, L, ZPT, 1>(a, c, w, group0, fi[1], fj[1], fk0, (packed >> 2) & 3, acc);
+            sym_rotation<FAMILY, L, ZPT, 2>(a, c, w, group0, fi[2], fj[2], fk0, (packed >> 4) & 3, acc);
+            sym_rotation<FAMILY, L, ZPT, 3>(a, c, w, group0, fi[3], fj[3], fk0, (packed >> 6) & 3, acc);
+        }
+    }
+    if (!active) return;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int ti = static_cast<int>(fi[q]), tj = static_cast<int>(fj[q]);
+#pragma unroll
+        for (int z = 0; z < ZPT; ++z) {
+            const int k = k0 + z;
+            if (k < a.nz) {
+                float *dst = a.vol + (static_cast<long long>(k) * a.ny + tj) * a.nx + ti;
+                *dst = a.accumulate ? *dst + acc[q][z] : acc[q][z];
+            }
+        }
+    }
+}
+
+template <int FAMILY, class Q>
+void launch_sym_q(const BpArgs &a, int zpt, int bx, int by, cudaStream_t s)
+{
+    const int h = a.nx / 2;
+    const dim3 block(bx, by);
+    const dim3 grid((h + bx - 1) / bx, (h + by - 1) / by, (a.nz + zpt - 1) / zpt);
+    switch (zpt) {
+        case 1: bp_sym_kernel<FAMILY, Q, 1><<<grid, block, 0, s>>>(a); break;
+        case 2: bp_sym_kernel<FAMILY, Q, 2><<<grid, block, 0, s>>>(a); break;
+        case 4: bp_sym_kernel<FAMILY, Q, 4><<<grid, block, 0, s>>>(a); break;
+        default: bp_sym_kernel<FAMILY, Q, 8><<<grid, block, 0, s>>>(a); break;
     }
 }
 
@@ -445,6 +730,19 @@ __global__ void __launch_bounds__(kQueueThreads, ZC == 0 ? 4 : 2)
 }
 
 }  // namespace
+
+void launch_backproject_sym(const BpArgs &a, int family, int storage, int zpt, int bx, int by, cudaStream_t s)
+{
+    if (storage == 0) {
+        if (family == 0) launch_sym_q<0, QuadF32>(a, zpt, bx, by, s);
+        else if (family == 1) launch_sym_q<1, QuadF32>(a, zpt, bx, by, s);
+        else launch_sym_q<2, QuadF32>(a, zpt, bx, by, s);
+    } else {
+        if (family == 0) launch_sym_q<0, QuadF16>(a, zpt, bx, by, s);
+        else if (family == 1) launch_sym_q<1, QuadF16>(a, zpt, bx, by, s);
+        else launch_sym_q<2, QuadF16>(a, zpt, bx, by, s);
+    }
+}
 
 int queue_blocks_per_sm(int storage, int zclass)
 {

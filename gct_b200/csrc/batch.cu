@@ -278,7 +278,7 @@ void build_batch(gct_fdk_batch *b, const gct_batch_item *items, uint32_t n, cons
         it->proj = src.proj_dev;
         it->vol = src.vol_dev;
         it->ws.alloc(src.plan->workspace_bytes(), "batch item workspace");
-        it->st = stack_of(src.plan, it->ws.p);
+        it->st = stack_of(src.plan, it->ws.p, true);
         b->items.push_back(std::move(it));
     }
     // filter stages: items of one plan share its filter scratch, so they run on one side stream

@@ -37,14 +37,17 @@ __device__ __forceinline__ float4 quad_f32(float p00, float p01, float p10, floa
 }
 
 // FP16 storage of the same quad: half2 (A, C) in .x and half2 (B, D) in .y.
-__device__ __forceinline__ uint2 quad_f16(float p00, float p01, float p10, float p11)
+__device__ __forceinline__ uint2 quad_f16_of(float4 q)
 {
-    const float4 q = quad_f32(p00, p01, p10, p11);
     const __half2 lo = __floats2half2_rn(q.x, q.z), hi = __floats2half2_rn(q.y, q.w);
     uint2 u;
     u.x = *reinterpret_cast<const unsigned *>(&lo);
     u.y = *reinterpret_cast<const unsigned *>(&hi);
     return u;
+}
+__device__ __forceinline__ uint2 quad_f16(float p00, float p01, float p10, float p11)
+{
+    return quad_f16_of(quad_f32(p00, p01, p10, p11));
 }
 
 // floor(x) and x - floor(x) for |x| < 2^22 with three FP32 adds and one integer subtract:

@@ -152,7 +152,10 @@ __device__ __forceinline__ void write_quad_row(const FilterArgs &a, int v, int r
 {
     const int nc = a.nc;
     const int qpitch = nc + 2 * kQuadPad;
-    const long long row0 = (static_cast<long long>(v) * (a.nr + 2 * kQuadPad) + (r + kQuadPad)) * qpitch;
+    long long first;
+    int step;
+    quad_layout(a.v0 + v, static_cast<long long>(a.nr + 2 * kQuadPad) * qpitch, a.quarter, first, step);
+    const long long row0 = first + static_cast<long long>(r + kQuadPad) * qpitch * step;
     auto tv = [&](int c) -> float { return (top && c >= 0 && c < nc) ? top[c] : 0.0f; };
     auto bv = [&](int c) -> float {
         if (!bot || c < 0 || c >= nc) return 0.0f;
@@ -161,7 +164,7 @@ __device__ __forceinline__ void write_quad_row(const FilterArgs &a, int v, int r
     };
     for (int cq = tid; cq < qpitch; cq += nthr) {
         const int c = cq - kQuadPad;
-        store_quad<MODE>(a.out, row0 + cq, tv(c), tv(c + 1), bv(c), bv(c + 1));
+        store_quad<MODE>(a.out, row0 + static_cast<long long>(cq) * step, tv(c), tv(c + 1), bv(c), bv(c + 1));
     }
 }
 
@@ -170,7 +173,7 @@ template <int MODE>
 __device__ __forceinline__ void write_quads_t1d(const FilterArgs &a, int v, const float *y, int tid, int nthr)
 {
     const int nc = a.nc, rows = nc + 2 * kQuadPad;
-    const long long base = static_cast<long long>(v) * rows * kT1dPitch;
+    const long long base = static_cast<long long>(a.v0 + v) * rows * kT1dPitch;
     auto yv = [&](int r) -> float { return (r >= 0 && r < nc) ? y[r] : 0.0f; };
     for (int e = tid; e < rows * kT1dPitch; e += nthr) {
         const int r = e / kT1dPitch - kQuadPad, c = e % kT1dPitch - kQuadPad;

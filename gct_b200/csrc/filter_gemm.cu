@@ -393,16 +393,73 @@ __global__ void quads_from_rows_kernel(QuadArgs a)
         const float sc = a.vscale ? a.vscale[v] : 1.0f;
         const float *top = (r >= 0 && r < a.nr) ? a.Y + (static_cast<long long>(vl) * a.nr + r) * a.ldy : nullptr;
         const float *bot = (r + 1 >= 0 && r + 1 < a.nr) ? a.Y + (static_cast<long long>(vl) * a.nr + r + 1) * a.ldy : nullptr;
-        const long long qbase = (static_cast<long long>(v) * qrows + (r + kQuadPad)) * qpitch;
+        long long first;
+        int step;
+        quad_layout(v, static_cast<long long>(qrows) * qpitch, a.quarter, first, step);
+        const long long qbase = first + static_cast<long long>(r + kQuadPad) * qpitch * step;
         for (int cq = threadIdx.x; cq < qpitch; cq += blockDim.x) {
             const int c = cq - kQuadPad;
             const bool c0 = c >= 0 && c < a.nc, c1 = c + 1 >= 0 && c + 1 < a.nc;
             const float p00 = (top && c0) ? sc * __ldg(top + c) : 0.f, p01 = (top && c1) ? sc * __ldg(top + c + 1) : 0.f;
             const float p10 = (bot && c0) ? sc * __ldg(bot + c) : 0.f, p11 = (bot && c1) ? sc * __ldg(bot + c + 1) : 0.f;
+            const long long at = qbase + static_cast<long long>(cq) * step;
             if (MODE == kOutQuadF32)
-                static_cast<float4 *>(a.out)[qbase + cq] = quad_f32(p00, p01, p10, p11);
+                static_cast<float4 *>(a.out)[at] = quad_f32(p00, p01, p10, p11);
             else
-                static_cast<uint2 *>(a.out)[qbase + cq] = quad_f16(p00, p01, p10, p11);
+                static_cast<uint2 *>(a.out)[at] = quad_f16(p00, p01, p10, p11);
+        }
+    }
+}
+
+// Quarter-turn stacks (quad_layout with quarter > 0): quads of base views [v0, v0 + nv) and their
+// three partners from the filtered rows of all four (Y holds view v's row r at row v * nr + r).
+// One block per (base view, padded row); each thread writes the whole group of four partner quads
+// of one detector position (32 or 64 contiguous bytes), so the stores stay coalesced.
+template <int MODE>
+__global__ void quads_partners_kernel(QuadArgs a)
+{
+    const int qpitch = a.nc + 2 * kQuadPad, qrows = a.nr + 2 * kQuadPad;
+    const long long nrows = static_cast<long long>(a.nv) * qrows;
+    const long long qview = static_cast<long long>(qrows) * qpitch;
+    for (long long qr = blockIdx.x; qr < nrows; qr += gridDim.x) {
+        const int bl = static_cast<int>(qr / qrows);
+        const int r = static_cast<int>(qr - static_cast<long long>(bl) * qrows) - kQuadPad;
+        const int b = a.v0 + bl;
+        const float *top[4], *bot[4];
+        float sc[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const long long v = b + static_cast<long long>(q) * a.quarter;
+            sc[q] = a.vscale ? a.vscale[v] : 1.0f;
+            top[q] = (r >= 0 && r < a.nr) ? a.Y + (v * a.nr + r) * a.ldy : nullptr;
+            bot[q] = (r + 1 >= 0 && r + 1 < a.nr) ? a.Y + (v * a.nr + r + 1) * a.ldy : nullptr;
+        }
+        const long long gbase = (static_cast<long long>(b) * qview + static_cast<long long>(r + kQuadPad) * qpitch) * 4;
+        for (int cq = threadIdx.x; cq < qpitch; cq += blockDim.x) {
+            const int c = cq - kQuadPad;
+            const bool c0 = c >= 0 && c < a.nc, c1 = c + 1 >= 0 && c + 1 < a.nc;
+            float4 g[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float p00 = (top[q] && c0) ? sc[q] * __ldg(top[q] + c) : 0.f;
+                const float p01 = (top[q] && c1) ? sc[q] * __ldg(top[q] + c + 1) : 0.f;
+                const float p10 = (bot[q] && c0) ? sc[q] * __ldg(bot[q] + c) : 0.f;
+                const float p11 = (bot[q] && c1) ? sc[q] * __ldg(bot[q] + c + 1) : 0.f;
+                g[q] = quad_f32(p00, p01, p10, p11);
+            }
+            const long long at = gbase + static_cast<long long>(cq) * 4;
+            if (MODE == kOutQuadF32) {
+                float4 *o = static_cast<float4 *>(a.out) + at;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) o[q] = g[q];
+            } else {
+                uint2 h[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) h[q] = quad_f16_of(g[q]);
+                uint4 *o = reinterpret_cast<uint4 *>(static_cast<uint2 *>(a.out) + at);
+                o[0] = make_uint4(h[0].x, h[0].y, h[1].x, h[1].y);
+                o[1] = make_uint4(h[2].x, h[2].y, h[3].x, h[3].y);
+            }
         }
     }
 }
@@ -465,6 +522,16 @@ void launch_quads_from_rows(const QuadArgs &a, int mode, int num_sms, cudaStream
         quads_from_rows_kernel<kOutQuadF32><<<static_cast<unsigned>(grid < 1 ? 1 : grid), 256, 0, s>>>(a);
     else
         quads_from_rows_kernel<kOutQuadF16><<<static_cast<unsigned>(grid < 1 ? 1 : grid), 256, 0, s>>>(a);
+}
+
+void launch_quads_partners(const QuadArgs &a, int mode, int num_sms, cudaStream_t s)
+{
+    long long grid = static_cast<long long>(a.nv) * (a.nr + 2 * kQuadPad);
+    if (grid > static_cast<long long>(num_sms) * 32) grid = static_cast<long long>(num_sms) * 32;
+    if (mode == kOutQuadF32)
+        quads_partners_kernel<kOutQuadF32><<<static_cast<unsigned>(grid < 1 ? 1 : grid), 256, 0, s>>>(a);
+    else
+        quads_partners_kernel<kOutQuadF16><<<static_cast<unsigned>(grid < 1 ? 1 : grid), 256, 0, s>>>(a);
 }
 
 cudaError_t launch_toeplitz_gemm(const GemmLaunch &g, int num_sms, cudaStream_t s)

@@ -46,8 +46,12 @@ struct QuadArgs {
     int v0 = 0, nv = 0, nr = 0, nc = 0;
     const float *vscale = nullptr;
     void *out = nullptr;       // quads of the full stack
+    int quarter = 0;           // quad_layout (kernels.hpp)
     int t1d = 0;               // one-row detector: transposed quad grid (kernels.hpp, kT1dPitch)
 };
 void launch_quads_from_rows(const QuadArgs &a, int mode, int num_sms, cudaStream_t s);
+// Quarter-turn stacks: the partner groups of base views [v0, v0 + nv) (quarter = nv of the stack
+// / 4), from rows of all views at their stack positions in Y.
+void launch_quads_partners(const QuadArgs &a, int mode, int num_sms, cudaStream_t s);
 
 }  // namespace gct

@@ -389,7 +389,8 @@ ViewDerived derive_view(gct_geom_kind kind, const gct_ct_geom &g, unsigned vi)
 // DCSToPCS (:142-145): pixel = coord / width + centre.
 std::vector<float> bp_coefficients(const gct_ct_geom &g, const gct_vol_geom &vol,
                                    const std::vector<ViewDerived> &vd,
-                                   const std::vector<double> &wscale, bool *z_affine)
+                                   const std::vector<double> &wscale, bool *z_affine,
+                                   std::vector<double> *c64)
 {
     const auto kind = static_cast<gct_geom_kind>(g.kind);
     const bool vol3d = is_2d_detector(kind);
@@ -399,7 +400,7 @@ std::vector<float> bp_coefficients(const gct_ct_geom &g, const gct_vol_geom &vol
     const double DX[3] = {vol.dx, vol.dy, vol3d ? vol.dz : 0.0};
     const double du = g.det_row.sampling_width;
     const double dv = vol3d ? g.det_col.sampling_width : 1.0;
-    std::vector<float> out(static_cast<size_t>(g.num_views) * kCoefPerView, 0.0f);
+    std::vector<double> cd(static_cast<size_t>(g.num_views) * kCoefPerView, 0.0);
     bool affine_z = true;
     // affine form of e . (X - S): value at (0,0,0) and slopes per index step.
     auto aff = [&](const double *e, const double *S, double *c4) {
@@ -410,15 +411,15 @@ std::vector<float> bp_coefficients(const gct_ct_geom &g, const gct_vol_geom &vol
     };
     for (unsigned v = 0; v < g.num_views; ++v) {
         const ViewDerived &d = vd[v];
-        float *c = &out[static_cast<size_t>(v) * kCoefPerView];
+        double *c = &cd[static_cast<size_t>(v) * kCoefPerView];
         switch (family_of(kind)) {
             case Family::Affine: {
                 // detCoordAxialParallel (coord_trans_proj.cuh:157-166): x cos(t+pi/2) + y sin(t+pi/2).
                 const double t = d.theta + kPi / 2.0;
                 const double ct = std::cos(t), st = std::sin(t);
-                c[0] = static_cast<float>((X0[0] * ct + X0[1] * st) / du + d.c0);
-                c[1] = static_cast<float>(DX[0] * ct / du);
-                c[2] = static_cast<float>(DX[1] * st / du);
+                c[0] = (X0[0] * ct + X0[1] * st) / du + d.c0;
+                c[1] = DX[0] * ct / du;
+                c[2] = DX[1] * st / du;
                 double vk = 0.0, v0 = 0.0;
                 if (kind == GCT_GEOM_PARALLEL_2D) {  // t = -z
                     v0 = -X0[2] / dv + d.r0;
@@ -428,9 +429,9 @@ std::vector<float> bp_coefficients(const gct_ct_geom &g, const gct_vol_geom &vol
                     v0 = -X0[2] * m / dv + d.r0;
                     vk = -DX[2] * m / dv;
                 }
-                c[3] = static_cast<float>(v0);
-                c[4] = static_cast<float>(vk);
-                c[5] = static_cast<float>(wscale[v]);
+                c[3] = v0;
+                c[4] = vk;
+                c[5] = wscale[v];
                 break;
             }
             case Family::Projective: {
@@ -439,11 +440,11 @@ std::vector<float> bp_coefficients(const gct_ct_geom &g, const gct_vol_geom &vol
                 aff(d.ew, d.src, D);
                 if (vol3d) aff(d.ev, d.src, V);
                 for (int i = 0; i < 4; ++i) {
-                    c[i] = static_cast<float>(d.sdd / du * U[i] + d.c0 * D[i]);
-                    c[4 + i] = vol3d ? static_cast<float>(d.sdd / dv * V[i] + d.r0 * D[i]) : 0.0f;
-                    c[8 + i] = static_cast<float>(D[i]);
+                    c[i] = d.sdd / du * U[i] + d.c0 * D[i];
+                    c[4 + i] = vol3d ? d.sdd / dv * V[i] + d.r0 * D[i] : 0.0;
+                    c[8 + i] = D[i];
                 }
-                c[12] = static_cast<float>(wscale[v]);
+                c[12] = wscale[v];
                 if (U[3] != 0.0 || D[3] != 0.0) affine_z = false;
                 break;
             }
@@ -453,22 +454,77 @@ std::vector<float> bp_coefficients(const gct_ct_geom &g, const gct_vol_geom &vol
                 aff(d.ew, d.src, B);
                 if (vol3d) aff(d.ev, d.src, T);
                 for (int i = 0; i < 4; ++i) {
-                    c[i] = static_cast<float>(A[i]);
-                    c[4 + i] = static_cast<float>(B[i]);
-                    c[8 + i] = static_cast<float>(T[i]);
+                    c[i] = A[i];
+                    c[4 + i] = B[i];
+                    c[8 + i] = T[i];
                 }
-                c[12] = static_cast<float>(1.0 / du);
-                c[13] = static_cast<float>(d.c0);
-                c[14] = static_cast<float>(vol3d ? d.sdd / dv : 0.0);
-                c[15] = static_cast<float>(d.r0);
-                c[16] = static_cast<float>(wscale[v]);
+                c[12] = 1.0 / du;
+                c[13] = d.c0;
+                c[14] = vol3d ? d.sdd / dv : 0.0;
+                c[15] = d.r0;
+                c[16] = wscale[v];
                 if (A[3] != 0.0 || B[3] != 0.0 || T[1] != 0.0 || T[2] != 0.0) affine_z = false;
                 break;
             }
         }
     }
     *z_affine = affine_z;
+    std::vector<float> out(cd.size());
+    for (size_t n = 0; n < cd.size(); ++n) out[n] = static_cast<float>(cd[n]);
+    if (c64) *c64 = std::move(cd);
     return out;
+}
+
+int quarter_turn_symmetry(gct_geom_kind kind, const std::vector<double> &c64, unsigned nv, unsigned nx,
+                          unsigned ny, unsigned nz)
+{
+    if (nv < 4 || nv % 4 != 0 || nx != ny || nx % 2 != 0 || c64.size() != static_cast<size_t>(nv) * kCoefPerView)
+        return 0;
+    // Affine forms c0 + ci i + cj j + ck k of each family as slot indices (-1: absent), and the
+    // per-view weight scale, which may differ between partner views. Every other slot must match.
+    struct Form {
+        int c0, ci, cj, ck;
+    };
+    std::vector<Form> forms;
+    int free_slot = -1;
+    switch (family_of(kind)) {
+        case Family::Affine: forms = {{0, 1, 2, -1}, {3, 6, 7, 4}}; free_slot = 5; break;
+        case Family::Projective: forms = {{0, 1, 2, 3}, {4, 5, 6, 7}, {8, 9, 10, 11}}; free_slot = 12; break;
+        case Family::Arc: forms = {{0, 1, 2, 3}, {4, 5, 6, 7}, {8, 9, 10, 11}}; free_slot = 16; break;
+    }
+    bool in_form[kCoefPerView] = {};
+    for (const Form &f : forms)
+        for (int s : {f.c0, f.ci, f.cj, f.ck})
+            if (s >= 0) in_form[s] = true;
+    const double n1 = nx - 1.0, kRel = 1e-9;
+    const unsigned q = nv / 4;
+    for (int dir : {1, -1}) {
+        bool ok = true;
+        for (unsigned v = 0; ok && v + q < nv; ++v) {
+            const double *a = &c64[static_cast<size_t>(v) * kCoefPerView];
+            const double *b = &c64[static_cast<size_t>(v + q) * kCoefPerView];
+            for (const Form &f : forms) {
+                const double c0 = a[f.c0], ci = a[f.ci], cj = a[f.cj], ck = f.ck >= 0 ? a[f.ck] : 0.0;
+                // b's form at R(i, j) equals a's at (i, j): R = (n-1-j, i) for +1, (j, n-1-i) for -1
+                const double e0 = dir > 0 ? c0 + cj * n1 : c0 + ci * n1;
+                const double ei = dir > 0 ? -cj : cj, ej = dir > 0 ? ci : -ci;
+                const double scale = std::max({std::fabs(c0), std::fabs(ci) * nx, std::fabs(cj) * nx,
+                                               std::fabs(ck) * nz, std::fabs(b[f.c0])});
+                const double tol = kRel * scale;
+                if (std::fabs(b[f.c0] - e0) > tol || std::fabs(b[f.ci] - ei) > tol || std::fabs(b[f.cj] - ej) > tol ||
+                    (f.ck >= 0 && std::fabs(b[f.ck] - ck) > tol)) {
+                    ok = false;
+                    break;
+                }
+            }
+            for (int s = 0; ok && s < kCoefPerView; ++s)
+                if (!in_form[s] && s != free_slot &&
+                    std::fabs(a[s] - b[s]) > kRel * std::max(std::fabs(a[s]), std::fabs(b[s])))
+                    ok = false;
+        }
+        if (ok) return dir;
+    }
+    return 0;
 }
 
 }  // namespace gct

@@ -82,6 +82,15 @@ ViewDerived derive_view(gct_geom_kind kind, const gct_ct_geom &g, unsigned v);
 constexpr int kCoefPerView = 20;
 std::vector<float> bp_coefficients(const gct_ct_geom &g, const gct_vol_geom &vol,
                                    const std::vector<ViewDerived> &vd,
-                                   const std::vector<double> &wscale, bool *z_affine);
+                                   const std::vector<double> &wscale, bool *z_affine,
+                                   std::vector<double> *c64 = nullptr);
+
+// Quarter-turn symmetry of a circular scan on a square grid. Returns +1 when, for every view v
+// below 3 nv / 4, view v + nv / 4 maps voxel column R(i, j) = (n - 1 - j, i) exactly where view v
+// maps (i, j) (u, v and the weight up to the per-view weight scale), -1 for the opposite turn
+// R(i, j) = (j, n - 1 - i), and 0 when neither holds (to 1e-9 of each form's range). c64 are the
+// FP64 coefficients of bp_coefficients.
+int quarter_turn_symmetry(gct_geom_kind kind, const std::vector<double> &c64, unsigned nv, unsigned nx,
+                          unsigned ny, unsigned nz);
 
 }  // namespace gct

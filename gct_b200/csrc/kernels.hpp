@@ -21,10 +21,27 @@ struct FilterArgs {
     const float2 *H = nullptr;     // [L] filter spectrum, scaled by 1/L
     const float2 *twiddle = nullptr; // [L] per-stage twiddles: tw[Ns + k] = exp(-2 pi i k / (R Ns))
     int mode = kOutPlainF32;
-    void *out = nullptr;           // plain: [nv][nr][nc] f32; quads: [nv][nr+4][nc+4]
+    void *out = nullptr;           // plain: rows of views [0, nv); quads: view 0 of the stack (quad_layout)
+    int v0 = 0;                    // quads: stack index of the first view filtered
+    int quarter = 0;               // quads: quad_layout's quarter
     const float *vscale = nullptr; // per-view output scale for quads (nullable = 1)
     int t1d = 0;                   // one-row detectors: write the transposed quad grid (t1d_quad_layout)
 };
+
+// Where view v's quad grid (qview entries) lives in a stack: view after view (quarter = 0), or,
+// for quarter-turn plans (quarter = nv / 4), with the four partner views v mod quarter + q quarter
+// (q = 0..3) interleaved entry by entry, so that one 32-byte (FP16) or 64-byte (FP32) load brings
+// all four partners of a detector position. Entry e of view v is at first + e * step.
+__host__ __device__ inline void quad_layout(long long v, long long qview, int quarter, long long &first, int &step)
+{
+    if (quarter == 0) {
+        first = v * qview;
+        step = 1;
+    } else {
+        first = (v % quarter) * qview * 4 + v / quarter;
+        step = 4;
+    }
+}
 
 // Transposed quads of a one-row detector (1D parallel kind): the nc cells become the rows of a
 // one-column image, so that the backprojector's row coordinate runs along the image's y axis (an
@@ -56,12 +73,21 @@ struct BpArgs {
     int nx = 0, ny = 0, nz = 0;
     float umax = 0.f, vmax = 0.f;  // nc, nr
     int accumulate = 0;
+    int quarter = 0;  // quad_layout of the stack
+    // quarter-turn launches (quarter > 0): v_begin / v_count count base views, whose partners are
+    // v + q * quarter (q = 1..3); sym (+1 / -1) is the turn that maps their voxel columns
+    int sym = 0;
 };
 
 // Voxel-driven backprojection. family: 0 affine, 1 projective, 2 arc. storage: 0 f32, 1 f16.
 // z_affine selects the column kernel (u and the denominator constant along z).
 void launch_backproject(const BpArgs &a, int family, int storage, bool z_affine, int zpt,
                         int bx, int by, cudaStream_t s);
+
+// Quarter-turn form (a.sym != 0, z-affine geometries, nx == ny even): threads cover the first
+// quadrant of (x, y) columns; each evaluates the detector coordinates of its column once per base
+// view and accumulates them into the column's four quarter-turn images from the four partner views.
+void launch_backproject_sym(const BpArgs &a, int family, int storage, int zpt, int bx, int by, cudaStream_t s);
 
 // How a block writes its sums: overwrite, add (views processed in order by successive launches)
 // or add atomically (several blocks of one launch share the voxels; the volume starts at zero).

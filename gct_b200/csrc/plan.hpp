@@ -99,6 +99,10 @@ struct gct_fdk_plan {
     // as kx x 1 x kz voxels (z = image y) over a one-column detector of nc rows.
     bool t1d = false;
     int kx = 0, ky = 0, kz = 0;  // backprojector grid (the image's [z][y][x] memory either way)
+    // Quarter-turn symmetry (+1 / -1 / 0, quarter_turn_symmetry): whole-scan backprojections then
+    // run over the first quarter of the views and of the (x, y) columns, each thread serving the
+    // four rotated columns from the four partner views, with zpt_sym voxels along z.
+    int sym = 0, zpt_sym = 8, bx_sym = 8, by_sym = 16;
     DevBuf<float4> fview;
     DevBuf<float> parker;
     DevBuf<float2> H, tw;
@@ -139,12 +143,17 @@ struct gct_fdk_plan {
 struct StackRef {
     unsigned char *quads = nullptr;
     float *amax = nullptr, *vscale = nullptr, *vinv = nullptr;
+    int quarter = 0;  // quad_layout of the quads (kernels.hpp)
 };
 
-inline StackRef stack_of(const gct_fdk_plan *p, void *workspace)
+// A plan's stack in `workspace`. Quarter-turn plans interleave partner views (quad_layout) unless
+// `view_major` asks for the plain layout, which the work-queue backprojector of batches and the
+// server reads.
+inline StackRef stack_of(const gct_fdk_plan *p, void *workspace, bool view_major = false)
 {
     StackRef r;
     r.quads = static_cast<unsigned char *>(workspace);
+    r.quarter = (p->sym && !view_major) ? p->nv / 4 : 0;
     if (p->opts.storage == GCT_STORAGE_F16) {
         r.amax = reinterpret_cast<float *>(r.quads + p->quad_region());
         r.vscale = r.amax + p->nv;
@@ -155,10 +164,15 @@ inline StackRef stack_of(const gct_fdk_plan *p, void *workspace)
 
 // Stage functions (abi.cu). `out` / StackRef bases are view-0 addresses; [vb, vb + vc) is the
 // view range worked on.
-void run_filter(gct_fdk_plan *p, const float *proj, void *out, const float *vscale, int mode, int vb, int vc,
-                cudaStream_t s);
+void run_filter(gct_fdk_plan *p, const float *proj, void *out, const float *vscale, int mode, int quarter, int vb,
+                int vc, cudaStream_t s);
 void prepare(gct_fdk_plan *p, const float *proj, const StackRef &st, int vb, int vc, cudaStream_t s);
+// Quarter-turn stacks (st.quarter > 0): base views [b, b + n) and their partners, through the
+// plan's FP32 row buffer and one coalesced pass that writes the partner groups.
+void prepare_partners(gct_fdk_plan *p, const float *proj, const StackRef &st, int b, int n, cudaStream_t s);
 gct::BpArgs bp_args(const gct_fdk_plan *p, const StackRef &st, float *vol, int v_begin, int v_count);
+void run_backproject_sym(gct_fdk_plan *p, const StackRef &st, float *vol, int b_begin, int b_count,
+                         bool accumulate, cudaStream_t s);
 void run_backproject(gct_fdk_plan *p, const StackRef &st, float *vol, int v_begin, int v_count, bool accumulate,
                      cudaStream_t s);
 void check_range(const gct_fdk_plan *p, uint32_t vb, uint32_t vc);

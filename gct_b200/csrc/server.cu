@@ -197,7 +197,7 @@ void start(gct_fdk_server *s, Request *r)
     r->proj_dev = reinterpret_cast<float *>(base);
     unsigned char *ws = base + gct::Arena::round_up(r->proj_bytes);
     r->vol_dev = reinterpret_cast<float *>(ws + gct::Arena::round_up(r->plan->workspace_bytes()));
-    r->st = stack_of(r->plan, ws);
+    r->st = stack_of(r->plan, ws, true);
     for (cudaEvent_t *e : {&r->e_in, &r->e_prep, &r->e_out})
         cuda_check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "request event");
     cuda_check(cudaMemcpyAsync(r->proj_dev, r->proj_host, r->proj_bytes, cudaMemcpyHostToDevice, s->s_in),

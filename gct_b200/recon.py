@@ -24,6 +24,9 @@ FILTER_TOEPLITZ_BF16X3 = 1
 FILTER_TOEPLITZ_BF16X4 = 2
 STORAGE_F32 = 0
 STORAGE_F16 = 1
+SYMMETRY_AUTO = 0
+SYMMETRY_OFF = 1
+SYMMETRY_ON = 2
 
 
 @dataclass
@@ -43,11 +46,12 @@ class FdkOptions:
     z_per_thread: int = 0
     block_x: int = 0
     block_y: int = 0
+    symmetry: int = SYMMETRY_AUTO
 
     def struct(self) -> _lib.gct_fdk_opts:
         o = _lib.gct_fdk_opts()
         o.filter, o.storage, o.z_per_thread = self.filter, self.storage, self.z_per_thread
-        o.block_x, o.block_y = self.block_x, self.block_y
+        o.block_x, o.block_y, o.symmetry = self.block_x, self.block_y, self.symmetry
         return o
 
 
@@ -123,6 +127,13 @@ class FdkPlan:
         n = C.c_uint64(0)
         _lib.check(self._lib.gct_fdk_plan_workspace_bytes(self._handle, C.byref(n)))
         return int(n.value)
+
+    @property
+    def quarter_turn(self) -> int:
+        """+1 / -1 when whole-scan backprojections use the quarter-turn symmetry, else 0."""
+        t = C.c_int32(0)
+        _lib.check(self._lib.gct_fdk_plan_symmetry(self._handle, C.byref(t)))
+        return int(t.value)
 
     def execute(self, proj, vol, workspace=None, stream=None) -> None:
         _lib.check(self._lib.gct_fdk_execute(self._handle, C.c_void_p(_ptr(proj)), C.c_void_p(_ptr(vol)),

@@ -155,13 +155,24 @@ enum {
     GCT_STORAGE_F32 = 0, /* filtered projections kept in FP32 */
     GCT_STORAGE_F16 = 1  /* filtered projections kept in FP16 with a per-view power-of-two scale */
 };
+enum {
+    /* Full scans whose views come in quarter-turn partners (view v + nv/4 is view v turned by 90
+     * degrees about the rotation axis) on a square, even, centred grid can evaluate detector
+     * coordinates once per four voxel-view updates, with the partner views' filtered projections
+     * interleaved in the workspace. Detected on the host in FP64 at plan creation. AUTO uses it
+     * with FP16 storage (where it is faster), ON with either storage, OFF never. */
+    GCT_SYMMETRY_AUTO = 0,
+    GCT_SYMMETRY_OFF = 1,
+    GCT_SYMMETRY_ON = 2
+};
 typedef struct gct_fdk_opts {
     int32_t filter;        /* GCT_FILTER_* */
     int32_t storage;       /* GCT_STORAGE_* */
     int32_t z_per_thread;  /* backprojection voxels per thread along z; 0 = tuned default */
     int32_t block_x;       /* backprojection block shape; 0 = tuned default */
     int32_t block_y;
-    int32_t reserved[3];
+    int32_t symmetry;      /* GCT_SYMMETRY_* */
+    int32_t reserved[2];
 } gct_fdk_opts;
 
 typedef struct gct_fdk_plan gct_fdk_plan;
@@ -234,6 +245,11 @@ gct_status gct_fdk_plan_check(gct_fdk_plan *plan);
  * prepared stack reads, so several stacks prepared with one plan into separate workspaces stay
  * independent. */
 gct_status gct_fdk_plan_workspace_bytes(const gct_fdk_plan *plan, uint64_t *bytes);
+
+/* Quarter-turn symmetry the plan found (GCT_SYMMETRY_AUTO): +1 when view v + nv/4 sees voxel
+ * column (n-1-y, x) where view v sees (x, y), -1 for (y, n-1-x), 0 when the geometry has neither
+ * or the option is off. No reference counterpart (an execution property of this engine). */
+gct_status gct_fdk_plan_symmetry(const gct_fdk_plan *plan, int32_t *quarter_turn);
 
 /* Full FDK on device buffers, asynchronous on `stream`: fused cosine + Parker weighting and
  * ramp filtering, then backprojection and the angular-increment scale. proj_dev is

@@ -20,7 +20,7 @@ pytestmark = pytest.mark.gpu
 def _dev(case, storage=g.STORAGE_F32, filt=g.FILTER_FFT):
     import torch
     proj = oracle_projections(case)
-    plan = g.FdkPlan(case.cg, case.vg, opts=g.FdkOptions(storage=storage, filter=filt))
+    plan = g.FdkPlan(case.cg, case.vg, opts=g.FdkOptions(storage=storage, filter=filt, symmetry=g.SYMMETRY_OFF))
     dproj = torch.from_numpy(proj).cuda()
     vol = torch.full(case.vg.shape, float("nan"), dtype=torch.float32, device="cuda")
     return plan, dproj, vol, proj

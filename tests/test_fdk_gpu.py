@@ -18,32 +18,35 @@ from oracle import oracle as orc
 pytestmark = pytest.mark.gpu
 
 
-def _run(case, proj_np, storage=g.STORAGE_F32, zpt=0, filt=None):
+def _run(case, proj_np, storage=g.STORAGE_F32, zpt=0, filt=None, sym=g.SYMMETRY_AUTO):
     import torch
     proj = torch.from_numpy(proj_np).cuda()
     vol = torch.empty(case.vg.shape, dtype=torch.float32, device="cuda")
-    with g.FdkPlan(case.cg, case.vg, filt=filt, opts=g.FdkOptions(storage=storage, z_per_thread=zpt)) as plan:
+    with g.FdkPlan(case.cg, case.vg, filt=filt,
+                   opts=g.FdkOptions(storage=storage, z_per_thread=zpt, symmetry=sym)) as plan:
         plan.execute(proj, vol)
         torch.cuda.synchronize()
     return vol.cpu().numpy()
 
 
+@pytest.mark.parametrize("sym", [g.SYMMETRY_ON, g.SYMMETRY_OFF])
 @pytest.mark.parametrize("kind", KINDS)
-def test_fdk_fp32_matches_oracle(kind):
+def test_fdk_fp32_matches_oracle(kind, sym):
     case = make_case(kind)
     proj = oracle_projections(case)
-    got = _run(case, proj)
+    got = _run(case, proj, sym=sym)
     ref = orc.fdk(case.og, case.ov, proj).reshape(got.shape)
     err = rel_rms(got, ref)
     assert err <= 1e-4, f"{kind}: relRMS {err:.3e}"
     assert np.abs(got - ref).max() <= 1e-3 * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("sym", [g.SYMMETRY_AUTO, g.SYMMETRY_OFF])
 @pytest.mark.parametrize("kind", KINDS)
-def test_fdk_fp16_storage_matches_oracle(kind):
+def test_fdk_fp16_storage_matches_oracle(kind, sym):
     case = make_case(kind)
     proj = oracle_projections(case)
-    got = _run(case, proj, storage=g.STORAGE_F16)
+    got = _run(case, proj, storage=g.STORAGE_F16, sym=sym)
     ref = orc.fdk(case.og, case.ov, proj).reshape(got.shape)
     err = rel_rms(got, ref)
     assert err <= 1e-3, f"{kind}: relRMS {err:.3e}"

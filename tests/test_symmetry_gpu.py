@@ -1,0 +1,153 @@
+"""Quarter-turn backprojection (full scans in quarter-turn view partners on a square, even,
+centred grid) against the plain column kernel and the FP64 oracle.
+
+Tolerances (relative RMS): quarter-turn vs plain kernel of the same plan options <= 1e-5 (the
+rotated columns take their detector coordinates from the base view's FP32 coefficients instead of
+their own; the coefficients agree to FP32 rounding); against the FP64 oracle as for the engine
+(1e-4 FP32 quads, 1e-3 FP16 quads); chunked host-buffer path vs one launch <= 1e-5 (the sum over
+chunks is rounded once per chunk, and the partial sums of ramp-filtered views cancel heavily, so
+their rounding is large against the final value: measured 1.9e-6 with FP16 quads).
+"""
+import math
+
+import numpy as np
+import pytest
+
+import gct_b200 as g
+from cases import make_case, oracle_projections
+from conftest import rel_rms
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+SYM_KINDS = ["fan_arc", "fan_line", "parallel_2d", "cone_parallel", "cone_cyl", "cone_flat"]
+
+
+def _plan(case, storage=g.STORAGE_F32, sym=g.SYMMETRY_ON, zpt=0, filt=g.FILTER_FFT):
+    return g.FdkPlan(case.cg, case.vg, opts=g.FdkOptions(storage=storage, symmetry=sym, z_per_thread=zpt,
+                                                         filter=filt))
+
+
+def _execute(plan, case, proj):
+    import torch
+    vol = torch.full(case.vg.shape, float("nan"), dtype=torch.float32, device="cuda")
+    plan.execute(torch.from_numpy(proj).cuda(), vol)
+    torch.cuda.synchronize()
+    return vol.cpu().numpy()
+
+
+@pytest.mark.parametrize("kind", SYM_KINDS)
+def test_detected_on_full_scans(kind):
+    cw = make_case(kind)
+    ccw = make_case(kind, rot_dir=g.RotDir.CCW, init_ang=0.3)
+    with _plan(cw) as a, _plan(ccw) as b, _plan(cw, sym=g.SYMMETRY_OFF) as off:
+        assert a.quarter_turn in (1, -1) and b.quarter_turn in (1, -1)
+        assert off.quarter_turn == 0
+
+
+def test_auto_takes_it_for_fp16_storage_only():
+    case = make_case("cone_flat")
+    with _plan(case, g.STORAGE_F16, sym=g.SYMMETRY_AUTO) as a, _plan(case, g.STORAGE_F32, sym=g.SYMMETRY_AUTO) as b:
+        assert a.quarter_turn != 0
+        assert b.quarter_turn == 0
+
+
+@pytest.mark.parametrize("case_kw", [
+    dict(n=21, nz=7),                          # odd grid side
+    dict(mid=(3.0, -2.0, 1.5)),                # grid off the rotation axis
+    dict(nv=122),                              # views not in quarter-turn partners
+    dict(nv=100, range_rad=math.pi + 0.5),     # short scan
+])
+def test_not_detected(case_kw):
+    case = make_case("cone_flat", **case_kw)
+    with _plan(case) as p:
+        assert p.quarter_turn == 0
+    with _plan(make_case("parallel_1d")) as p:  # the transposed 1D kind keeps its own kernel
+        assert p.quarter_turn == 0
+
+
+@pytest.mark.parametrize("storage", [g.STORAGE_F32, g.STORAGE_F16])
+@pytest.mark.parametrize("kind", SYM_KINDS)
+def test_matches_plain_kernel_and_oracle(kind, storage):
+    for rot in (g.RotDir.CW, g.RotDir.CCW):
+        case = make_case(kind, rot_dir=rot, init_ang=0.2)
+        proj = oracle_projections(case)
+        with _plan(case, storage) as ps, _plan(case, storage, sym=g.SYMMETRY_OFF) as pp:
+            assert ps.quarter_turn != 0
+            got, plain = _execute(ps, case, proj), _execute(pp, case, proj)
+        assert rel_rms(got, plain) <= 1e-5, (kind, rot)
+        ref = orc.fdk(case.og, case.ov, proj).reshape(got.shape)
+        tol = 1e-4 if storage == g.STORAGE_F32 else 1e-3
+        assert rel_rms(got, ref) <= tol, (kind, rot)
+
+
+@pytest.mark.parametrize("kind", ["cone_flat", "cone_cyl", "fan_arc"])
+def test_z_per_thread_variants_agree(kind):
+    case = make_case(kind, nz=10)
+    proj = oracle_projections(case)
+    outs = []
+    for zpt in (1, 2, 4, 8):
+        with _plan(case, zpt=zpt) as p:
+            assert p.quarter_turn != 0
+            outs.append(_execute(p, case, proj))
+    for o in outs[1:]:
+        assert rel_rms(o, outs[0]) <= 1e-6
+
+
+@pytest.mark.parametrize("storage", [g.STORAGE_F32, g.STORAGE_F16])
+def test_host_buffer_path_chunks_base_views(storage):
+    case = make_case("cone_flat", nv=240)
+    proj = oracle_projections(case)
+    with _plan(case, storage) as p:
+        dev = _execute(p, case, proj)
+        host = np.empty(case.vg.shape, np.float32)
+        p.execute_host(proj, host)
+    assert rel_rms(host, dev) <= 1e-5
+
+
+def test_partial_view_range_uses_plain_kernel():
+    # prepare + backproject over two halves accumulate the same volume as one execute
+    import torch
+    case = make_case("cone_flat")
+    proj = oracle_projections(case)
+    with _plan(case) as p:
+        full = _execute(p, case, proj)
+        dproj = torch.from_numpy(proj).cuda()
+        vol = torch.zeros(case.vg.shape, dtype=torch.float32, device="cuda")
+        half = case.cg.num_views // 2
+        p.prepare(dproj)
+        p.backproject(vol, view_begin=0, view_count=half)
+        p.backproject(vol, view_begin=half, view_count=case.cg.num_views - half, accumulate=True)
+        torch.cuda.synchronize()
+        assert rel_rms(vol.cpu().numpy(), full) <= 1e-5
+
+
+@pytest.mark.parametrize("storage", [g.STORAGE_F32, g.STORAGE_F16])
+def test_prepare_in_parts_matches_whole(storage):
+    # partial prepares write single views into the interleaved stack; a whole prepare writes the
+    # partner groups from FP32 rows in one pass: the same quads up to the order of one scaling,
+    # which can flip an FP16 rounding (measured 3e-6 with FP16 storage)
+    import torch
+    case = make_case("cone_flat")
+    proj = oracle_projections(case)
+    with _plan(case, storage) as p:
+        full = _execute(p, case, proj)
+        dproj = torch.from_numpy(proj).cuda()
+        half = case.cg.num_views // 2 + 3
+        p.prepare(dproj, view_begin=0, view_count=half)
+        p.prepare(dproj, view_begin=half, view_count=case.cg.num_views - half)
+        vol = torch.full(case.vg.shape, float("nan"), dtype=torch.float32, device="cuda")
+        p.backproject(vol)
+        torch.cuda.synchronize()
+        assert rel_rms(vol.cpu().numpy(), full) <= (1e-6 if storage == g.STORAGE_F32 else 1e-5)
+
+
+def test_toeplitz_filter_with_quarter_turns():
+    case = make_case("cone_flat")
+    proj = oracle_projections(case)
+    with _plan(case, g.STORAGE_F16, filt=g.FILTER_TOEPLITZ_BF16X4) as p:
+        assert p.quarter_turn != 0
+        got = _execute(p, case, proj)
+        p.check()
+    ref = orc.fdk(case.og, case.ov, proj).reshape(got.shape)
+    assert rel_rms(got, ref) <= 1e-3
