@@ -448,6 +448,8 @@ def run_gct(args, cfg, rank, world, local_rank):
     bp_label = ("backproject, quarter-turn partners (FP16 quads, bp_sym_kernel)" if quarter
                 else "backproject (FP16 quads, bp_kernel)")
     traffic = profiled_traffic(f"backproject_{'sym_' if quarter else ''}{args.config}_f16.md")
+    sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    l1_peak = 128 * torch.cuda.get_device_properties(local_rank).multi_processor_count * sm_mhz * 1e6 / 1e9
     line = {
         "metric": "FDK backprojection GUPS (voxel x view updates / s), mixed precision", "value": mixed["gups"],
         "unit": "GUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -468,7 +470,10 @@ def run_gct(args, cfg, rank, world, local_rank):
         "roofline": {"bound": "hbm", "kernel": bp_label, "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_kind,
                      "algorithmic_bytes_per_update": bytes_per_update,
-                     "traffic": traffic},
+                     "traffic": traffic,
+                     # the taps come through the SM's L1 data path, which bounds this kernel
+                     "l1_data_path": {"achieved": achieved, "peak": l1_peak, "unit": "GB/s", "frac": achieved / l1_peak,
+                                      "peak_source": "nominal 128 B/clk per SM x SMs x median SM clock under load"}},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "clocks": clocks,

@@ -199,9 +199,10 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
         gct::fail(GCT_ERR_INVALID_ARG, "backprojection block must hold 32..256 threads");
     // quarter-turn form: the z-affine column kernels (not the transposed 1D kind, whose kernel
     // grid is x by image rows); at most 8 voxels per thread, since each thread keeps four columns.
-    // Measured on B200 (512^3, 720 views): FP16 quads 35.7 ms against 47.2 ms for the plain kernel
-    // (8 voxels per thread, 4 x 16 blocks); FP32 quads 88 ms against 64 ms (a 64-byte partner group
-    // per voxel), so AUTO takes it for FP16 storage only and ON for both.
+    // Measured on B200 (512^3, 720 views): FP16 quads 34.4 ms against 47.2 ms for the plain kernel
+    // (8 voxels per thread, 2 x 32 blocks; 4 x 16: 35.5, 8 x 16: 36.6, 4 voxels: 36.9); FP32 quads
+    // 88 ms against 64 ms (a 64-byte partner group per voxel), so AUTO takes it for FP16 storage
+    // only and ON for both.
     const int so = p->opts.symmetry;
     if (so != GCT_SYMMETRY_AUTO && so != GCT_SYMMETRY_OFF && so != GCT_SYMMETRY_ON)
         gct::fail(GCT_ERR_INVALID_ARG, "unknown symmetry option");
@@ -214,8 +215,8 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
     if (p->sym && !p->ybuf.p)
         p->ybuf.alloc(static_cast<size_t>(p->nv) * p->nr * p->nc, "filtered rows of quarter-turn stacks");
     p->zpt_sym = p->opts.z_per_thread > 0 ? std::min(p->zpt, 8) : (vol3d ? (f16 ? 8 : 4) : 1);
-    p->bx_sym = p->opts.block_x > 0 ? p->bx : (vol3d ? 4 : 8);
-    p->by_sym = p->opts.block_y > 0 ? p->by : (vol3d ? 16 : 8);
+    p->bx_sym = p->opts.block_x > 0 ? p->bx : (vol3d ? (f16 ? 2 : 4) : 8);
+    p->by_sym = p->opts.block_y > 0 ? p->by : (vol3d ? (f16 ? 32 : 16) : 8);
 }
 
 // Toeplitz-GEMM form of run_filter: split, tcgen05 GEMM into FP32 rows, then quads (or the rows
@@ -438,8 +439,10 @@ void execute_host(gct_fdk_plan *p, const float *proj_host, float *vol_host, cuda
     if (!p->host_vol.p) p->host_vol.alloc(vol_n, "staging volume");
     const StackRef st = stack_of(p, plan_workspace(p, nullptr));
     if (!p->copy_stream) cuda_check(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking), "copy stream");
-    // about 8 chunks, at least 16 views each; a quarter-turn plan chunks its base views and takes
-    // each chunk's partner views with it
+    // About 8 chunks, at least 16 views each; a quarter-turn plan chunks its base views and takes
+    // each chunk's partner views with it. (Measured and rejected at 512^3 / 720 views: splitting the
+    // last quarter into chunks a quarter that size, to shorten the work after the last upload:
+    // 74.8 against 61.2 ms per reconstruction, the small chunks' filter launches cost more.)
     const int parts = st.quarter ? 4 : 1, span = p->nv / parts;
     const int chunk = std::max(16 / parts, (span + 7) / 8);
     const int nchunks = (span + chunk - 1) / chunk;

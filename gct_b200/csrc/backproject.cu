@@ -618,6 +618,8 @@ __global__ void __launch_bounds__(256) bp_sym_kernel(BpArgs a)
         for (int vv = 0; vv < nvc; ++vv) {
             const int packed = s_cls[vv];
             if (packed == 0) continue;  // every turned box off the detector (kBoxOff == 0)
+            // read from shared memory by each evaluation: copying them to registers once per base
+            // view measured slower (128 registers, 37.0 against 34.4 ms at 512^3)
             const float *c = reinterpret_cast<const float *>(s_coef) + vv * kC;
             const float4 w = s_w[vv];
             // base views are below quarter, so their partner groups start at 4 qview per view
