@@ -13,4 +13,6 @@ from .recon import (FILTER_FFT, FILTER_TOEPLITZ_BF16X3, FILTER_TOEPLITZ_BF16X4, 
                     SYMMETRY_AUTO, SYMMETRY_OFF, SYMMETRY_ON, FdkBatch, FdkOptions, FdkPlan, FdkServer, FiltParams,
                     forward_project, phantom_project, reconstruct)
 
+from . import io
+
 __all__ = [name for name in dir() if not name.startswith("_")]

@@ -103,6 +103,10 @@ class gct_server_stats(C.Structure):
                 ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("recons_per_s", C.c_double)]
 
 
+class gct_array_metadata(C.Structure):
+    _fields_ = [("num_rows", C.c_uint32), ("num_cols", C.c_uint32), ("num_slices", C.c_uint32), ("type", C.c_int32)]
+
+
 class gct_ellipsoid(C.Structure):
     _fields_ = [("center", C.c_double * 3), ("semi_axes", C.c_double * 3), ("phi", C.c_double),
                 ("mu", C.c_double)]
@@ -151,6 +155,13 @@ SIGNATURES = {
     "gct_fdk_server_destroy": [VP],
     "gct_phantom_project": [P(gct_ct_geom), P(gct_ellipsoid), C.c_uint32, VP, VP],
     "gct_forward_project": [P(gct_ct_geom), P(gct_vol_geom), VP, C.c_float, VP, VP],
+    "gct_array_read_metadata": [C.c_char_p, C.c_int32, P(gct_array_metadata)],
+    "gct_array_read": [C.c_char_p, C.c_int32, C.c_int32, P(gct_array_metadata), C.c_int32, VP, C.c_uint64,
+                       P(C.c_uint64)],
+    "gct_meta_image_write": [C.c_char_p, C.c_uint32, P(C.c_uint32), P(C.c_float), P(C.c_float), C.c_int32, VP,
+                             C.c_uint64],
+    "gct_den_write": [C.c_char_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32, VP, C.c_uint64],
+    "gct_raw_write": [C.c_char_p, C.c_int32, VP, C.c_uint64],
 }
 _RESTYPES = {"gct_abi_version": C.c_int32, "gct_last_error_string": C.c_char_p}
 

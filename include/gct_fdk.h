@@ -460,6 +460,70 @@ gct_status gct_forward_project(const gct_ct_geom *geom, const gct_vol_geom *vol,
                                const float *vol_dev, float step_vox, float *proj_dev,
                                void *stream);
 
+/* ---- array files (host) ---------------------------------------------------------------- */
+
+/* Element types of array files: GCT::IO::ArrayElemType (src/cpp/io/metadata.h:10-22). */
+typedef enum gct_elem_type {
+    GCT_T_UINT8 = 0,
+    GCT_T_INT8 = 1,
+    GCT_T_UINT16 = 2,
+    GCT_T_INT16 = 3,
+    GCT_T_UINT32 = 4,
+    GCT_T_INT32 = 5,
+    GCT_T_UINT64 = 6,
+    GCT_T_INT64 = 7,
+    GCT_T_FLOAT = 8,
+    GCT_T_DOUBLE = 9
+} gct_elem_type;
+
+/* GCT::IO::ArrayMetadata (src/cpp/io/metadata.h:24-30): one file's rows x columns x slices. */
+typedef struct gct_array_metadata {
+    uint32_t num_rows;
+    uint32_t num_cols;
+    uint32_t num_slices;
+    int32_t type; /* gct_elem_type */
+} gct_array_metadata;
+
+/* Readers: GCT::IO::MetaImgFileReader (src/cpp/io/file_reader/meta_img_reader.cpp:10-165; .mha
+ * with ElementDataFile = LOCAL, or a header naming a data file in its directory),
+ * DenFileReader (den_file_reader.cpp: three uint16 then the data, the type from the file size)
+ * and RawDataFileReader (raw_data_file_reader.h: the caller gives the metadata). */
+typedef enum gct_file_format {
+    GCT_FILE_META_IMAGE = 0,
+    GCT_FILE_DEN = 1,
+    GCT_FILE_RAW = 2
+} gct_file_format;
+
+/* ArrayFileReader::readMetadata (array_file_reader.h:25). For GCT_FILE_RAW, *md is the input
+ * metadata and is returned unchanged once the file is found. */
+gct_status gct_array_read_metadata(const char *filename, int32_t format, gct_array_metadata *md);
+
+/* ArrayFileReader::readData<OpType> (array_file_reader.h:60-65): the data of the file, or with
+ * `series` of every file in its directory tree with its extension and size in sorted order
+ * (getAllFiles, src/cpp/io/file_utils.cpp:7-27), each element static_cast to out_type.
+ * raw_md: metadata of GCT_FILE_RAW files (else ignored). *count (optional) receives the number of
+ * elements; with out == NULL nothing else happens (a size query), else out_count must equal it.
+ * Data sizes are checked exactly (readDataFromBinFile); a LOCAL MetaImage shorter than its header
+ * promises is an error (the reference leaves the missing elements zero). */
+gct_status gct_array_read(const char *filename, int32_t format, int32_t series, const gct_array_metadata *raw_md,
+                          int32_t out_type, void *out, uint64_t out_count, uint64_t *count);
+
+/* GCT::IO::ArrayFileWriter::write(MetaImgMetaData, data, filename)
+ * (src/cpp/io/file_writer/meta_img_file_writer.h): the reference's header lines in its order;
+ * a ".mha" name keeps the data after the header, any other writes <stem>.raw beside it. dim_size,
+ * spacing and offset hold ndims (1..3) entries, x first; data holds count elements of `type`. */
+gct_status gct_meta_image_write(const char *filename, uint32_t ndims, const uint32_t *dim_size,
+                                const float *spacing, const float *offset, int32_t type, const void *data,
+                                uint64_t count);
+
+/* ArrayFileWriter::write(DenMetaData, ...) (den_file_writer.h): uint16 rows, columns, slices,
+ * then the data. Dimensions above 65535 are rejected (the reference truncates them). */
+gct_status gct_den_write(const char *filename, uint32_t num_rows, uint32_t num_cols, uint32_t num_slices,
+                         int32_t type, const void *data, uint64_t count);
+
+/* ArrayFileWriter::write(data, filename) (raw_data_file_writer.h): the bytes of the data. */
+gct_status gct_raw_write(const char *filename, int32_t type, const void *data, uint64_t count);
+
 #ifdef __cplusplus
 }
 #endif

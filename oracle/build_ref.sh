@@ -7,7 +7,9 @@
 #                       entry points of oracle/ref_host.cu, for the golden vectors and CPU tests;
 #   ref_fdk             the reference's CUDA FDK (GCT::Recon::CUDA::reconstruct and everything it
 #                       calls) for sm_100a, driven by oracle/ref_fdk_main.cu, for the GPU parity
-#                       tests against the reference itself.
+#                       tests against the reference itself;
+#   libgct_ref_io.so    the reference's array-file readers and writers (src/cpp/io) behind the C
+#                       entry points of oracle/ref_io.cpp, for the IO golden files.
 #
 # The reference's Eigen submodule is empty in its tree. The translation units used here compile
 # without it except for declarations in src/cpp/geom/projection_matrix.h, which
@@ -53,4 +55,10 @@ for p in "${pids[@]}"; do wait "$p"; done
     "$OUT"/ref_parker_weighting.o "$OUT"/ref_ramp_filtering_fft.o "$OUT"/ref_check_error.o "$OUT"/ref_cuda_config.o \
     "$OUT/ramp_filter.o" "$OUT/proj_filt_kernel.o" "$OUT/rotation_geom.o" "$OUT/proj_meta_info.o" "$OUT/vec_wcs.o" \
     -lcufft -lcudart
-echo "$OUT/libgct_ref_host.so $OUT/ref_fdk"
+# the reference's array-file readers and writers
+IO=(cpp/io/file_reader/meta_img_reader.cpp cpp/io/file_reader/array_file_reader.cpp
+    cpp/io/file_reader/den_file_reader.cpp cpp/io/file_reader/raw_data_file_reader.cpp cpp/io/file_utils.cpp
+    cpp/io/string_utils.cpp cpp/io/file_writer/meta_img_file_writer.cpp)
+g++ -std=c++20 -O2 -fPIC -w -I "$REF/src" -shared -o "$OUT/libgct_ref_io.so" "$HERE/ref_io.cpp" \
+    "${IO[@]/#/$REF/src/}"
+echo "$OUT/libgct_ref_host.so $OUT/ref_fdk $OUT/libgct_ref_io.so"
