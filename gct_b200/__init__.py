@@ -8,7 +8,7 @@ from .geometry import (ApodFunc, AxialCTGeom, ConeBeamProjGeomParams, CTGeom, De
                        DetParallel, EqDistSampler, FanBeamProjGeomParams, GeomKind, Parallel1DProjGeomParams,
                        Parallel2DProjGeomParams, ProjectionStack, ProjGeom, ProjGeomFactory, ReconImg,
                        ReconImgGeom, RotationGeom, RotationParams, RotDir, is_valid_axial_recon, kind_of,
-                       map_point, parker_weights, ramp_filter_taps, VIEW_DTYPE)
+                       map_point, parker_weights, ProjectionMatrix, ramp_filter_taps, VIEW_DTYPE)
 from .recon import (FILTER_FFT, FILTER_TOEPLITZ_BF16X3, FILTER_TOEPLITZ_BF16X4, STORAGE_F16, STORAGE_F32,
                     SYMMETRY_AUTO, SYMMETRY_OFF, SYMMETRY_ON, FdkBatch, FdkOptions, FdkPlan, FdkServer, FiltParams,
                     forward_project, phantom_project, reconstruct)

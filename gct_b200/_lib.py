@@ -103,6 +103,11 @@ class gct_server_stats(C.Structure):
                 ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("recons_per_s", C.c_double)]
 
 
+class gct_proj_matrix(C.Structure):
+    _fields_ = [("matrix", C.c_double * 12), ("intrinsic", C.c_double * 9), ("rotation", C.c_double * 9),
+                ("src_pos", C.c_double * 3)]
+
+
 class gct_array_metadata(C.Structure):
     _fields_ = [("num_rows", C.c_uint32), ("num_cols", C.c_uint32), ("num_slices", C.c_uint32), ("type", C.c_int32)]
 
@@ -120,6 +125,9 @@ SIGNATURES = {
     "gct_abi_version": [],
     "gct_last_error_string": [],
     "gct_proj_geom_create": [C.c_int32, P(gct_geom_params), C.c_uint32, P(gct_view_geom)],
+    "gct_proj_matrix_decompose": [P(C.c_double), P(gct_proj_matrix)],
+    "gct_proj_matrix_compose": [P(gct_view_geom), C.c_double, C.c_double, P(gct_proj_matrix)],
+    "gct_proj_geom_from_matrix": [P(C.c_double), P(gct_view_geom)],
     "gct_rotation_geom_get": [P(gct_ct_geom), P(gct_rotation_geom), P(C.c_double), P(C.c_double)],
     "gct_is_valid_axial_recon": [P(gct_ct_geom), C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32,
                                  P(C.c_int32)],

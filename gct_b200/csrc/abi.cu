@@ -502,6 +502,41 @@ gct_status gct_proj_geom_create(int32_t kind, const gct_geom_params *params, uin
     });
 }
 
+namespace {
+void export_matrix(const gct::ProjMatrix &pm, gct_proj_matrix *out)
+{
+    std::copy(pm.m, pm.m + 12, out->matrix);
+    std::copy(pm.K, pm.K + 9, out->intrinsic);
+    std::copy(pm.R, pm.R + 9, out->rotation);
+    std::copy(pm.src, pm.src + 3, out->src_pos);
+}
+}  // namespace
+
+gct_status gct_proj_matrix_decompose(const double *matrix, gct_proj_matrix *out)
+{
+    return guarded([&] {
+        if (!matrix || !out) gct::fail(GCT_ERR_INVALID_ARG, "NULL argument");
+        export_matrix(gct::decompose_projection_matrix(matrix), out);
+    });
+}
+
+gct_status gct_proj_matrix_compose(const gct_view_geom *view, double pix_width_mm, double pix_height_mm,
+                                   gct_proj_matrix *out)
+{
+    return guarded([&] {
+        if (!view || !out) gct::fail(GCT_ERR_INVALID_ARG, "NULL argument");
+        export_matrix(gct::compose_projection_matrix(*view, pix_width_mm, pix_height_mm), out);
+    });
+}
+
+gct_status gct_proj_geom_from_matrix(const double *matrix, gct_view_geom *out)
+{
+    return guarded([&] {
+        if (!matrix || !out) gct::fail(GCT_ERR_INVALID_ARG, "NULL argument");
+        *out = gct::view_from_projection_matrix(gct::decompose_projection_matrix(matrix));
+    });
+}
+
 gct_status gct_rotation_geom_get(const gct_ct_geom *geom, gct_rotation_geom *out, double *rot_ang,
                                  double *rel_rot_ang)
 {

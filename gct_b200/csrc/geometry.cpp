@@ -527,4 +527,127 @@ int quarter_turn_symmetry(gct_geom_kind kind, const std::vector<double> &c64, un
     return 0;
 }
 
+// ---- projection matrices -----------------------------------------------------------------------
+
+namespace {
+void mat3_inverse(const double *a, double *inv)
+{
+    const double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
+    const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+    if (!(std::fabs(det) > 0.0) || !std::isfinite(det)) fail(GCT_ERR_INVALID_ARG, "singular projection matrix");
+    const double r = 1.0 / det;
+    inv[0] = c00 * r;
+    inv[1] = (a[2] * a[7] - a[1] * a[8]) * r;
+    inv[2] = (a[1] * a[5] - a[2] * a[4]) * r;
+    inv[3] = c01 * r;
+    inv[4] = (a[0] * a[8] - a[2] * a[6]) * r;
+    inv[5] = (a[2] * a[3] - a[0] * a[5]) * r;
+    inv[6] = c02 * r;
+    inv[7] = (a[1] * a[6] - a[0] * a[7]) * r;
+    inv[8] = (a[0] * a[4] - a[1] * a[3]) * r;
+}
+void mat3_mul(const double *a, const double *b, double *c)
+{
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) c[3 * i + j] = a[3 * i] * b[j] + a[3 * i + 1] * b[3 + j] + a[3 * i + 2] * b[6 + j];
+}
+}  // namespace
+
+// ProjectionMatrix(matrix) (src/cpp/geom/projection_matrix.cpp:4-62): with M the left 3 x 3 block,
+// QR of M^-1 = Q U gives M = U^-1 Q^T, so K = U^-1 (upper triangular) and R = Q^T; signs are fixed
+// so that K has a positive diagonal, K is normalised to K[2][2] = 1 and the source is
+// -M^-1 times the fourth column. FP64 throughout (the reference keeps FP32 copies). The QR here is
+// modified Gram-Schmidt on the three columns, which with the sign rule gives the same K and R as
+// the reference's Householder QR.
+ProjMatrix decompose_projection_matrix(const double *m)
+{
+    ProjMatrix pm{};
+    std::copy(m, m + 12, pm.m);
+    const double M[9] = {m[0], m[1], m[2], m[4], m[5], m[6], m[8], m[9], m[10]};
+    double Mi[9];
+    mat3_inverse(M, Mi);
+    // columns of Mi -> Q (columns q0..q2) and U
+    double q[3][3], U[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int j = 0; j < 3; ++j) {
+        double a[3] = {Mi[j], Mi[3 + j], Mi[6 + j]};
+        for (int k = 0; k < j; ++k) {
+            const double r = q[k][0] * a[0] + q[k][1] * a[1] + q[k][2] * a[2];
+            U[3 * k + j] = r;
+            for (int t = 0; t < 3; ++t) a[t] -= r * q[k][t];
+        }
+        const double n = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        if (!(n > 0.0)) fail(GCT_ERR_INVALID_ARG, "singular projection matrix");
+        U[3 * j + j] = n;
+        for (int t = 0; t < 3; ++t) q[j][t] = a[t] / n;
+    }
+    double K[9];
+    mat3_inverse(U, K);
+    K[3] = K[6] = K[7] = 0.0;  // exactly upper triangular
+    double R[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) R[3 * i + j] = q[i][j];  // R = Q^T: row i is column q_i
+    for (int d = 0; d < 3; ++d) {
+        const double sgn = std::copysign(1.0, K[4 * d]);
+        for (int i = 0; i < 3; ++i) K[3 * i + d] *= sgn;  // K D
+        for (int j = 0; j < 3; ++j) R[3 * d + j] *= sgn;  // D R
+    }
+    const double k22 = K[8];
+    for (double &k : K) k /= k22;
+    std::copy(K, K + 9, pm.K);
+    std::copy(R, R + 9, pm.R);
+    for (int i = 0; i < 3; ++i) pm.src[i] = -(Mi[3 * i] * m[3] + Mi[3 * i + 1] * m[7] + Mi[3 * i + 2] * m[11]);
+    return pm;
+}
+
+// ProjectionMatrix(ProjGeom<DetFanLine, DetFanLine>, pix_width, pix_height)
+// (projection_matrix.cpp:64-97): K from the source-detector distance in pixels and the centres,
+// R from the detector directions and their cross product, M = K [R | -R src] scaled to M[2][3] = 1.
+ProjMatrix compose_projection_matrix(const gct_view_geom &v, double pix_w, double pix_h)
+{
+    if (!(pix_w > 0.0) || !(pix_h > 0.0)) fail(GCT_ERR_INVALID_ARG, "pixel sizes must be positive");
+    ProjMatrix pm{};
+    const double K[9] = {v.src_det_dist / pix_w, 0.0, v.det_row_center, 0.0, v.src_det_dist / pix_h, v.det_col_center,
+                         0.0, 0.0, 1.0};
+    double w[3];
+    cross3(v.det_row_dir, v.det_col_dir, w);
+    const double R[9] = {v.det_row_dir[0], v.det_row_dir[1], v.det_row_dir[2], v.det_col_dir[0], v.det_col_dir[1],
+                         v.det_col_dir[2], w[0], w[1], w[2]};
+    double KR[9];
+    mat3_mul(K, R, KR);
+    double t[3];
+    for (int i = 0; i < 3; ++i) t[i] = -(R[3 * i] * v.src_pos[0] + R[3 * i + 1] * v.src_pos[1] + R[3 * i + 2] * v.src_pos[2]);
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) pm.m[4 * i + j] = KR[3 * i + j];
+        pm.m[4 * i + 3] = K[3 * i] * t[0] + K[3 * i + 1] * t[1] + K[3 * i + 2] * t[2];
+    }
+    const double s = pm.m[11];
+    if (!(std::fabs(s) > 0.0)) fail(GCT_ERR_INVALID_ARG, "the source lies in the detector's plane through the origin");
+    for (double &x : pm.m) x /= s;
+    std::copy(K, K + 9, pm.K);
+    std::copy(R, R + 9, pm.R);
+    std::copy(v.src_pos, v.src_pos + 3, pm.src);
+    return pm;
+}
+
+// ProjGeomFactory<DetFanLine, DetFanLine>::create(ProjectionMatrix)
+// (src/cpp/io/geom_reader/proj_geom_factory_proj_mat.cpp:7-26): the flat-panel view of a matrix.
+// As in the reference, the source-detector distance is the focal length in detector-row pixels
+// (the caller multiplies by the pixel width).
+gct_view_geom view_from_projection_matrix(const ProjMatrix &pm)
+{
+    gct_view_geom v{};
+    v.src_det_dist = pm.K[0];
+    v.det_row_center = pm.K[2];
+    v.det_col_center = pm.K[5];
+    for (int i = 0; i < 3; ++i) {
+        v.src_pos[i] = pm.src[i];
+        v.det_row_dir[i] = pm.R[i];
+        v.det_col_dir[i] = pm.R[3 + i];
+    }
+    v.src_iso_dist = norm3(v.src_pos);
+    v.rot_ang = view_rot_angle(GCT_GEOM_CONE_FLAT, v);
+    return v;
+}
+
 }  // namespace gct
+

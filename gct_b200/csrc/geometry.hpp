@@ -54,6 +54,14 @@ void check_vol_geom(const gct_vol_geom *v, bool volume_3d);
 
 gct_view_geom make_view(gct_geom_kind kind, const gct_geom_params &p, unsigned idx);
 
+// Projection matrices of flat-panel views (row-major 3 x 4 matrix, K, R, source), FP64.
+struct ProjMatrix {
+    double m[12], K[9], R[9], src[3];
+};
+ProjMatrix decompose_projection_matrix(const double *m);
+ProjMatrix compose_projection_matrix(const gct_view_geom &v, double pix_w, double pix_h);
+gct_view_geom view_from_projection_matrix(const ProjMatrix &pm);
+
 std::vector<double> ramp_taps(gct_geom_kind kind, const gct_detector &det_row,
                               const gct_filt_params &fp);
 

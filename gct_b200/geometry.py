@@ -176,17 +176,76 @@ def _params_struct(params) -> _lib.gct_geom_params:
     return p
 
 
+class ProjectionMatrix:
+    """GCT::Geom::ProjectionMatrix (src/cpp/geom/projection_matrix.{h,cpp}) in FP64: a 3 x 4
+    flat-panel projection matrix with its intrinsic matrix K (upper triangular, positive diagonal,
+    K[2][2] = 1), rotation R (rows: detector row direction, column direction, their cross product)
+    and source position."""
+
+    def __init__(self, matrix):
+        m = np.ascontiguousarray(np.asarray(matrix, dtype=np.float64).reshape(12))
+        out = _lib.gct_proj_matrix()
+        _lib.check(_lib.load().gct_proj_matrix_decompose(m.ctypes.data_as(C.POINTER(C.c_double)), C.byref(out)))
+        self._set(out)
+
+    def _set(self, s: _lib.gct_proj_matrix) -> None:
+        self._matrix = np.array(s.matrix[:], dtype=np.float64).reshape(3, 4)
+        self._k = np.array(s.intrinsic[:], dtype=np.float64).reshape(3, 3)
+        self._r = np.array(s.rotation[:], dtype=np.float64).reshape(3, 3)
+        self._src = np.array(s.src_pos[:], dtype=np.float64)
+
+    @classmethod
+    def compose(cls, pg: ProjGeom, pix_width_mm: float, pix_height_mm: float) -> "ProjectionMatrix":
+        """ProjectionMatrix(ProjGeom<DetFanLine, DetFanLine>, pix_width_mm, pix_height_mm)."""
+        v = _lib.gct_view_geom.from_buffer_copy(pg.to_record().tobytes())
+        out = _lib.gct_proj_matrix()
+        _lib.check(_lib.load().gct_proj_matrix_compose(C.byref(v), float(pix_width_mm), float(pix_height_mm),
+                                                       C.byref(out)))
+        obj = cls.__new__(cls)
+        obj._set(out)
+        return obj
+
+    def matrix(self) -> np.ndarray:
+        return self._matrix.copy()
+
+    def intrinsic_matrix(self) -> np.ndarray:
+        return self._k.copy()
+
+    def rotation_matrix(self) -> np.ndarray:
+        return self._r.copy()
+
+    def src_pos(self) -> np.ndarray:
+        return self._src.copy()
+
+    def principal_point_det_row(self) -> float:
+        return float(self._k[0, 2])
+
+    def principal_point_det_col(self) -> float:
+        return float(self._k[1, 2])
+
+    def focal_length_det_row(self) -> float:
+        """Source-detector distance in detector-row pixels."""
+        return float(self._k[0, 0])
+
+
 class ProjGeomFactory:
-    """``ProjGeomFactory(DetRow[, DetCol]).create(params, proj_idx)``."""
+    """``ProjGeomFactory(DetRow[, DetCol]).create(params, proj_idx)``, and for flat panels
+    ``create(ProjectionMatrix)`` (src/cpp/io/geom_reader/proj_geom_factory_proj_mat.cpp:7-26)."""
 
     def __init__(self, *det_types: type):
         self.kind = kind_of(det_types)
 
-    def create(self, params, proj_idx: int) -> ProjGeom:
+    def create(self, params, proj_idx: int | None = None) -> ProjGeom:
         out = _lib.gct_view_geom()
         lib = _lib.load()
-        _lib.check(lib.gct_proj_geom_create(int(self.kind), C.byref(_params_struct(params)),
-                                            int(proj_idx), C.byref(out)))
+        if isinstance(params, ProjectionMatrix):
+            if self.kind != GeomKind.CONE_FLAT:
+                raise TypeError("projection matrices describe flat-panel (DetFanLine, DetFanLine) views")
+            m = np.ascontiguousarray(params.matrix().reshape(12))
+            _lib.check(lib.gct_proj_geom_from_matrix(m.ctypes.data_as(C.POINTER(C.c_double)), C.byref(out)))
+        else:
+            _lib.check(lib.gct_proj_geom_create(int(self.kind), C.byref(_params_struct(params)),
+                                                int(proj_idx), C.byref(out)))
         rec = np.frombuffer(bytearray(out), dtype=VIEW_DTYPE)[0]
         return ProjGeom.from_record(rec)
 

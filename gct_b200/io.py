@@ -16,7 +16,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from .geometry import ProjectionStack, ReconImg
+from .geometry import ProjectionMatrix, ProjectionStack, ReconImg
 
 
 class ArrayElemType(enum.IntEnum):
@@ -134,6 +134,21 @@ class ProjectionReader:
         if dim == 2:
             return ProjectionStack(md.num_cols, data.size // (md.num_cols * md.num_rows), md.num_rows, data=data)
         raise ValueError("projections are 1D or 2D")
+
+
+class ProjMatReader:
+    """ProjMatReader<FileReader>::read (src/cpp/io/geom_reader/proj_mat_reader.h:9-45): a file
+    of num_slices 3 x 4 projection matrices (12 elements each, row-major), read as doubles."""
+
+    @staticmethod
+    def read(reader: _ArrayFileReader) -> list[ProjectionMatrix]:
+        md = reader.read_metadata()
+        data = reader.read_data(np.float64)
+        n = md.num_slices
+        if data.size != 12 * n:
+            raise ValueError(f"Error during the reading of projection matrix file {reader.filename}.\n"
+                             "There should be 12 elements in each projection matrix.")
+        return [ProjectionMatrix(data[12 * i: 12 * i + 12]) for i in range(n)]
 
 
 def _contig(data) -> np.ndarray:

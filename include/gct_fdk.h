@@ -190,6 +190,34 @@ const char *gct_last_error_string(void);
 gct_status gct_proj_geom_create(int32_t kind, const gct_geom_params *params, uint32_t proj_idx,
                                 gct_view_geom *out);
 
+/* Projection matrix of a flat-panel view: GCT::Geom::ProjectionMatrix
+ * (src/cpp/geom/projection_matrix.{h,cpp}), in FP64. matrix is 3 x 4 row-major; intrinsic K is
+ * upper triangular with a positive diagonal and K[2][2] = 1 (focalLengthDetRow = K[0][0],
+ * principalPointDetRow = K[0][2], principalPointDetCol = K[1][2]); rotation R holds the detector
+ * row direction, column direction and their cross product as rows; src_pos is the focal spot. */
+typedef struct gct_proj_matrix {
+    double matrix[12];
+    double intrinsic[9];
+    double rotation[9];
+    double src_pos[3];
+} gct_proj_matrix;
+
+/* ProjectionMatrix(matrix): RQ decomposition of the left 3 x 3 block (through QR of its
+ * inverse) and the source position -M^-1 m4 (projection_matrix.cpp:4-62). */
+gct_status gct_proj_matrix_decompose(const double *matrix, gct_proj_matrix *out);
+
+/* ProjectionMatrix(ProjGeom<DetFanLine, DetFanLine>, pix_width_mm, pix_height_mm)
+ * (projection_matrix.cpp:64-97): M = K [R | -R src], scaled so that M[2][3] = 1. view holds the
+ * CONE_FLAT fields (src_det_dist in mm, centres in pixels, src_pos, det_row_dir, det_col_dir). */
+gct_status gct_proj_matrix_compose(const gct_view_geom *view, double pix_width_mm, double pix_height_mm,
+                                   gct_proj_matrix *out);
+
+/* ProjGeomFactory<DetFanLine, DetFanLine>::create(ProjectionMatrix)
+ * (src/cpp/io/geom_reader/proj_geom_factory_proj_mat.cpp:7-26): the CONE_FLAT view of a 3 x 4
+ * matrix. As in the reference, src_det_dist is the focal length in detector-row pixels; multiply
+ * it by the pixel width before use. src_iso_dist = |src_pos|. */
+gct_status gct_proj_geom_from_matrix(const double *matrix, gct_view_geom *out);
+
 /* Replaces GCT::Geom::getRotationGeom (src/cpp/geom/rotation_geom.h:90-115,
  * src/cpp/geom/rotation_geom.cpp:7-134). rot_ang / rel_rot_ang may be NULL; otherwise they
  * receive num_views angles each. Returns GCT_ERR_INVALID_ARG where the reference returns
