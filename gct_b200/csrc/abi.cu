@@ -477,6 +477,71 @@ void execute_host(gct_fdk_plan *p, const float *proj_host, float *vol_host, cuda
     cuda_check(cudaStreamSynchronize(s), "reconstruction");
 }
 
+// Streaming FDK with a bounded device footprint for the projections: views go through two
+// staging slots of `chunk` views (upload of the next chunk on the copy stream while the current
+// one is filtered) into a view-major stack of one chunk, and each chunk is backprojected into the
+// device volume (chunk 0 stores, later chunks add). Replaces reconFDKLowMem
+// (src/cuda/recon/fdk_axial.cuh:91-149), which moves one view at a time with a synchronous copy.
+void execute_host_budget(gct_fdk_plan *p, const float *proj_host, float *vol_host, uint64_t budget, cudaStream_t s)
+{
+    if (!proj_host || !vol_host) gct::fail(GCT_ERR_INVALID_ARG, "NULL projection or volume pointer");
+    const size_t pix = static_cast<size_t>(p->nr) * p->nc;
+    const size_t vol_n = static_cast<size_t>(p->vol.nx) * p->vol.ny * p->vol.nz;
+    const bool f16 = p->opts.storage == GCT_STORAGE_F16;
+    const size_t per_view = 2 * pix * sizeof(float) + p->view_bytes() + (f16 ? 3 * sizeof(float) : 0);
+    const size_t chunk = std::min<size_t>(static_cast<size_t>(p->nv), (budget > 512 ? budget - 512 : 0) / per_view);
+    if (chunk < 1)
+        gct::fail(GCT_ERR_BUDGET, "one view needs " + std::to_string(per_view) + " bytes of streaming buffers; the budget is " +
+                                      std::to_string(budget));
+    if (p->stream_chunk != static_cast<int>(chunk)) {
+        p->stream_stage.alloc(2 * chunk * pix, "streaming projection slots");
+        p->stream_ws.alloc(((chunk * p->view_bytes() + 255) & ~static_cast<size_t>(255)) +
+                               (f16 ? 3 * chunk * sizeof(float) : 0),
+                           "streaming filtered-projection stack");
+        p->stream_chunk = static_cast<int>(chunk);
+    }
+    if (!p->host_vol.p) p->host_vol.alloc(vol_n, "staging volume");
+    if (!p->copy_stream) cuda_check(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking), "copy stream");
+    for (cudaEvent_t &e : p->stream_events)
+        if (!e) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    cudaEvent_t *filled = p->stream_events, *freed = p->stream_events + 2;
+    // the slots are free once everything earlier on `s` (a previous call) is done
+    cuda_check(cudaEventRecord(freed[0], s), "event record");
+    cuda_check(cudaEventRecord(freed[1], s), "event record");
+    unsigned char *ws = p->stream_ws.p;
+    float *scales = reinterpret_cast<float *>(ws + ((chunk * p->view_bytes() + 255) & ~static_cast<size_t>(255)));
+    const int nchunks = static_cast<int>((p->nv + chunk - 1) / chunk);
+    for (int c = 0; c < nchunks; ++c) {
+        const int vb = c * static_cast<int>(chunk), vc = std::min(static_cast<int>(chunk), p->nv - vb);
+        const int slot = c & 1;
+        float *stage = p->stream_stage.p + slot * chunk * pix;
+        cuda_check(cudaStreamWaitEvent(p->copy_stream, freed[slot], 0), "stream wait");
+        cuda_check(cudaMemcpyAsync(stage, proj_host + static_cast<size_t>(vb) * pix, sizeof(float) * pix * vc,
+                                   cudaMemcpyHostToDevice, p->copy_stream),
+                   "projection upload");
+        cuda_check(cudaEventRecord(filled[slot], p->copy_stream), "event record");
+        cuda_check(cudaStreamWaitEvent(s, filled[slot], 0), "stream wait");
+        // prepare() and run_backproject() address view v at view-0 bases: shifting them by vb views
+        // puts this chunk at the start of the slot and of the chunk stack
+        StackRef st;
+        st.quads = reinterpret_cast<unsigned char *>(reinterpret_cast<uintptr_t>(ws) -
+                                                     static_cast<uintptr_t>(vb) * p->view_bytes());
+        if (f16) {
+            st.amax = scales - vb;
+            st.vscale = scales + chunk - vb;
+            st.vinv = scales + 2 * chunk - vb;
+        }
+        const float *proj0 = reinterpret_cast<const float *>(reinterpret_cast<uintptr_t>(stage) -
+                                                             static_cast<uintptr_t>(vb) * pix * sizeof(float));
+        prepare(p, proj0, st, vb, vc, s);
+        cuda_check(cudaEventRecord(freed[slot], s), "event record");
+        run_backproject(p, st, p->host_vol.p, vb, vc, c > 0, s);
+    }
+    cuda_check(cudaMemcpyAsync(vol_host, p->host_vol.p, sizeof(float) * vol_n, cudaMemcpyDeviceToHost, s),
+               "volume download");
+    cuda_check(cudaStreamSynchronize(s), "reconstruction");
+}
+
 namespace {
 
 struct PlanHolder {
@@ -862,6 +927,16 @@ gct_status gct_fdk_execute_noalloc(gct_fdk_plan *plan, const float *proj_dev, fl
     });
 }
 
+gct_status gct_fdk_execute_host_budget(gct_fdk_plan *plan, const float *proj_host, float *vol_host,
+                                       uint64_t device_bytes, void *stream)
+{
+    return guarded([&] {
+        if (!plan) gct::fail(GCT_ERR_INVALID_ARG, "NULL plan");
+        DeviceGuard dg(plan->device);
+        execute_host_budget(plan, proj_host, vol_host, device_bytes, static_cast<cudaStream_t>(stream));
+    });
+}
+
 gct_status gct_reconstruct_ex(const gct_ct_geom *geom, const gct_vol_geom *vol,
                               const gct_filt_params *filt, const gct_fdk_opts *opts,
                               const float *proj_host, float *vol_host)
@@ -874,6 +949,17 @@ gct_status gct_reconstruct_ex(const gct_ct_geom *geom, const gct_vol_geom *vol,
         gct_fdk_plan *p = h.p;
         const size_t proj_n = static_cast<size_t>(p->nv) * p->nr * p->nc;
         const size_t vol_n = static_cast<size_t>(p->vol.nx) * p->vol.ny * p->vol.nz;
+        // reconFDK's choice (src/cuda/recon/fdk_axial.cuh:68-89): all projections on the device
+        // when they, the volume and the filtered stack need under 75 % of the device memory,
+        // else the streaming path with half of the memory left after the volume
+        size_t free_b = 0, total_b = 0;
+        cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+        const double req = static_cast<double>(proj_n + vol_n) * sizeof(float) + static_cast<double>(p->workspace_bytes());
+        if (req >= 0.75 * static_cast<double>(total_b)) {
+            const size_t vol_b = vol_n * sizeof(float);
+            execute_host_budget(p, proj_host, vol_host, free_b > vol_b ? (free_b - vol_b) / 2 : 0, nullptr);
+            return;
+        }
         DevBuf<float> dproj, dvol;
         dproj.alloc(proj_n, "projection stack");
         dvol.alloc(vol_n, "volume");

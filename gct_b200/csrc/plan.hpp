@@ -118,10 +118,18 @@ struct gct_fdk_plan {
     DevBuf<float> host_proj, host_vol;
     cudaStream_t copy_stream = nullptr;
     std::vector<cudaEvent_t> chunk_events;
+    // bounded-memory streaming (gct_fdk_execute_host_budget): two projection slots of
+    // stream_chunk views and a view-major stack of one chunk
+    DevBuf<float> stream_stage;
+    DevBuf<unsigned char> stream_ws;
+    int stream_chunk = 0;
+    cudaEvent_t stream_events[4] = {nullptr, nullptr, nullptr, nullptr};  // slot filled x2, slot free x2
 
     ~gct_fdk_plan()
     {
         for (cudaEvent_t e : chunk_events) cudaEventDestroy(e);
+        for (cudaEvent_t e : stream_events)
+            if (e) cudaEventDestroy(e);
         if (copy_stream) cudaStreamDestroy(copy_stream);
     }
 

@@ -316,6 +316,17 @@ gct_status gct_fdk_backproject(gct_fdk_plan *plan, const void *workspace, float 
 gct_status gct_fdk_execute_host(gct_fdk_plan *plan, const float *proj_host, float *vol_host,
                                 void *stream);
 
+/* Host buffers with a bounded device footprint for the projections (stacks larger than the
+ * device): the views stream through two upload slots and a filtered stack of one chunk, where a
+ * chunk is as many views as device_bytes holds (two float32 views plus one filtered view each),
+ * and each chunk is backprojected into the plan's device volume. The volume itself must fit
+ * besides. Replaces reconFDKLowMem (src/cuda/recon/fdk_axial.cuh:91-149), which the reference
+ * picks when the whole stack needs 75 % of the device memory or more; gct_reconstruct_ex applies
+ * the same rule and calls this path with half the memory left after the volume.
+ * GCT_ERR_BUDGET if device_bytes holds no view. Synchronous on `stream`. */
+gct_status gct_fdk_execute_host_budget(gct_fdk_plan *plan, const float *proj_host, float *vol_host,
+                                       uint64_t device_bytes, void *stream);
+
 /* Full FDK on device buffers without allocating device memory. No counterpart in the reference.
  * For callers that cannot allocate device memory when they reconstruct: a host application whose
  * own memory manager has already reserved the device's memory, or an acquisition loop that

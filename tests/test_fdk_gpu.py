@@ -235,3 +235,27 @@ def test_flat_panel_views_from_projection_matrices():
     assert rel_rms(got, base) <= 1e-6
     ref = orc.fdk(case.og, case.ov, proj).reshape(got.shape)
     assert rel_rms(got, ref) <= 1e-4
+
+
+@pytest.mark.parametrize("storage", [g.STORAGE_F32, g.STORAGE_F16])
+def test_streaming_budget_path(storage):
+    # a budget of a few views: many chunks through the two upload slots; view-major chunk stacks
+    # and the plain kernel, so against execute() with the quarter-turn form off only the chunked
+    # summation differs (rounding; FP16 scale roundings can flip: 1e-5)
+    import torch
+    case = make_case("cone_flat")
+    proj = oracle_projections(case)
+    with g.FdkPlan(case.cg, case.vg, opts=g.FdkOptions(storage=storage, symmetry=g.SYMMETRY_OFF)) as plan:
+        dev = torch.empty(case.vg.shape, dtype=torch.float32, device="cuda")
+        plan.execute(torch.from_numpy(proj).cuda(), dev)
+        torch.cuda.synchronize()
+        pix = case.cg.num_rows * case.cg.num_cols
+        per_view = 2 * pix * 4 + (case.cg.num_rows + 4) * (case.cg.num_cols + 4) * (16 if storage == g.STORAGE_F32 else 8)
+        out = np.empty(case.vg.shape, np.float32)
+        plan.execute_host_budget(proj, out, 7 * per_view + 4096)
+        assert rel_rms(out, dev.cpu().numpy()) <= (1e-6 if storage == g.STORAGE_F32 else 1e-5)
+        again = np.empty_like(out)
+        plan.execute_host_budget(proj, again, 7 * per_view + 4096)
+        assert np.array_equal(out, again)
+        with pytest.raises(g.GctError, match="budget"):
+            plan.execute_host_budget(proj, out, per_view // 2)
