@@ -69,7 +69,7 @@ class gct_geom_params(C.Structure):
 class gct_fdk_opts(C.Structure):
     _fields_ = [("filter", C.c_int32), ("storage", C.c_int32), ("z_per_thread", C.c_int32),
                 ("block_x", C.c_int32), ("block_y", C.c_int32), ("symmetry", C.c_int32),
-                ("reserved", C.c_int32 * 2)]
+                ("scan", C.c_int32), ("reserved", C.c_int32 * 1)]
 
 
 class gct_batch_item(C.Structure):
@@ -128,6 +128,8 @@ SIGNATURES = {
     "gct_proj_matrix_decompose": [P(C.c_double), P(gct_proj_matrix)],
     "gct_proj_matrix_compose": [P(gct_view_geom), C.c_double, C.c_double, P(gct_proj_matrix)],
     "gct_proj_geom_from_matrix": [P(C.c_double), P(gct_view_geom)],
+    "gct_spiral_geom_check": [P(gct_ct_geom), P(C.c_uint32), P(C.c_double)],
+    "gct_spiral_proj_indices": [P(gct_ct_geom), C.c_double, P(C.c_int64), P(C.c_int64)],
     "gct_rotation_geom_get": [P(gct_ct_geom), P(gct_rotation_geom), P(C.c_double), P(C.c_double)],
     "gct_is_valid_axial_recon": [P(gct_ct_geom), C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32,
                                  P(C.c_int32)],

@@ -120,8 +120,19 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
     for (int v = 0; v < p->nv; ++v)
         fview[v] = make_float4(static_cast<float>(vd[v].c0), static_cast<float>(vd[v].r0),
                                static_cast<float>(vd[v].sdd), 0.f);
-    const std::vector<double> parker_d = gct::parker_table(p->geom, p->rot);
-    std::vector<float> parker(parker_d.begin(), parker_d.end());
+    if (p->opts.scan != GCT_SCAN_AXIAL && p->opts.scan != GCT_SCAN_SPIRAL)
+        gct::fail(GCT_ERR_INVALID_ARG, "unknown scan option");
+    p->spiral = p->opts.scan == GCT_SCAN_SPIRAL;
+    gct::SpiralInfo spiral_si;
+    if (p->spiral) spiral_si = gct::spiral_info(p->geom);  // validates like SpiralCTGeom
+    // spiral scans: no Parker weights (fdk_spiral.cuh applies cosine weights and the filter only)
+    std::vector<float> parker;
+    if (p->spiral) {
+        parker.assign(static_cast<size_t>(p->nv) * p->nc, 1.0f);
+    } else {
+        const std::vector<double> parker_d = gct::parker_table(p->geom, p->rot);
+        parker.assign(parker_d.begin(), parker_d.end());
+    }
     const std::vector<double> taps = gct::ramp_taps(kind, g->det_row, p->filt);
     double l1 = 0.0;
     for (double t : taps) l1 += std::fabs(t);
@@ -214,6 +225,22 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
     // its row buffer already
     if (p->sym && !p->ybuf.p)
         p->ybuf.alloc(static_cast<size_t>(p->nv) * p->nr * p->nc, "filtered rows of quarter-turn stacks");
+    if (p->spiral) {
+        // one slice per thread along z: each slice has its own window of views
+        p->sym = 0;
+        p->zpt = 1;
+        if (p->opts.block_x <= 0) p->bx = 32;
+        if (p->opts.block_y <= 0) p->by = 8;
+        std::vector<int2> win(p->kz);
+        const double z0 = vol->mid[2] - (vol->nz - 1.0) * vol->dz / 2.0;
+        for (int k = 0; k < p->kz; ++k) {
+            long long first = 0, last = 0;
+            gct::spiral_window(spiral_si, z0 + k * vol->dz, &first, &last);
+            win[k] = (first > 0 && last < p->nv) ? make_int2(static_cast<int>(first), static_cast<int>(last - first))
+                                                 : make_int2(0, 0);
+        }
+        p->slice_views.upload(win.data(), win.size(), "spiral slice windows");
+    }
     p->zpt_sym = p->opts.z_per_thread > 0 ? std::min(p->zpt, 8) : (vol3d ? (f16 ? 8 : 4) : 1);
     p->bx_sym = p->opts.block_x > 0 ? p->bx : (vol3d ? (f16 ? 2 : 4) : 8);
     p->by_sym = p->opts.block_y > 0 ? p->by : (vol3d ? (f16 ? 32 : 16) : 8);
@@ -327,6 +354,7 @@ gct::BpArgs bp_args(const gct_fdk_plan *p, const StackRef &st, float *vol, int v
     ba.v_begin = v_begin;
     ba.v_count = v_count;
     ba.quarter = st.quarter;
+    ba.slice_views = p->slice_views.p;
     ba.vol = vol;
     ba.nx = p->kx;
     ba.ny = p->ky;
@@ -599,6 +627,28 @@ gct_status gct_proj_geom_from_matrix(const double *matrix, gct_view_geom *out)
     return guarded([&] {
         if (!matrix || !out) gct::fail(GCT_ERR_INVALID_ARG, "NULL argument");
         *out = gct::view_from_projection_matrix(gct::decompose_projection_matrix(matrix));
+    });
+}
+
+gct_status gct_spiral_geom_check(const gct_ct_geom *geom, uint32_t *num_proj_per_rot, double *pitch_mm_per_rad)
+{
+    return guarded([&] {
+        gct::check_ct_geom(geom);
+        const gct::SpiralInfo si = gct::spiral_info(*geom);
+        if (num_proj_per_rot) *num_proj_per_rot = si.npr;
+        if (pitch_mm_per_rad) *pitch_mm_per_rad = si.pitch;
+    });
+}
+
+gct_status gct_spiral_proj_indices(const gct_ct_geom *geom, double slice_pos_mm, int64_t *first, int64_t *last)
+{
+    return guarded([&] {
+        gct::check_ct_geom(geom);
+        if (!first || !last) gct::fail(GCT_ERR_INVALID_ARG, "NULL argument");
+        long long f = 0, l = 0;
+        gct::spiral_window(gct::spiral_info(*geom), slice_pos_mm, &f, &l);
+        *first = f;
+        *last = l;
     });
 }
 

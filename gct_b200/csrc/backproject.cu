@@ -347,10 +347,17 @@ __global__ void __launch_bounds__(256) bp_kernel(BpArgs a)
     const int k0 = blockIdx.z * ZPT;
     if (threadIdx.x == 0 && threadIdx.y == 0)
         s_box = block_box(a, blockIdx.x * blockDim.x, blockIdx.y * blockDim.y, blockDim.x, blockDim.y, k0, ZPT);
-    // the first barrier of bp_column orders this store before any read
-    bp_column<FAMILY, Q, ZPT, ZAFFINE, ES>(a, i, j, k0, i < a.nx && j < a.ny, kViewsPerChunk, s_coef, s_cls, &s_box,
-                                       threadIdx.y * blockDim.x + threadIdx.x, blockDim.x * blockDim.y,
-                                       a.accumulate ? kBpAccumulate : kBpStore);
+    BpArgs la = a;
+    if (a.slice_views) {  // spiral scans: this slice's rotation of views (ZPT == 1, uniform per block)
+        const int2 w = a.slice_views[k0 < a.nz ? k0 : a.nz - 1];
+        const int b = max(w.x, a.v_begin), e = min(w.x + w.y, a.v_begin + a.v_count);
+        la.v_begin = b;
+        la.v_count = max(0, e - b);
+    }
+    // the first barrier of bp_column orders the s_box store before any read
+    bp_column<FAMILY, Q, ZPT, ZAFFINE, ES>(la, i, j, k0, i < a.nx && j < a.ny, kViewsPerChunk, s_coef, s_cls, &s_box,
+                                           threadIdx.y * blockDim.x + threadIdx.x, blockDim.x * blockDim.y,
+                                           a.accumulate ? kBpAccumulate : kBpStore);
 }
 
 template <int FAMILY, class Q, int ZPT>

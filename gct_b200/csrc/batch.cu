@@ -29,6 +29,7 @@ BpItem make_item(const gct_fdk_plan *p, const StackRef &st, float *vol, const Ti
 {
     if (c.bx * c.by != kQueueThreads || c.bx < 1 || !queue_zpt_ok(c.zpt) || c.vps < 1 || c.vps > kQueueMaxVps)
         fail(GCT_ERR_INVALID_ARG, "queue tile shape must cover 256 threads with z per thread 1, 4, 8 or 16");
+    if (p->spiral) fail(GCT_ERR_NOT_SUPPORTED, "spiral plans run through gct_fdk_execute*, not batches or the server");
     BpItem it;
     it.a = bp_args(p, st, vol, 0, p->nv);
     it.family = static_cast<int>(p->family);

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <functional>
 #include <numeric>
 
 namespace gct {
@@ -647,6 +648,55 @@ gct_view_geom view_from_projection_matrix(const ProjMatrix &pm)
     v.src_iso_dist = norm3(v.src_pos);
     v.rot_ang = view_rot_angle(GCT_GEOM_CONE_FLAT, v);
     return v;
+}
+
+// ---- spiral scans --------------------------------------------------------------------------------
+
+// SpiralCTGeom's constructor (src/cpp/geom/spiral_ct_geom.h:30-50): a 2D detector, a positive
+// number of projections per rotation, source z sorted either way and a positive pitch (the source
+// z travel over one rotation / 2 pi).
+SpiralInfo spiral_info(const gct_ct_geom &g)
+{
+    const auto kind = static_cast<gct_geom_kind>(g.kind);
+    if (!is_2d_detector(kind) || family_of(kind) == Family::Affine)
+        fail(GCT_ERR_NOT_SUPPORTED, "spiral scans need a cone-beam 2D detector (flat or cylindrical)");
+    RotationInfo ri;
+    if (!rotation_info(g, &ri)) fail(GCT_ERR_INVALID_ARG, "Invalid X-ray source trajectory.");
+    if (ri.num_proj_per_rot == 0)
+        fail(GCT_ERR_INVALID_ARG, "Invalid spiral CT geometry: number of projections per rotation should not be zero.");
+    SpiralInfo si;
+    si.npr = ri.num_proj_per_rot;
+    si.src_z.resize(g.num_views);
+    for (unsigned v = 0; v < g.num_views; ++v) si.src_z[v] = g.views[v].src_pos[2];
+    if (!std::is_sorted(si.src_z.begin(), si.src_z.end()) &&
+        !std::is_sorted(si.src_z.begin(), si.src_z.end(), std::greater<>()))
+        fail(GCT_ERR_INVALID_ARG, "Invalid spiral CT geometry: the z-coordinate of source position should be sorted "
+                                  "either in ascending or descending order.");
+    if (si.npr >= g.num_views)
+        fail(GCT_ERR_INVALID_ARG, "Invalid spiral CT geometry: the scan covers less than one rotation after the first");
+    si.pitch = std::fabs(si.src_z.front() - si.src_z[si.npr]) / kTwoPi;
+    if (!(si.pitch > 0.0))
+        fail(GCT_ERR_INVALID_ARG, "Invalid spiral CT geometry: spiral pitch cannot be zero or negative.");
+    return si;
+}
+
+// firstAndLastProjIndices (spiral_ct_geom.h:57-75): the view whose source z is nearest the slice
+// (the first of equals), and the npr views starting npr / 2 before it. Signed here: the
+// reference's unsigned first index wraps when it would be negative, and fdk_spiral.cuh:60-79 then
+// does no work for the slice, as it does for first == 0 or last >= num_views.
+void spiral_window(const SpiralInfo &si, double slice_pos, long long *first, long long *last)
+{
+    size_t mid = 0;
+    double best = std::fabs(si.src_z[0] - slice_pos);
+    for (size_t v = 1; v < si.src_z.size(); ++v) {
+        const double d = std::fabs(si.src_z[v] - slice_pos);
+        if (d < best) {
+            best = d;
+            mid = v;
+        }
+    }
+    *first = static_cast<long long>(mid) - static_cast<long long>(si.npr / 2);
+    *last = *first + si.npr;
 }
 
 }  // namespace gct

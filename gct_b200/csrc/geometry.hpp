@@ -54,6 +54,15 @@ void check_vol_geom(const gct_vol_geom *v, bool volume_3d);
 
 gct_view_geom make_view(gct_geom_kind kind, const gct_geom_params &p, unsigned idx);
 
+// Spiral (helical) scans.
+struct SpiralInfo {
+    unsigned npr = 0;            // projections per rotation
+    double pitch = 0.0;          // source z travel per radian (mm)
+    std::vector<double> src_z;   // per view
+};
+SpiralInfo spiral_info(const gct_ct_geom &g);
+void spiral_window(const SpiralInfo &si, double slice_pos, long long *first, long long *last);
+
 // Projection matrices of flat-panel views (row-major 3 x 4 matrix, K, R, source), FP64.
 struct ProjMatrix {
     double m[12], K[9], R[9], src[3];

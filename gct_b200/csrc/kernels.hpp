@@ -74,6 +74,9 @@ struct BpArgs {
     float umax = 0.f, vmax = 0.f;  // nc, nr
     int accumulate = 0;
     int quarter = 0;  // quad_layout of the stack
+    // spiral scans (one voxel per thread along z): slice k backprojects views [x, x + y) of
+    // slice_views[k], intersected with [v_begin, v_begin + v_count)
+    const int2 *slice_views = nullptr;
     // quarter-turn launches (quarter > 0): v_begin / v_count count base views, whose partners are
     // v + q * quarter (q = 1..3); sym (+1 / -1) is the turn that maps their voxel columns
     int sym = 0;

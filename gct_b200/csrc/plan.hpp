@@ -103,6 +103,9 @@ struct gct_fdk_plan {
     // run over the first quarter of the views and of the (x, y) columns, each thread serving the
     // four rotated columns from the four partner views, with zpt_sym voxels along z.
     int sym = 0, zpt_sym = 8, bx_sym = 8, by_sym = 16;
+    // spiral scans: per-slice view windows (first, count); count 0 leaves the slice zero
+    bool spiral = false;
+    DevBuf<int2> slice_views;
     DevBuf<float4> fview;
     DevBuf<float> parker;
     DevBuf<float2> H, tw;

@@ -355,6 +355,27 @@ class AxialCTGeom:
 CTGeom = AxialCTGeom
 
 
+class SpiralCTGeom(AxialCTGeom):
+    """Geometry of a spiral (helical) cone-beam scan: GCT::Geom::SpiralCTGeom
+    (src/cpp/geom/spiral_ct_geom.h:9-95). The constructor checks what the reference's does
+    (projections per rotation > 0, source z sorted either way, positive pitch)."""
+
+    def __init__(self, det_geom: tuple, proj_geom):
+        super().__init__(det_geom, proj_geom)
+        npr, pitch = C.c_uint32(0), C.c_double(0.0)
+        _lib.check(_lib.load().gct_spiral_geom_check(C.byref(self.struct()), C.byref(npr), C.byref(pitch)))
+        self.num_proj_per_rot = int(npr.value)
+        self.spiral_pitch = float(pitch.value)  # source z travel per radian (mm)
+
+    def first_and_last_proj_indices(self, slice_pos_mm: float) -> tuple:
+        """[first, last) of the rotation of views centred on the view nearest the slice (first may
+        be negative where the reference's unsigned index wraps)."""
+        f, l = C.c_int64(0), C.c_int64(0)
+        _lib.check(_lib.load().gct_spiral_proj_indices(C.byref(self.struct()), float(slice_pos_mm), C.byref(f),
+                                                       C.byref(l)))
+        return int(f.value), int(l.value)
+
+
 @dataclass(frozen=True)
 class EqDistSampler:
     num_samples: int

@@ -12,12 +12,13 @@ calls fail.
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
 from dataclasses import dataclass
 
 import numpy as np
 
 from . import _lib
-from .geometry import ApodFunc, AxialCTGeom, ProjectionStack, ReconImg, ReconImgGeom
+from .geometry import ApodFunc, AxialCTGeom, ProjectionStack, ReconImg, ReconImgGeom, SpiralCTGeom
 
 FILTER_FFT = 0
 FILTER_TOEPLITZ_BF16X3 = 1
@@ -27,6 +28,8 @@ STORAGE_F16 = 1
 SYMMETRY_AUTO = 0
 SYMMETRY_OFF = 1
 SYMMETRY_ON = 2
+SCAN_AXIAL = 0
+SCAN_SPIRAL = 1
 
 
 @dataclass
@@ -47,11 +50,12 @@ class FdkOptions:
     block_x: int = 0
     block_y: int = 0
     symmetry: int = SYMMETRY_AUTO
+    scan: int = SCAN_AXIAL
 
     def struct(self) -> _lib.gct_fdk_opts:
         o = _lib.gct_fdk_opts()
         o.filter, o.storage, o.z_per_thread = self.filter, self.storage, self.z_per_thread
-        o.block_x, o.block_y, o.symmetry = self.block_x, self.block_y, self.symmetry
+        o.block_x, o.block_y, o.symmetry, o.scan = self.block_x, self.block_y, self.symmetry, self.scan
         return o
 
 
@@ -89,7 +93,8 @@ def _stream(stream) -> int | None:
 def reconstruct(cg: AxialCTGeom, proj, vol, filt: FiltParams | None = None,
                 opts: FdkOptions | None = None) -> None:
     """Host-to-host FDK: ``proj`` is a ProjectionStack (or float32 array [view][row][col]),
-    ``vol`` a ReconImg whose ``elements`` receive the result."""
+    ``vol`` a ReconImg whose ``elements`` receive the result. A SpiralCTGeom selects the spiral
+    FDK (reconFDK(SpiralCTGeom), src/cuda/recon/fdk_spiral.cuh:33-94)."""
     pe = proj.elements if isinstance(proj, ProjectionStack) else np.ascontiguousarray(proj, dtype=np.float32)
     if not (pe.flags.c_contiguous and pe.dtype == np.float32):
         pe = np.ascontiguousarray(pe, dtype=np.float32)
@@ -102,9 +107,11 @@ def reconstruct(cg: AxialCTGeom, proj, vol, filt: FiltParams | None = None,
         raise TypeError("vol must be a ReconImg")
     fp = C.POINTER(C.c_float)
     lib = _lib.load()
+    o = opts or FdkOptions()
+    if isinstance(cg, SpiralCTGeom):
+        o = dataclasses.replace(o, scan=SCAN_SPIRAL)
     _lib.check(lib.gct_reconstruct_ex(C.byref(cg.struct()), C.byref(geom.struct()),
-                                      C.byref((filt or FiltParams()).struct()),
-                                      C.byref((opts or FdkOptions()).struct()),
+                                      C.byref((filt or FiltParams()).struct()), C.byref(o.struct()),
                                       pe.ctypes.data_as(fp), ve.ctypes.data_as(fp)))
 
 

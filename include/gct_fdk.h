@@ -165,6 +165,15 @@ enum {
     GCT_SYMMETRY_OFF = 1,
     GCT_SYMMETRY_ON = 2
 };
+enum {
+    GCT_SCAN_AXIAL = 0,  /* circular scans: GCT::Recon::CUDA::reconFDK(AxialCTGeom) */
+    /* spiral (helical) cone-beam scans, Wang's FDK: every z slice backprojects the one rotation of
+     * views centred on the view whose source z is nearest the slice, with cosine weights and the
+     * ramp filter but no Parker weights; slices whose rotation would start at view 0 or end at or
+     * after the last view stay zero (GCT::Recon::CUDA::reconFDK(SpiralCTGeom),
+     * src/cuda/recon/fdk_spiral.cuh:33-94; src/cpp/geom/spiral_ct_geom.h:30-95). */
+    GCT_SCAN_SPIRAL = 1
+};
 typedef struct gct_fdk_opts {
     int32_t filter;        /* GCT_FILTER_* */
     int32_t storage;       /* GCT_STORAGE_* */
@@ -172,7 +181,8 @@ typedef struct gct_fdk_opts {
     int32_t block_x;       /* backprojection block shape; 0 = tuned default */
     int32_t block_y;
     int32_t symmetry;      /* GCT_SYMMETRY_* */
-    int32_t reserved[2];
+    int32_t scan;          /* GCT_SCAN_* */
+    int32_t reserved[1];
 } gct_fdk_opts;
 
 typedef struct gct_fdk_plan gct_fdk_plan;
@@ -217,6 +227,16 @@ gct_status gct_proj_matrix_compose(const gct_view_geom *view, double pix_width_m
  * matrix. As in the reference, src_det_dist is the focal length in detector-row pixels; multiply
  * it by the pixel width before use. src_iso_dist = |src_pos|. */
 gct_status gct_proj_geom_from_matrix(const double *matrix, gct_view_geom *out);
+
+/* GCT::Geom::SpiralCTGeom's checks (src/cpp/geom/spiral_ct_geom.h:30-50): a cone-beam 2D
+ * detector, projections per rotation > 0, source z sorted either way and a positive pitch; returns
+ * the projections per rotation and the pitch (source z travel per radian, mm). */
+gct_status gct_spiral_geom_check(const gct_ct_geom *geom, uint32_t *num_proj_per_rot, double *pitch_mm_per_rad);
+
+/* SpiralCTGeom::firstAndLastProjIndices (spiral_ct_geom.h:57-75): the views [first, last) of the
+ * rotation centred on the view whose source z is nearest slice_pos_mm. Signed: first is negative
+ * where the reference's unsigned index wraps. */
+gct_status gct_spiral_proj_indices(const gct_ct_geom *geom, double slice_pos_mm, int64_t *first, int64_t *last);
 
 /* Replaces GCT::Geom::getRotationGeom (src/cpp/geom/rotation_geom.h:90-115,
  * src/cpp/geom/rotation_geom.cpp:7-134). rot_ang / rel_rot_ang may be NULL; otherwise they

@@ -20,6 +20,8 @@
  *                        142-345, src/cuda/geom/coord_trans_img.cuh:52-66, texture addressing of
  *                        src/cuda/data/nd_array_texture.cuh:33-56 (linear filter, border 0)
  *   final scale          src/cuda/recon/fdk_axial.cuh:196-199
+ *   spiral scans         src/cuda/recon/fdk_spiral.cuh:33-94 (no Parker weights: or_filter_np;
+ *                        the per-slice view windows are restated in oracle.py)
  * The texture unit's 8-bit fractional lerp weights can be emulated (lerp_bits = 8) to quantify
  * that difference separately from the exact bilinear interpolation (lerp_bits = 0).
  */
@@ -359,12 +361,14 @@ static unsigned alias_free_len(unsigned n)
 }
 
 static int run_filter(const or_geom *g, const float *proj, double fc, int apod, const long *rows,
-                      long nrows, double *out, int use_fft, int nthreads)
+                      long nrows, double *out, int use_fft, int nthreads, int use_parker)
 {
     const unsigned n = g->nc;
     double *parker = malloc(sizeof(double) * (size_t)g->nv * n);
     double *taps = malloc(sizeof(double) * n);
-    if (!parker || !taps || or_parker(g, parker) != 0) {
+    if (parker && !use_parker)
+        for (size_t i = 0; i < (size_t)g->nv * n; ++i) parker[i] = 1.0;
+    if (!parker || !taps || (use_parker && or_parker(g, parker) != 0)) {
         free(parker);
         free(taps);
         return -1;
@@ -416,7 +420,14 @@ static int run_filter(const or_geom *g, const float *proj, double fc, int apod, 
 int or_filter(const or_geom *g, const float *proj, double fc, int apod, int use_fft, double *out,
               int nthreads)
 {
-    return run_filter(g, proj, fc, apod, NULL, (long)g->nv * g->nr, out, use_fft, nthreads);
+    return run_filter(g, proj, fc, apod, NULL, (long)g->nv * g->nr, out, use_fft, nthreads, 1);
+}
+
+/* The same without Parker weights (the spiral FDK weights by cosine only). */
+int or_filter_np(const or_geom *g, const float *proj, double fc, int apod, int use_fft, double *out,
+                 int nthreads)
+{
+    return run_filter(g, proj, fc, apod, NULL, (long)g->nv * g->nr, out, use_fft, nthreads, 0);
 }
 
 /* ---- backprojection ----------------------------------------------------------------------- */
@@ -669,7 +680,7 @@ int or_fdk(const or_geom *g, const or_vol *vol, const float *proj, double fc, in
             rows[s] = (long)i;
             slot[i] = s++;
         }
-    if (run_filter(g, proj, fc, apod, rows, nsel, filt, use_fft, nthreads) != 0) {
+    if (run_filter(g, proj, fc, apod, rows, nsel, filt, use_fft, nthreads, 1) != 0) {
         free(slot);
         free(rows);
         free(filt);

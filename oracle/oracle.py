@@ -75,6 +75,7 @@ def load() -> C.CDLL:
             lib.or_cos_weight.restype = C.c_double
             lib.or_parker.argtypes = [C.POINTER(_Geom), dp]
             lib.or_filter.argtypes = [C.POINTER(_Geom), vp, C.c_double, C.c_int, C.c_int, dp, C.c_int]
+            lib.or_filter_np.argtypes = [C.POINTER(_Geom), vp, C.c_double, C.c_int, C.c_int, dp, C.c_int]
             lib.or_backproject.argtypes = [C.POINTER(_Geom), C.POINTER(_Vol), dp, vp, C.c_long, C.c_int, dp, C.c_int]
             lib.or_fdk.argtypes = [C.POINTER(_Geom), C.POINTER(_Vol), vp, C.c_double, C.c_int, C.c_int, vp,
                                    C.c_long, C.c_int, dp, C.c_int]
@@ -178,10 +179,11 @@ def cos_weight(g: Geometry, v: int, r: int, c: int) -> float:
 
 
 def filter_stack(g: Geometry, proj: np.ndarray, cut_off: float = 1.0, apod: int = 0, use_fft: bool = False,
-                 threads: int | None = None) -> np.ndarray:
+                 threads: int | None = None, parker: bool = True) -> np.ndarray:
     p = np.ascontiguousarray(proj, dtype=np.float32).reshape(g.shape)
     out = np.zeros(g.shape)
-    rc = load().or_filter(C.byref(g._s), p.ctypes.data, cut_off, apod, int(use_fft), _dp(out), threads or os.cpu_count())
+    fn = load().or_filter if parker else load().or_filter_np
+    rc = fn(C.byref(g._s), p.ctypes.data, cut_off, apod, int(use_fft), _dp(out), threads or os.cpu_count())
     if rc != 0:
         raise ValueError("invalid trajectory")
     return out
@@ -213,6 +215,46 @@ def fdk(g: Geometry, vol: Volume, proj: np.ndarray, voxels: np.ndarray | None = 
                        lerp_bits, _dp(out), threads or os.cpu_count())
     if rc != 0:
         raise ValueError("oracle FDK failed (invalid trajectory or allocation)")
+    return out
+
+
+def spiral_windows(g: Geometry, vol: Volume) -> list:
+    """Per z slice, the views [first, last) the spiral FDK backprojects, or None for a slice it
+    leaves zero. Restates src/cpp/geom/spiral_ct_geom.h:57-75 (firstAndLastProjIndices: the view
+    whose source z is nearest the slice, the first of equals, and the num_proj_per_rot views
+    starting num_proj_per_rot / 2 before it) and src/cuda/recon/fdk_spiral.cuh:60-79 (a slice
+    is reconstructed only when first > 0 and last < num_views; the reference's unsigned first
+    index wraps below zero, which also leaves the slice zero)."""
+    rot = rotation(g)
+    if rot is None or rot[3] == 0:
+        raise ValueError("invalid spiral trajectory")
+    npr = rot[3]
+    z = np.array([v["src_pos"][2] for v in g.views], dtype=np.float64)
+    z0 = vol.mid[2] - (vol.nz - 1) * vol.dz / 2.0
+    out = []
+    for k in range(vol.nz):
+        mid = int(np.argmin(np.abs(z - (z0 + k * vol.dz))))
+        first = mid - npr // 2
+        last = first + npr
+        out.append((first, last) if (first > 0 and last < g.nv) else None)
+    return out
+
+
+def fdk_spiral(g: Geometry, vol: Volume, proj: np.ndarray, cut_off: float = 1.0, apod: int = 0,
+               threads: int | None = None) -> np.ndarray:
+    """FP64 spiral FDK ([z][y][x]): cosine weights and the ramp filter on every view (no Parker
+    weights), then per slice the backprojection of its window of views with the final angular
+    increment scale (src/cuda/recon/fdk_spiral.cuh:33-94)."""
+    filt = filter_stack(g, proj, cut_off, apod, use_fft=g.nc > 256, threads=threads, parker=False)
+    out = np.zeros(vol.shape)
+    z0 = vol.mid[2] - (vol.nz - 1) * vol.dz / 2.0
+    for k, w in enumerate(spiral_windows(g, vol)):
+        if w is None:
+            continue
+        first, last = w
+        gs = Geometry(g.kind, g.nc, g.du, g.views[first:last], g.nr, g.dv)
+        vs = Volume(vol.nx, vol.ny, 1, vol.dx, vol.dy, vol.dz, (vol.mid[0], vol.mid[1], z0 + k * vol.dz))
+        out[k] = backproject(gs, vs, filt[first:last], threads=threads)[0]
     return out
 
 

@@ -86,3 +86,36 @@ def oracle_projections(case: Case, scale: float = 1.0) -> np.ndarray:
     ph[:, :6] *= scale
     ph[:, 7] /= scale  # keep line integrals of the same order
     return orc.phantom(case.og, ph).astype(np.float32)
+
+
+def make_spiral_case(name: str = "cone_cyl", npr: int = 60, turns: int = 3, pitch: float = 1.0, nc: int = 96,
+                     nr: int = 24, n: int = 48, nz: int = 16, rot_dir: g.RotDir = g.RotDir.CW) -> Case:
+    """Helical cone-beam scan: `turns` rotations of `npr` views, source z = -pitch * angle (mm per
+    radian); the grid is centred on the middle of the helix so that the slices near both ends have
+    no complete rotation of views (the spiral FDK leaves them zero)."""
+    incr = 2 * math.pi / npr
+    rot = g.RotationParams(rot_dir, 0.0, incr, npr * turns, pitch)
+    c0, r0 = (nc - 1) / 2.0, (nr - 1) / 2.0
+    if name == "cone_cyl":
+        det = (g.DetFanArc(nc, 0.11 / nc * 2.0), g.DetFanLine(nr, 1.14))
+        params = g.ConeBeamProjGeomParams(c0, rot, 1000.0, 500.0, r0)
+    elif name == "cone_flat":
+        det = (g.DetFanLine(nc, 2.0), g.DetFanLine(nr, 2.0))
+        params = g.ConeBeamProjGeomParams(c0, rot, 1000.0, 500.0, r0)
+    else:
+        raise KeyError(name)
+    views = g.ProjGeomFactory(*(type(d) for d in det)).create_all(params)
+    cg = g.SpiralCTGeom(det, views)
+    og = orc.Geometry(int(cg.kind), nc, det[0].sampling_width, cg.views, nr, det[1].sampling_width)
+    zmid = -pitch * incr * (npr * turns - 1) / 2.0
+    vg = g.ReconImgGeom(g.EqDistSampler(n, 1.0), g.EqDistSampler(n, 1.0), g.EqDistSampler(nz, 1.5), (0.0, 0.0, zmid))
+    ov = orc.Volume(n, n, nz, 1.0, 1.0, 1.5, (0.0, 0.0, zmid))
+    return Case(name + "_spiral", cg, og, vg, ov)
+
+
+def spiral_projections(case: Case) -> np.ndarray:
+    """Line integrals of PHANTOM stretched along z to cover the helix, centred on the grid."""
+    ph = np.array(PHANTOM)
+    ph[:, 2] = ph[:, 2] * 0.5 + case.ov.mid[2]
+    ph[:, 5] *= 1.5
+    return orc.phantom(case.og, ph).astype(np.float32)
