@@ -148,6 +148,8 @@ SIGNATURES = {
     "gct_fdk_backproject": [VP, VP, VP, C.c_uint32, C.c_uint32, C.c_int32, VP],
     "gct_fdk_execute_host": [VP, P(C.c_float), P(C.c_float), VP],
     "gct_fdk_execute_noalloc": [VP, VP, VP, VP],
+    "gct_fdk_execute_host_async": [VP, P(C.c_float), P(C.c_float), VP],
+    "gct_fdk_host_sync": [VP],
     "gct_fdk_execute_host_budget": [VP, P(C.c_float), P(C.c_float), C.c_uint64, VP],
     "gct_reconstruct": [P(gct_ct_geom), P(gct_vol_geom), P(C.c_float), P(C.c_float)],
     "gct_reconstruct_ex": [P(gct_ct_geom), P(gct_vol_geom), P(gct_filt_params), P(gct_fdk_opts),

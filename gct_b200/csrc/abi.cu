@@ -458,15 +458,23 @@ void execute(gct_fdk_plan *p, const float *proj, float *vol, void *workspace, cu
     run_backproject(p, st, vol, 0, p->nv, false, s);
 }
 
-void execute_host(gct_fdk_plan *p, const float *proj_host, float *vol_host, cudaStream_t s)
+// Host buffers through a plan. The upload of chunk c on the copy stream waits only for the
+// previous call's filter of chunk c (its staging slot), and the volume download runs on a third
+// stream into one of two device volumes, so consecutive calls overlap: one call's uploads run under
+// the previous call's backprojections and one call's download under the next call's work. With
+// `sync` the call returns when the volume is on the host; otherwise gct_fdk_host_sync waits.
+void execute_host(gct_fdk_plan *p, const float *proj_host, float *vol_host, cudaStream_t s, bool sync)
 {
     if (!proj_host || !vol_host) gct::fail(GCT_ERR_INVALID_ARG, "NULL projection or volume pointer");
     const size_t pix = static_cast<size_t>(p->nr) * p->nc;
     const size_t vol_n = static_cast<size_t>(p->vol.nx) * p->vol.ny * p->vol.nz;
     if (!p->host_proj.p) p->host_proj.alloc(pix * p->nv, "staging projections");
-    if (!p->host_vol.p) p->host_vol.alloc(vol_n, "staging volume");
+    const int slot = static_cast<int>(p->host_calls & 1u);
+    DevBuf<float> &vbuf = slot ? p->host_vol2 : p->host_vol;
+    if (!vbuf.p) vbuf.alloc(vol_n, "staging volume");
     const StackRef st = stack_of(p, plan_workspace(p, nullptr));
     if (!p->copy_stream) cuda_check(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking), "copy stream");
+    if (!p->d2h_stream) cuda_check(cudaStreamCreateWithFlags(&p->d2h_stream, cudaStreamNonBlocking), "download stream");
     // About 8 chunks, at least 16 views each; a quarter-turn plan chunks its base views and takes
     // each chunk's partner views with it. (Measured and rejected at 512^3 / 720 views: splitting the
     // last quarter into chunks a quarter that size, to shorten the work after the last upload:
@@ -474,16 +482,22 @@ void execute_host(gct_fdk_plan *p, const float *proj_host, float *vol_host, cuda
     const int parts = st.quarter ? 4 : 1, span = p->nv / parts;
     const int chunk = std::max(16 / parts, (span + 7) / 8);
     const int nchunks = (span + chunk - 1) / chunk;
-    while (static_cast<int>(p->chunk_events.size()) < nchunks + 1) {
-        cudaEvent_t e;
-        cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-        p->chunk_events.push_back(e);
-    }
-    // the copy stream must not overwrite staging still read by a previous call on `s`
-    cuda_check(cudaEventRecord(p->chunk_events[nchunks], s), "event record");
-    cuda_check(cudaStreamWaitEvent(p->copy_stream, p->chunk_events[nchunks], 0), "stream wait");
+    auto grow = [](std::vector<cudaEvent_t> &v, size_t n) {
+        while (v.size() < n) {
+            cudaEvent_t e;
+            cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+            v.push_back(e);
+        }
+    };
+    grow(p->chunk_events, nchunks);
+    grow(p->prep_events, nchunks);
+    for (cudaEvent_t *e : {&p->vol_free[0], &p->vol_free[1], &p->bp_done})
+        if (!*e) cuda_check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "event");
     for (int c = 0; c < nchunks; ++c) {
         const int vb = c * chunk, vc = std::min(chunk, span - vb);
+        // the staging of chunk c is free once the previous call has filtered it (an event never
+        // recorded lets the first call through)
+        cuda_check(cudaStreamWaitEvent(p->copy_stream, p->prep_events[c], 0), "stream wait");
         for (int q = 0; q < parts; ++q) {
             const size_t v0 = static_cast<size_t>(vb + q * span);
             cuda_check(cudaMemcpyAsync(p->host_proj.p + v0 * pix, proj_host + v0 * pix, sizeof(float) * pix * vc,
@@ -492,17 +506,21 @@ void execute_host(gct_fdk_plan *p, const float *proj_host, float *vol_host, cuda
         }
         cuda_check(cudaEventRecord(p->chunk_events[c], p->copy_stream), "event record");
         cuda_check(cudaStreamWaitEvent(s, p->chunk_events[c], 0), "stream wait");
-        if (st.quarter) {
-            prepare_partners(p, p->host_proj.p, st, vb, vc, s);
-            run_backproject_sym(p, st, p->host_vol.p, vb, vc, c > 0, s);
-        } else {
-            prepare(p, p->host_proj.p, st, vb, vc, s);
-            run_backproject(p, st, p->host_vol.p, vb, vc, c > 0, s);
-        }
+        // this volume is free once the download two calls back has read it
+        if (c == 0) cuda_check(cudaStreamWaitEvent(s, p->vol_free[slot], 0), "stream wait");
+        if (st.quarter) prepare_partners(p, p->host_proj.p, st, vb, vc, s);
+        else prepare(p, p->host_proj.p, st, vb, vc, s);
+        cuda_check(cudaEventRecord(p->prep_events[c], s), "event record");
+        if (st.quarter) run_backproject_sym(p, st, vbuf.p, vb, vc, c > 0, s);
+        else run_backproject(p, st, vbuf.p, vb, vc, c > 0, s);
     }
-    cuda_check(cudaMemcpyAsync(vol_host, p->host_vol.p, sizeof(float) * vol_n, cudaMemcpyDeviceToHost, s),
+    cuda_check(cudaEventRecord(p->bp_done, s), "event record");
+    cuda_check(cudaStreamWaitEvent(p->d2h_stream, p->bp_done, 0), "stream wait");
+    cuda_check(cudaMemcpyAsync(vol_host, vbuf.p, sizeof(float) * vol_n, cudaMemcpyDeviceToHost, p->d2h_stream),
                "volume download");
-    cuda_check(cudaStreamSynchronize(s), "reconstruction");
+    cuda_check(cudaEventRecord(p->vol_free[slot], p->d2h_stream), "event record");
+    ++p->host_calls;
+    if (sync) cuda_check(cudaStreamSynchronize(p->d2h_stream), "reconstruction");
 }
 
 // Streaming FDK with a bounded device footprint for the projections: views go through two
@@ -530,6 +548,8 @@ void execute_host_budget(gct_fdk_plan *p, const float *proj_host, float *vol_hos
     }
     if (!p->host_vol.p) p->host_vol.alloc(vol_n, "staging volume");
     if (!p->copy_stream) cuda_check(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking), "copy stream");
+    // the device volume may still be downloading for an asynchronous host call
+    if (p->vol_free[0]) cuda_check(cudaStreamWaitEvent(s, p->vol_free[0], 0), "stream wait");
     for (cudaEvent_t &e : p->stream_events)
         if (!e) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
     cudaEvent_t *filled = p->stream_events, *freed = p->stream_events + 2;
@@ -901,7 +921,25 @@ gct_status gct_fdk_execute_host(gct_fdk_plan *plan, const float *proj_host, floa
     return guarded([&] {
         if (!plan) gct::fail(GCT_ERR_INVALID_ARG, "NULL plan");
         DeviceGuard dg(plan->device);
-        execute_host(plan, proj_host, vol_host, static_cast<cudaStream_t>(stream));
+        execute_host(plan, proj_host, vol_host, static_cast<cudaStream_t>(stream), true);
+    });
+}
+
+gct_status gct_fdk_execute_host_async(gct_fdk_plan *plan, const float *proj_host, float *vol_host, void *stream)
+{
+    return guarded([&] {
+        if (!plan) gct::fail(GCT_ERR_INVALID_ARG, "NULL plan");
+        DeviceGuard dg(plan->device);
+        execute_host(plan, proj_host, vol_host, static_cast<cudaStream_t>(stream), false);
+    });
+}
+
+gct_status gct_fdk_host_sync(gct_fdk_plan *plan)
+{
+    return guarded([&] {
+        if (!plan) gct::fail(GCT_ERR_INVALID_ARG, "NULL plan");
+        DeviceGuard dg(plan->device);
+        if (plan->d2h_stream) cuda_check(cudaStreamSynchronize(plan->d2h_stream), "reconstruction");
     });
 }
 

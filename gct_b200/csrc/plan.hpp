@@ -117,10 +117,13 @@ struct gct_fdk_plan {
     DevBuf<__nv_bfloat16> xll, tll;  // four-term filter: third piece of the rows and of the central taps
     DevBuf<float> ybuf;
     DevBuf<int> gemm_err;
-    // staging for gct_fdk_execute_host
-    DevBuf<float> host_proj, host_vol;
-    cudaStream_t copy_stream = nullptr;
-    std::vector<cudaEvent_t> chunk_events;
+    // staging for gct_fdk_execute_host: projections, two device volumes (consecutive calls
+    // alternate, so one call's download overlaps the next call's backprojection)
+    DevBuf<float> host_proj, host_vol, host_vol2;
+    cudaStream_t copy_stream = nullptr, d2h_stream = nullptr;
+    std::vector<cudaEvent_t> chunk_events, prep_events;  // per chunk: upload done, filter done
+    cudaEvent_t vol_free[2] = {nullptr, nullptr}, bp_done = nullptr;
+    unsigned host_calls = 0;
     // bounded-memory streaming (gct_fdk_execute_host_budget): two projection slots of
     // stream_chunk views and a view-major stack of one chunk
     DevBuf<float> stream_stage;
@@ -131,6 +134,10 @@ struct gct_fdk_plan {
     ~gct_fdk_plan()
     {
         for (cudaEvent_t e : chunk_events) cudaEventDestroy(e);
+        for (cudaEvent_t e : prep_events) cudaEventDestroy(e);
+        for (cudaEvent_t e : {vol_free[0], vol_free[1], bp_done})
+            if (e) cudaEventDestroy(e);
+        if (d2h_stream) cudaStreamDestroy(d2h_stream);
         for (cudaEvent_t e : stream_events)
             if (e) cudaEventDestroy(e);
         if (copy_stream) cudaStreamDestroy(copy_stream);

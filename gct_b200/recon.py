@@ -173,6 +173,24 @@ class FdkPlan:
         _lib.check(self._lib.gct_fdk_execute_host(self._handle, proj.ctypes.data_as(fp), vol.ctypes.data_as(fp),
                                                   C.c_void_p(_stream(stream))))
 
+    def execute_host_async(self, proj: np.ndarray, vol: np.ndarray, stream=None) -> None:
+        """As execute_host without the final wait; consecutive calls overlap. The arrays must stay
+        untouched until host_sync()."""
+        fp = C.POINTER(C.c_float)
+        for a in (proj, vol):
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags.c_contiguous):
+                raise TypeError("expected contiguous float32 numpy arrays")
+        if proj.size != self.cg.num_views * self.cg.num_rows * self.cg.num_cols:
+            raise ValueError("projection array does not match the geometry")
+        if vol.size != int(np.prod(self.vol_geom.shape)):
+            raise ValueError("volume array does not match the grid")
+        _lib.check(self._lib.gct_fdk_execute_host_async(self._handle, proj.ctypes.data_as(fp), vol.ctypes.data_as(fp),
+                                                        C.c_void_p(_stream(stream))))
+
+    def host_sync(self) -> None:
+        """Waits for every execute_host_async call of this plan."""
+        _lib.check(self._lib.gct_fdk_host_sync(self._handle))
+
     def execute_host_budget(self, proj: np.ndarray, vol: np.ndarray, device_bytes: int, stream=None) -> None:
         """Host arrays in and out with at most `device_bytes` of device buffers for the projections
         (streamed in chunks of views; synchronous)."""

@@ -336,6 +336,15 @@ gct_status gct_fdk_backproject(gct_fdk_plan *plan, const void *workspace, float 
 gct_status gct_fdk_execute_host(gct_fdk_plan *plan, const float *proj_host, float *vol_host,
                                 void *stream);
 
+/* The same without the final wait: the call enqueues its uploads, filters, backprojections and
+ * the volume download and returns. Consecutive calls on one plan overlap (a call's uploads run
+ * under the previous call's backprojections, its download under the next call's work; two device
+ * volumes alternate). proj_host and vol_host must stay valid and untouched until
+ * gct_fdk_host_sync(plan) returns, which waits for every such call of the plan. */
+gct_status gct_fdk_execute_host_async(gct_fdk_plan *plan, const float *proj_host, float *vol_host,
+                                      void *stream);
+gct_status gct_fdk_host_sync(gct_fdk_plan *plan);
+
 /* Host buffers with a bounded device footprint for the projections (stacks larger than the
  * device): the views stream through two upload slots and a filtered stack of one chunk, where a
  * chunk is as many views as device_bytes holds (two float32 views plus one filtered view each),

@@ -259,3 +259,24 @@ def test_streaming_budget_path(storage):
         assert np.array_equal(out, again)
         with pytest.raises(g.GctError, match="budget"):
             plan.execute_host_budget(proj, out, per_view // 2)
+
+
+@pytest.mark.parametrize("storage", [g.STORAGE_F32, g.STORAGE_F16])
+def test_async_host_calls_overlap_and_match(storage):
+    # three back-to-back asynchronous calls with different inputs and outputs (two device volumes
+    # alternate, uploads wait per chunk) give the synchronous results
+    case = make_case("cone_flat")
+    proj = oracle_projections(case)
+    inputs = [proj, (proj * 2.0).astype(np.float32), (proj + 0.5).astype(np.float32)]
+    with g.FdkPlan(case.cg, case.vg, opts=g.FdkOptions(storage=storage)) as plan:
+        ref = []
+        for p in inputs:
+            out = np.empty(case.vg.shape, np.float32)
+            plan.execute_host(p, out)
+            ref.append(out)
+        outs = [np.full(case.vg.shape, np.nan, np.float32) for _ in inputs]
+        for p, o in zip(inputs, outs):
+            plan.execute_host_async(p, o)
+        plan.host_sync()
+    for o, r in zip(outs, ref):
+        assert np.array_equal(o, r)
