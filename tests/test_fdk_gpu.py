@@ -174,31 +174,6 @@ def test_two_workspaces_one_plan(storage):
     p1 = oracle_projections(case)
     p2 = (p1 * 3.0 + 0.5).astype(np.float32)
     with g.FdkPlan(case.cg, case.vg, opts=g.FdkOptions(storage=storage)) as plan:
-        nbytes = plan.workspace_bytes()
-        ws = [torch.empty(nbytes, dtype=torch.uint8, device="cuda") for _ in range(2)]
-        d = [torch.from_numpy(p).cuda() for p in (p1, p2)]
-        vols = [torch.empty(case.vg.shape, dtype=torch.float32, device="cuda") for _ in range(2)]
-        plan.prepare(d[0], ws[0])
-        plan.prepare(d[1], ws[1])
-        plan.backproject(vols[0], ws[0])
-        plan.backproject(vols[1], ws[1])
-        alone = [torch.empty_like(vols[0]) for _ in range(2)]
-        plan.execute(d[0], alone[0])
-        plan.execute(d[1], alone[1])
-        torch.cuda.synchronize()
-    for a, b in zip(vols, alone):
-        assert torch.equal(a, b)
-
-
-@pytest.mark.parametrize("storage", [g.STORAGE_F32, g.STORAGE_F16])
-def test_two_workspaces_one_plan(storage):
-    # A workspace carries a whole prepared stack (quads and FP16 view scales): preparing a second
-    # stack into another workspace must not change what the first one backprojects.
-    import torch
-    case = make_case("cone_flat")
-    p1 = oracle_projections(case)
-    p2 = (p1 * 3.0 + 0.5).astype(np.float32)
-    with g.FdkPlan(case.cg, case.vg, opts=g.FdkOptions(storage=storage)) as plan:
         nbytes = plan.workspace_bytes
         ws = [torch.empty(nbytes, dtype=torch.uint8, device="cuda") for _ in range(2)]
         d = [torch.from_numpy(p).cuda() for p in (p1, p2)]
