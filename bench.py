@@ -488,7 +488,7 @@ def run_gct(args, cfg, rank, world, local_rank):
         "clocks": clocks,
         # per mixed step: view max, view scale, (split, GEMM, quads | FFT filter), backprojection
         "gpu_launches": (4 if args.mixed_filter == "fft" else 6) * args.steps,
-        "mixed_filter": {"gemm4": "split-BF16 Toeplitz GEMM on tcgen05, 4 terms + banded 5th (rows and central "
+        "mixed_filter": {"gemm4": "split-BF16 Toeplitz GEMM on tcgen05, 3 full terms + 2 banded (rows and central "
                                   "taps in three BF16 pieces)",
                          "gemm3": "split-BF16 Toeplitz GEMM on tcgen05, 3 terms",
                          "fft": "shared-memory FFT"}[args.mixed_filter],

@@ -249,7 +249,7 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
 // Toeplitz-GEMM form of run_filter: split, tcgen05 GEMM into FP32 rows, then quads (or the rows
 // themselves for the plain output).
 void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float *vscale, int mode, int quarter,
-                     int vb, int vc, cudaStream_t s)
+                     int vb, int vc, cudaStream_t s, const StackRef *fused_scales)
 {
     const long long row0 = static_cast<long long>(vb) * p->nr, rows = static_cast<long long>(vc) * p->nr;
     gct::SplitArgs sa;
@@ -267,8 +267,14 @@ void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float 
     sa.xh = p->xh.p;
     sa.xl = p->xl.p;
     sa.xll = p->xll.p;
+    sa.amax = fused_scales ? fused_scales->amax : nullptr;
     gct::launch_split(sa, p->num_sms, s);
     cuda_check(cudaGetLastError(), "split kernel launch");
+    if (fused_scales) {  // the split found the view maxima: scales before the quads are written
+        gct::launch_view_scales(fused_scales->amax + vb, vc, p->l1, fused_scales->vscale + vb, fused_scales->vinv + vb,
+                                s);
+        cuda_check(cudaGetLastError(), "view scale kernel");
+    }
     gct::GemmLaunch gl;
     gl.xh = p->xh.p;
     gl.xl = p->xl.p;
@@ -306,13 +312,14 @@ void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float 
 }  // namespace
 
 // `out` is the view-0 address of the output; `vscale` (FP16 quads only) the view-0 scales;
-// `quarter` the quad_layout of a quad output.
+// `quarter` the quad_layout of a quad output. `fused_scales` (Toeplitz form only, amax zeroed by
+// the caller): the split pass also finds the view maxima and the scales follow it.
 void run_filter(gct_fdk_plan *p, const float *proj, void *out, const float *vscale, int mode, int quarter, int vb,
-                int vc, cudaStream_t s)
+                int vc, cudaStream_t s, const StackRef *fused_scales)
 {
     if (vc <= 0) return;
     if (p->opts.filter != GCT_FILTER_FFT) {
-        run_filter_gemm(p, proj, out, vscale, mode, quarter, vb, vc, s);
+        run_filter_gemm(p, proj, out, vscale, mode, quarter, vb, vc, s, fused_scales);
         return;
     }
     const long long pix = static_cast<long long>(p->nr) * p->nc;
@@ -419,8 +426,11 @@ void prepare(gct_fdk_plan *p, const float *proj, const StackRef &st, int vb, int
     if (!proj) gct::fail(GCT_ERR_INVALID_ARG, "NULL projection pointer");
     if (vc <= 0) return;
     const bool f16 = p->opts.storage == GCT_STORAGE_F16;
-    if (f16) view_scales(p, proj, st, vb, vc, s);
-    run_filter(p, proj, st.quads, st.vscale, f16 ? gct::kOutQuadF16 : gct::kOutQuadF32, st.quarter, vb, vc, s);
+    const bool fuse = f16 && p->opts.filter != GCT_FILTER_FFT;  // the split pass finds the maxima
+    if (fuse) cuda_check(cudaMemsetAsync(st.amax + vb, 0, sizeof(float) * vc, s), "view maxima reset");
+    else if (f16) view_scales(p, proj, st, vb, vc, s);
+    run_filter(p, proj, st.quads, st.vscale, f16 ? gct::kOutQuadF16 : gct::kOutQuadF32, st.quarter, vb, vc, s,
+               fuse ? &st : nullptr);
 }
 
 void prepare_partners(gct_fdk_plan *p, const float *proj, const StackRef &st, int b, int n, cudaStream_t s)
@@ -430,10 +440,12 @@ void prepare_partners(gct_fdk_plan *p, const float *proj, const StackRef &st, in
     if (n <= 0 || m <= 0) return;
     const bool f16 = p->opts.storage == GCT_STORAGE_F16;
     const bool whole = b == 0 && n == m;
+    const bool fuse = f16 && p->opts.filter != GCT_FILTER_FFT;  // the split pass finds the maxima
     for (int q = 0; q < (whole ? 1 : 4); ++q) {
         const int vb = whole ? 0 : b + q * m, vc = whole ? p->nv : n;
-        if (f16) view_scales(p, proj, st, vb, vc, s);
-        run_filter(p, proj, p->ybuf.p, nullptr, gct::kOutPlainF32, 0, vb, vc, s);
+        if (fuse) cuda_check(cudaMemsetAsync(st.amax + vb, 0, sizeof(float) * vc, s), "view maxima reset");
+        else if (f16) view_scales(p, proj, st, vb, vc, s);
+        run_filter(p, proj, p->ybuf.p, nullptr, gct::kOutPlainF32, 0, vb, vc, s, fuse ? &st : nullptr);
     }
     gct::QuadArgs qa;
     qa.Y = p->ybuf.p;

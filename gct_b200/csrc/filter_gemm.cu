@@ -9,8 +9,10 @@
 // (the dropped Xl Tl term is ~2^-16 relative), or in a four-term form with three pieces of X
 // and of the central taps:
 //     X = Xh + Xl + Xll,  Y = Xh Th + Xh Tl + Xl Th + Xll Th + Xh Tll,
-// where Tll is kept for |c - k| <= kBand only, so the last term runs over the few K blocks around
-// each output tile's diagonal. Two BF16 pieces hold a value to about 2^-17 relative, and ramp
+// where Tll is kept for |c - k| <= kBand only, and the Xll Th term also runs over that band only
+// (Xll is rounding noise 2^-16 below the values, so the far taps add nothing it carries): the
+// last two terms cover the few K blocks around each output tile's diagonal. Two BF16 pieces hold
+// a value to about 2^-17 relative, and ramp
 // filtering removes the large smooth part of a projection, so residuals of that part are a large
 // fraction of the filtered value. The two-piece taps keep a DC response of about 1e-6 that
 // multiplies the smooth part of every view alike and adds up over views: 1.1e-3 relative RMS in
@@ -21,7 +23,8 @@
 //      128 x 64 A tiles and 256 x 64 B tiles (128B swizzle) into a 4-stage shared-memory ring;
 //      one thread of warp 1 issues tcgen05.mma (M 128, N 256, K 16) into one of two TMEM
 //      accumulators of 256 FP32 columns; warps 2-5 drain the other accumulator with tcgen05.ld and
-//      store FP32 rows. The terms are one K loop of (terms x K/64) steps plus the band steps.
+//      store FP32 rows. The terms are one K loop of (3 x K/64) steps plus the band steps of the
+//      four-term form.
 //   3. quads_from_rows_kernel: the filtered rows become the backprojector's bilinear-coefficient
 //      quads (FP32 or FP16 with the per-view scale).
 // Every mbarrier wait is bounded (2 s of %globaltimer); on timeout the kernel records an error
@@ -191,7 +194,10 @@ __global__ void __launch_bounds__(192, 1)
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
     const int total = p.m_tiles * p.n_tiles;
-    const int kfull = p.terms * p.num_kb;  // full-K segments; the band segment follows
+    // three full-K segments (Xh Th, Xh Tl, Xl Th); the four-term form then adds Xll Th and Xh Tll over
+    // the K blocks of the diagonal band: the third pieces are 2^-16 of the values, so taps beyond
+    // the band add nothing they carry (Xll is rounding noise without a smooth part)
+    const int kfull = 3 * p.num_kb;
 
     if (warp == 0) {
         if (lane == 0) {  // TMA producer
@@ -201,11 +207,19 @@ __global__ void __launch_bounds__(192, 1)
                 const int m0 = p.m_begin + (t / p.n_tiles) * BM, n0 = (t % p.n_tiles) * BN;
                 int kb0, kb1;
                 band_blocks(p, n0, kb0, kb1);
-                const int ksteps = kfull + (kb1 - kb0);
+                const int nband = kb1 - kb0;
+                const int ksteps = kfull + 2 * nband;
                 for (int ks = 0; ks < ksteps; ++ks) {
-                    // segments: 0 Xh Th, 1 Xh Tl, 2 Xl Th, 3 Xll Th (full K); then Xh Tll over the band
-                    const bool band = ks >= kfull;
-                    const int seg = band ? 4 : ks / p.num_kb, kb = band ? kb0 + ks - kfull : ks - seg * p.num_kb;
+                    // segments: 0 Xh Th, 1 Xh Tl, 2 Xl Th (full K); then 3 Xll Th and 4 Xh Tll over the band
+                    int seg, kb;
+                    if (ks < kfull) {
+                        seg = ks / p.num_kb;
+                        kb = ks - seg * p.num_kb;
+                    } else {
+                        const int bs = ks - kfull;
+                        seg = bs < nband ? 3 : 4;
+                        kb = kb0 + (bs < nband ? bs : bs - nband);
+                    }
                     if (!mbar_wait(empty(stage), phase ^ 1)) {
                         atomicExch(&s_fail, 1);
                         break;
@@ -234,7 +248,7 @@ __global__ void __launch_bounds__(192, 1)
                 const uint32_t d = tmem_base + static_cast<uint32_t>(acc * BN);
                 int kb0, kb1;
                 band_blocks(p, (t % p.n_tiles) * BN, kb0, kb1);
-                const int ksteps = kfull + (kb1 - kb0);
+                const int ksteps = kfull + 2 * (kb1 - kb0);
                 bool ok = true;
                 for (int ks = 0; ks < ksteps; ++ks) {
                     if (!mbar_wait(full(stage), phase)) {
@@ -314,41 +328,72 @@ __global__ void __launch_bounds__(192, 1)
     }
 }
 
-// Cosine x Parker weighting and BF16 hi/lo split of rows [row0, row0 + rows) into [rows][Kp].
-// One warp per row (per-row view/row indices and geometry), two columns per lane step stored as
-// one bf16x2 word.
+// Cosine x Parker weighting and BF16 split of rows [row0, row0 + rows) into [rows][Kp]: two or
+// three pieces per value. One warp per row (per-row view/row indices and geometry), four columns
+// per lane step (one 16-byte load when rows are 16-byte aligned) stored as 8-byte bf16x4 words.
+// With `amax`, the row's largest raw |p| also goes into amax[view] (atomic max of the bit
+// pattern, non-negative floats), which replaces the separate view-maximum pass.
+__device__ __forceinline__ uint2 bf16x4(float a, float b, float c, float d)
+{
+    const __nv_bfloat162 lo = __floats2bfloat162_rn(a, b), hi = __floats2bfloat162_rn(c, d);
+    uint2 u;
+    u.x = *reinterpret_cast<const unsigned *>(&lo);
+    u.y = *reinterpret_cast<const unsigned *>(&hi);
+    return u;
+}
+__device__ __forceinline__ float bf16_lo(unsigned w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf16_hi(unsigned w) { return __uint_as_float(w & 0xffff0000u); }
+
 __global__ void split_kernel(SplitArgs a)
 {
     const int lane = threadIdx.x & 31;
     const long long warp0 = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
+    const bool vec = (a.nc & 3) == 0;
     for (long long rl = warp0; rl < a.rows; rl += nwarps) {
         const long long row = a.row0 + rl;
         const int v = static_cast<int>(row / a.nr), r = static_cast<int>(row - static_cast<long long>(v) * a.nr);
         const float4 gv = __ldg(&a.fview[v]);
         const float *src = a.proj + row * a.nc;
         const float *pk = a.parker + static_cast<long long>(v) * a.nc;
-        __nv_bfloat162 *dh = reinterpret_cast<__nv_bfloat162 *>(a.xh + row * a.Kp);
-        __nv_bfloat162 *dl = reinterpret_cast<__nv_bfloat162 *>(a.xl + row * a.Kp);
-        __nv_bfloat162 *dll = a.xll ? reinterpret_cast<__nv_bfloat162 *>(a.xll + row * a.Kp) : nullptr;
-        for (int k2 = lane; k2 < a.Kp / 2; k2 += 32) {
-            float x[2];
+        uint2 *dh = reinterpret_cast<uint2 *>(a.xh + row * a.Kp);
+        uint2 *dl = reinterpret_cast<uint2 *>(a.xl + row * a.Kp);
+        uint2 *dll = a.xll ? reinterpret_cast<uint2 *>(a.xll + row * a.Kp) : nullptr;
+        float m = 0.f;
+        for (int k4 = lane; k4 < a.Kp / 4; k4 += 32) {
+            const int k = 4 * k4;
+            float raw[4], pw[4];
+            if (vec && k + 3 < a.nc) {
+                const float4 p4 = __ldg(reinterpret_cast<const float4 *>(src + k));
+                const float4 w4 = __ldg(reinterpret_cast<const float4 *>(pk + k));
+                raw[0] = p4.x, raw[1] = p4.y, raw[2] = p4.z, raw[3] = p4.w;
+                pw[0] = w4.x, pw[1] = w4.y, pw[2] = w4.z, pw[3] = w4.w;
+            } else {
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int k = 2 * k2 + h;
-                x[h] = (k < a.nc) ? __ldg(src + k) * __ldg(pk + k) * cos_weight_dev(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k, r)
-                                  : 0.f;
+                for (int h = 0; h < 4; ++h) {
+                    const bool in = k + h < a.nc;
+                    raw[h] = in ? __ldg(src + k + h) : 0.f;
+                    pw[h] = in ? __ldg(pk + k + h) : 0.f;
+                }
             }
-            const __nv_bfloat162 hi = __floats2bfloat162_rn(x[0], x[1]);
-            const float2 hf = __bfloat1622float2(hi);
-            dh[k2] = hi;
-            const float r0 = x[0] - hf.x, r1 = x[1] - hf.y;  // exact in FP32
-            const __nv_bfloat162 lo = __floats2bfloat162_rn(r0, r1);
-            dl[k2] = lo;
-            if (dll) {
-                const float2 lf = __bfloat1622float2(lo);
-                dll[k2] = __floats2bfloat162_rn(r0 - lf.x, r1 - lf.y);
+            float x[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                m = fmaxf(m, fabsf(raw[h]));
+                x[h] = raw[h] * pw[h] * cos_weight_dev(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k + h, r);
             }
+            const uint2 hi = bf16x4(x[0], x[1], x[2], x[3]);
+            dh[k4] = hi;
+            const float r0 = x[0] - bf16_lo(hi.x), r1 = x[1] - bf16_hi(hi.x);  // exact in FP32
+            const float r2 = x[2] - bf16_lo(hi.y), r3 = x[3] - bf16_hi(hi.y);
+            const uint2 lo = bf16x4(r0, r1, r2, r3);
+            dl[k4] = lo;
+            if (dll)
+                dll[k4] = bf16x4(r0 - bf16_lo(lo.x), r1 - bf16_hi(lo.x), r2 - bf16_lo(lo.y), r3 - bf16_hi(lo.y));
+        }
+        if (a.amax) {
+            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (lane == 0) atomicMax(reinterpret_cast<int *>(a.amax + v), __float_as_int(m));
         }
     }
 }

@@ -22,6 +22,7 @@ struct SplitArgs {
     const float *parker = nullptr;
     __nv_bfloat16 *xh = nullptr, *xl = nullptr;  // [all rows][Kp]
     __nv_bfloat16 *xll = nullptr;                // third piece (four-term GEMM), or NULL
+    float *amax = nullptr;                       // per-view max |raw value| (zeroed by the caller), or NULL
 };
 void launch_split(const SplitArgs &a, int num_sms, cudaStream_t s);
 

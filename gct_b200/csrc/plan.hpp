@@ -183,7 +183,7 @@ inline StackRef stack_of(const gct_fdk_plan *p, void *workspace, bool view_major
 // Stage functions (abi.cu). `out` / StackRef bases are view-0 addresses; [vb, vb + vc) is the
 // view range worked on.
 void run_filter(gct_fdk_plan *p, const float *proj, void *out, const float *vscale, int mode, int quarter, int vb,
-                int vc, cudaStream_t s);
+                int vc, cudaStream_t s, const StackRef *fused_scales = nullptr);
 void prepare(gct_fdk_plan *p, const float *proj, const StackRef &st, int vb, int vc, cudaStream_t s);
 // Quarter-turn stacks (st.quarter > 0): base views [b, b + n) and their partners, through the
 // plan's FP32 row buffer and one coalesced pass that writes the partner groups.

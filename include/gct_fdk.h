@@ -148,7 +148,7 @@ enum {
     GCT_FILTER_FFT = 0,             /* own row-batched shared-memory FFT, FP32 arithmetic */
     GCT_FILTER_TOEPLITZ_BF16X3 = 1, /* 3-term split BF16 Toeplitz GEMM on tcgen05, FP32 accumulate */
     GCT_FILTER_TOEPLITZ_BF16X4 = 2  /* projections in three BF16 pieces and the central taps
-                                     * (|c - k| <= 64) in three: four full GEMM terms plus one over
+                                     * (|c - k| <= 64) in three: three full GEMM terms plus two over
                                      * the diagonal band; removes the two-piece taps' DC error */
 };
 enum {
