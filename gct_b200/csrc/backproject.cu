@@ -551,21 +551,21 @@ __device__ __forceinline__ void sym_rotation(const BpArgs &a, const float *c, fl
     }
 }
 
+// One block's tile of the quarter-turn form: first-quadrant columns [i0, i0 + bx) x [j0, j0 + by)
+// and voxels [k0, k0 + ZPT) along z, over base views [a.v_begin, a.v_begin + a.v_count). tid is
+// the thread's index in the block (column i0 + tid % bx, j0 + tid / bx); every thread of the block
+// calls it (it holds block barriers). mode: kBpStore, kBpAccumulate or kBpAtomic for the four
+// turned columns of each thread.
 template <int FAMILY, class Q, int ZPT>
-__global__ void __launch_bounds__(256) bp_sym_kernel(BpArgs a)
+__device__ __forceinline__ void sym_tile(const BpArgs &a, int i0, int j0, int k0, int bx, int by, int tid, int nthr,
+                                         int mode, float4 *s_coef, float4 *s_w, int *s_cls)
 {
     using L = typename LerpOf<Q>::type;
     using S = typename L::S;
     constexpr bool kClassify = FAMILY != 2;
-    __shared__ float4 s_coef[kViewsPerChunk * kC / 4];
-    __shared__ float4 s_w[kViewsPerChunk];  // weight scales of the four partners of each base view
-    __shared__ int s_cls[kViewsPerChunk];   // box class of each of the block's four turned boxes, 2 bits each
     const int n = a.nx, h = n / 2;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k0 = blockIdx.z * ZPT;
-    const bool active = i < h && j < h;
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nthr = blockDim.x * blockDim.y;
+    const int i = i0 + tid % bx, j = j0 + tid / bx;
+    const bool active = tid < bx * by && i < h && j < h;
     const float fk0 = static_cast<float>(k0);
     const S *quads = static_cast<const S *>(a.quads);
     const int wslot = wscale_slot(FAMILY);
@@ -581,9 +581,8 @@ __global__ void __launch_bounds__(256) bp_sym_kernel(BpArgs a)
             turn(a.sym, n, ti, tj);
         }
     }
-    const int bi0 = blockIdx.x * blockDim.x, bj0 = blockIdx.y * blockDim.y;
-    const float4 box0 = make_float4(static_cast<float>(bi0), static_cast<float>(min(bi0 + static_cast<int>(blockDim.x), h) - 1),
-                                    static_cast<float>(bj0), static_cast<float>(min(bj0 + static_cast<int>(blockDim.y), h) - 1));
+    const float4 box0 = make_float4(static_cast<float>(i0), static_cast<float>(min(i0 + bx, h) - 1),
+                                    static_cast<float>(j0), static_cast<float>(min(j0 + by, h) - 1));
     const float bk0 = fk0, bk1 = static_cast<float>(k0 + ZPT - 1);
 
     float acc[4][ZPT];
@@ -646,10 +645,22 @@ __global__ void __launch_bounds__(256) bp_sym_kernel(BpArgs a)
             const int k = k0 + z;
             if (k < a.nz) {
                 float *dst = a.vol + (static_cast<long long>(k) * a.ny + tj) * a.nx + ti;
-                *dst = a.accumulate ? *dst + acc[q][z] : acc[q][z];
+                if (mode == kBpAtomic) atomicAdd(dst, acc[q][z]);
+                else *dst = mode == kBpAccumulate ? *dst + acc[q][z] : acc[q][z];
             }
         }
     }
+}
+
+template <int FAMILY, class Q, int ZPT>
+__global__ void __launch_bounds__(256) bp_sym_kernel(BpArgs a)
+{
+    __shared__ float4 s_coef[kViewsPerChunk * kC / 4];
+    __shared__ float4 s_w[kViewsPerChunk];  // weight scales of the four partners of each base view
+    __shared__ int s_cls[kViewsPerChunk];   // box class of each of the block's four turned boxes, 2 bits each
+    sym_tile<FAMILY, Q, ZPT>(a, blockIdx.x * blockDim.x, blockIdx.y * blockDim.y, blockIdx.z * ZPT, blockDim.x,
+                             blockDim.y, threadIdx.y * blockDim.x + threadIdx.x, blockDim.x * blockDim.y,
+                             a.accumulate ? kBpAccumulate : kBpStore, s_coef, s_w, s_cls);
 }
 
 template <int FAMILY, class Q>
@@ -738,6 +749,50 @@ __global__ void __launch_bounds__(kQueueThreads, ZC == 0 ? 4 : 2)
     }
 }
 
+// Quarter-turn items of the work queue: tile (tx, ty, tz) of first-quadrant columns.
+template <int FAMILY, class Q>
+__device__ __noinline__ void queue_sym_tile(const BpItem &it, const BpArgs &a, int tx, int ty, int tz, int tid,
+                                            int mode, float4 *s_coef, float4 *s_w, int *s_cls)
+{
+    sym_tile<FAMILY, Q, kSymQueueZpt>(a, tx * it.bx, ty * it.by, tz * kSymQueueZpt, it.bx, it.by, tid, kQueueThreads,
+                                      mode, s_coef, s_w, s_cls);
+}
+
+template <class Q>
+__global__ void __launch_bounds__(kQueueThreads, 2)
+    bp_queue_sym_kernel(const BpItem *__restrict__ items, const BpWork *__restrict__ work, int n_work, int *counter)
+{
+    __shared__ float4 s_coef[kViewsPerChunk * kC / 4];
+    __shared__ float4 s_w[kViewsPerChunk];
+    __shared__ int s_cls[kViewsPerChunk];
+    __shared__ BpItem s_item;
+    __shared__ BpWork s_work;
+    __shared__ int s_next;
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) s_next = atomicAdd(counter, 1);
+        __syncthreads();
+        const int w = s_next;
+        if (w >= n_work) return;
+        if (tid == 0) {
+            s_work = work[w];
+            s_item = items[s_work.item];
+        }
+        __syncthreads();
+        const BpItem &it = s_item;
+        BpArgs a = it.a;
+        a.v_begin = s_work.v_begin;
+        a.v_count = s_work.v_count;
+        const int mode = s_work.mode;
+        const int t = s_work.tile;
+        const int tx = t % it.tiles_x, ty = (t / it.tiles_x) % it.tiles_y, tz = t / (it.tiles_x * it.tiles_y);
+        if (it.family == 0) queue_sym_tile<0, Q>(it, a, tx, ty, tz, tid, mode, s_coef, s_w, s_cls);
+        else if (it.family == 1) queue_sym_tile<1, Q>(it, a, tx, ty, tz, tid, mode, s_coef, s_w, s_cls);
+        else queue_sym_tile<2, Q>(it, a, tx, ty, tz, tid, mode, s_coef, s_w, s_cls);
+        __syncthreads();  // s_item / s_work / s_next are rewritten for the next entry
+    }
+}
+
 }  // namespace
 
 void launch_backproject_sym(const BpArgs &a, int family, int storage, int zpt, int bx, int by, cudaStream_t s)
@@ -757,7 +812,10 @@ int queue_blocks_per_sm(int storage, int zclass)
 {
     int n = 0;
     cudaError_t e;
-    if (storage == 0)
+    if (zclass == kQueueSymClass)
+        e = storage == 0 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bp_queue_sym_kernel<QuadF32>, kQueueThreads, 0)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bp_queue_sym_kernel<QuadF16>, kQueueThreads, 0);
+    else if (storage == 0)
         e = zclass == 0 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bp_queue_kernel<QuadF32, 0>, kQueueThreads, 0)
                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, bp_queue_kernel<QuadF32, 1>, kQueueThreads, 0);
     else
@@ -769,6 +827,11 @@ int queue_blocks_per_sm(int storage, int zclass)
 void launch_backproject_queue(const BpItem *items, const BpWork *work, int n_work, int *counter, int storage,
                               int zclass, int grid, cudaStream_t s)
 {
+    if (zclass == kQueueSymClass) {
+        if (storage == 0) bp_queue_sym_kernel<QuadF32><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter);
+        else bp_queue_sym_kernel<QuadF16><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter);
+        return;
+    }
     if (storage == 0) {
         if (zclass == 0) bp_queue_kernel<QuadF32, 0><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter);
         else bp_queue_kernel<QuadF32, 1><<<grid, kQueueThreads, 0, s>>>(items, work, n_work, counter);

@@ -38,11 +38,22 @@ BpItem make_item(const gct_fdk_plan *p, const StackRef &st, float *vol, const Ti
     it.bx = c.bx;
     it.by = c.by;
     it.vps = c.vps;
-    it.tiles_x = (p->kx + c.bx - 1) / c.bx;
-    it.tiles_y = (p->ky + c.by - 1) / c.by;
+    if (st.quarter) {  // quarter-turn item: tiles of first-quadrant columns, kSymQueueZpt deep
+        if (c.zpt != kSymQueueZpt) fail(GCT_ERR_INVALID_ARG, "quarter-turn queue tiles hold 8 voxels per thread");
+        it.a.sym = p->sym;
+        it.a.v_count = st.quarter;
+        it.tiles_x = (p->kx / 2 + c.bx - 1) / c.bx;
+        it.tiles_y = (p->ky / 2 + c.by - 1) / c.by;
+    } else {
+        it.tiles_x = (p->kx + c.bx - 1) / c.bx;
+        it.tiles_y = (p->ky + c.by - 1) / c.by;
+    }
     it.tiles_z = (p->kz + c.zpt - 1) / c.zpt;
     return it;
 }
+
+int item_views(const gct_fdk_plan *p, const StackRef &st) { return st.quarter ? st.quarter : p->nv; }
+int item_class(const StackRef &st, const TileConfig &c) { return st.quarter ? kQueueSymClass : queue_class(c.zpt); }
 
 long long item_tiles(const BpItem &it) { return static_cast<long long>(it.tiles_x) * it.tiles_y * it.tiles_z; }
 
@@ -53,10 +64,14 @@ std::vector<BpWork> tile_entries(int item, long long tiles, int vb, int vc, int 
     return w;
 }
 
-TileConfig default_config(const gct_fdk_plan *p)
+TileConfig default_config(const gct_fdk_plan *p, bool quarter_turn)
 {
     TileConfig c;
-    if (p->ky == 1 && vol3d(p)) {  // one row of columns (the transposed 1D parallel kind)
+    if (quarter_turn) {
+        c.zpt = kSymQueueZpt;
+        c.bx = 8;
+        c.by = 32;
+    } else if (p->ky == 1 && vol3d(p)) {  // one row of columns (the transposed 1D parallel kind)
         c.bx = 256;
         c.by = 1;
         c.zpt = 16;
@@ -71,10 +86,13 @@ TileConfig default_config(const gct_fdk_plan *p)
 namespace {
 
 // Candidate (zpt, block) shapes; views per stage is tuned afterwards for the best shape.
-std::vector<TileConfig> shape_candidates(bool three_d, bool one_row)
+std::vector<TileConfig> shape_candidates(bool three_d, bool one_row, bool quarter_turn)
 {
     std::vector<TileConfig> c;
-    if (one_row) {
+    if (quarter_turn) {
+        for (auto b : {std::make_pair(8, 32), std::make_pair(4, 64), std::make_pair(16, 16), std::make_pair(32, 8)})
+            c.push_back({kSymQueueZpt, b.first, b.second, 32});
+    } else if (one_row) {
         for (int zpt : {8, 16}) c.push_back({zpt, 256, 1, 32});
     } else if (three_d) {
         for (int zpt : {8, 16})
@@ -99,10 +117,10 @@ struct QueueScratch {
 double time_config(const gct_fdk_plan *p, const StackRef &st, float *vol, const TileConfig &c, int num_sms,
                    QueueScratch &sc, cudaStream_t s)
 {
-    const int zc = queue_class(c.zpt);
+    const int zc = item_class(st, c);
     const int grid = std::max(1, queue_blocks_per_sm(p->opts.storage, zc)) * num_sms;
     const BpItem it = make_item(p, st, vol, c);
-    const int nvt = std::min(p->nv, 64);
+    const int nvt = std::min(item_views(p, st), st.quarter ? 16 : 64);
     const std::vector<BpWork> w = tile_entries(0, item_tiles(it), 0, nvt, kBpStore);
     sc.item.upload(&it, 1, "autotune item");
     sc.work.upload(w.data(), w.size(), "autotune work");
@@ -125,7 +143,7 @@ double time_config(const gct_fdk_plan *p, const StackRef &st, float *vol, const 
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    const double upd = static_cast<double>(p->vol.nx) * p->vol.ny * p->vol.nz * nvt;
+    const double upd = static_cast<double>(p->vol.nx) * p->vol.ny * p->vol.nz * nvt * (st.quarter ? 4 : 1);
     return upd / (static_cast<double>(best) * 1e-3);
 }
 
@@ -137,7 +155,7 @@ std::string tune_key(const gct_fdk_plan *p, int num_sms)
     return std::to_string(p->device) + "/" + std::to_string(static_cast<int>(p->kind)) + "/" +
            std::to_string(p->opts.storage) + "/" + std::to_string(p->z_affine) + "/" + std::to_string(p->kx) +
            "x" + std::to_string(p->ky) + "x" + std::to_string(p->kz) + "/" + std::to_string(p->nr) + "x" +
-           std::to_string(p->nc) + "/" + std::to_string(num_sms);
+           std::to_string(p->nc) + "/" + std::to_string(num_sms) + "/q" + std::to_string(p->sym);
 }
 
 }  // namespace
@@ -152,7 +170,7 @@ Tuned autotune(const gct_fdk_plan *p, const StackRef &st, float *vol, int num_sm
     }
     QueueScratch sc;
     Tuned best;
-    for (const TileConfig &c : shape_candidates(vol3d(p), p->ky == 1 && vol3d(p))) {
+    for (const TileConfig &c : shape_candidates(vol3d(p), p->ky == 1 && vol3d(p), st.quarter > 0)) {
         const double ups = time_config(p, st, vol, c, num_sms, sc, s);
         if (ups > best.ups) best = {c, ups};
     }
@@ -185,7 +203,7 @@ struct gct_fdk_batch {
     int num_sms = 148;
     bool use_graph = true;
     std::vector<std::unique_ptr<Item>> items;
-    // one queue per storage type and depth class present: index 2 * storage + class
+    // one queue per storage type and depth class present: index storage * kQueueClasses + class
     struct Queue {
         DevBuf<gct::BpItem> d_items;
         DevBuf<gct::BpWork> d_work;
@@ -235,7 +253,8 @@ void issue(gct_fdk_batch *b, cudaStream_t s)
         cudaStream_t ss = b->side[it.stream];
         if (!used[it.stream]) cuda_check(cudaStreamWaitEvent(ss, fork, 0), "stream wait");
         used[it.stream] = true;
-        prepare(it.plan, it.proj, it.st, 0, it.plan->nv, ss);
+        if (it.st.quarter) prepare_partners(it.plan, it.proj, it.st, 0, it.st.quarter, ss);
+        else prepare(it.plan, it.proj, it.st, 0, it.plan->nv, ss);
     }
     for (size_t k = 0; k < b->side.size(); ++k) {
         if (!used[k]) continue;
@@ -279,7 +298,8 @@ void build_batch(gct_fdk_batch *b, const gct_batch_item *items, uint32_t n, cons
         it->proj = src.proj_dev;
         it->vol = src.vol_dev;
         it->ws.alloc(src.plan->workspace_bytes(), "batch item workspace");
-        it->st = stack_of(src.plan, it->ws.p, true);
+        // quarter-turn plans keep their interleaved partner stacks and run in the quarter-turn queue
+        it->st = stack_of(src.plan, it->ws.p, false);
         b->items.push_back(std::move(it));
     }
     // filter stages: items of one plan share its filter scratch, so they run on one side stream
@@ -311,14 +331,14 @@ void build_batch(gct_fdk_batch *b, const gct_batch_item *items, uint32_t n, cons
             ip->cfg = t.cfg;
             ip->tuned_ups = t.ups;
         } else {
-            ip->cfg = default_config(ip->plan);
+            ip->cfg = default_config(ip->plan, ip->st.quarter > 0);
         }
     }
 
     // work queues: items by decreasing cost; an item whose single tile costs more than an even
     // share of the queue over 8 entries per block is split into view chunks (atomic adds)
     auto queue_of = [&](const gct_fdk_batch::Item &it) {
-        return (it.plan->opts.storage == GCT_STORAGE_F16 ? 1 : 0) * kQueueClasses + queue_class(it.cfg.zpt);
+        return (it.plan->opts.storage == GCT_STORAGE_F16 ? 1 : 0) * kQueueClasses + item_class(it.st, it.cfg);
     };
     for (int q = 0; q < 2 * kQueueClasses; ++q) {
         auto &Q = b->queue[q];
@@ -346,16 +366,17 @@ void build_batch(gct_fdk_batch *b, const gct_batch_item *items, uint32_t n, cons
             const gct_fdk_plan *p = it.plan;
             const BpItem bi = make_item(p, it.st, it.vol, it.cfg);
             const long long tiles = item_tiles(bi);
+            const int views = item_views(p, it.st);
             const double tile_cost = cost[o] / static_cast<double>(tiles);
             int split = static_cast<int>(std::ceil(tile_cost / std::max(target, 1.0)));
-            split = std::max(1, std::min(split, p->nv / 16));
+            split = std::max(1, std::min(split, views / 16));
             it.view_split = split;
             const int qi = static_cast<int>(qitems.size());
             qitems.push_back(bi);
             if (split > 1) Q.atomic_items.push_back(i);
             for (int c = 0; c < split; ++c) {
-                const int vb = static_cast<int>(static_cast<long long>(p->nv) * c / split);
-                const int ve = static_cast<int>(static_cast<long long>(p->nv) * (c + 1) / split);
+                const int vb = static_cast<int>(static_cast<long long>(views) * c / split);
+                const int ve = static_cast<int>(static_cast<long long>(views) * (c + 1) / split);
                 const auto w = tile_entries(qi, tiles, vb, ve - vb, split > 1 ? kBpAtomic : kBpStore);
                 work.insert(work.end(), w.begin(), w.end());
             }

@@ -116,8 +116,12 @@ constexpr int kQueueMaxVps = 64;    // views of coefficients staged per block ba
 inline bool queue_zpt_ok(int zpt) { return zpt == 1 || zpt == 4 || zpt == 8 || zpt == 16; }
 // Queue kernels by depth class, each compiled with its own register budget: class 0 runs tiles of
 // one voxel per thread along z (2D images; needs many resident warps to hide its gather latency),
-// class 1 tiles of 4, 8 or 16 (volumes; needs registers for its accumulators).
-constexpr int kQueueClasses = 2;
+// class 1 tiles of 4, 8 or 16 (volumes; needs registers for its accumulators), class 2 the tiles
+// of quarter-turn items (BpArgs.sym set, interleaved partner stacks): first-quadrant columns,
+// kSymQueueZpt voxels per thread along z, view ranges counted in base views.
+constexpr int kQueueClasses = 3;
+constexpr int kQueueSymClass = 2;
+constexpr int kSymQueueZpt = 8;
 inline int queue_class(int zpt) { return zpt == 1 ? 0 : 1; }
 // Blocks of a queue kernel resident per SM for the storage type (0 f32, 1 f16) and depth class.
 int queue_blocks_per_sm(int storage, int zclass);

@@ -222,7 +222,7 @@ void run_round(gct_fdk_server *s)
 {
     auto &sl = s->slot[s->round % 2];
     if (sl.used) cuda_check(cudaEventSynchronize(sl.done), "round slot");
-    constexpr int NQ = 2 * gct::kQueueClasses;  // index 2 * storage + depth class
+    constexpr int NQ = 2 * gct::kQueueClasses;  // index storage * kQueueClasses + depth class
     std::vector<gct::BpItem> items[NQ];
     std::vector<gct::BpWork> work[NQ];
     std::vector<std::pair<Request *, int>> advanced;

@@ -121,3 +121,42 @@ def test_batch_toeplitz_filter_items():
     ref = orc.fdk(case.og, case.ov, proj).reshape(got.shape)
     assert rel_rms(got, ref) <= 1e-3
     plan.close()
+
+
+def test_batch_quarter_turn_items():
+    # FP16 plans of full scans on square centred grids keep their interleaved partner stacks and
+    # run in the quarter-turn queue; against execute() of the same plans (the quarter-turn
+    # kernel, with another tile shape): <= 1e-5; a single-item batch of 240 views splits its 60
+    # base views into atomic chunks (at least 16 base views each)
+    import torch
+    kinds = ["cone_flat", "cone_cyl", "fan_arc", "cone_parallel", "parallel_2d"]
+    cases = [make_case(k) for k in kinds]
+    items = []
+    for c in cases:
+        proj = oracle_projections(c)
+        plan = g.FdkPlan(c.cg, c.vg, opts=g.FdkOptions(storage=g.STORAGE_F16))
+        assert plan.quarter_turn != 0
+        items.append((plan, torch.from_numpy(proj).cuda(),
+                      torch.full(c.vg.shape, float("nan"), dtype=torch.float32, device="cuda"), proj))
+    for tune in (True, False):
+        with g.FdkBatch([(p, d, v) for p, d, v, _ in items], autotune=tune) as batch:
+            batch.launch()
+            torch.cuda.synchronize()
+            for i, (case, (plan, dproj, vol, proj)) in enumerate(zip(cases, items)):
+                got = vol.cpu().numpy()
+                assert rel_rms(got, _alone(plan, dproj, case.vg.shape)) <= 1e-5, case.name
+                ref = orc.fdk(case.og, case.ov, proj).reshape(got.shape)
+                assert rel_rms(got, ref) <= 1e-3, case.name
+                assert batch.item_config(i)["z_per_thread"] == 8
+    for p, *_ in items:
+        p.close()
+    case = make_case("cone_flat", nv=240)
+    proj = oracle_projections(case)
+    with g.FdkPlan(case.cg, case.vg, opts=g.FdkOptions(storage=g.STORAGE_F16)) as plan:
+        dproj = torch.from_numpy(proj).cuda()
+        vol = torch.full(case.vg.shape, float("nan"), dtype=torch.float32, device="cuda")
+        with g.FdkBatch([(plan, dproj, vol)]) as batch:
+            assert batch.item_config(0)["view_split"] > 1
+            batch.launch()
+            torch.cuda.synchronize()
+            assert rel_rms(vol.cpu().numpy(), _alone(plan, dproj, case.vg.shape)) <= 1e-5
