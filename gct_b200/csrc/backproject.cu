@@ -750,12 +750,19 @@ __global__ void __launch_bounds__(kQueueThreads, ZC == 0 ? 4 : 2)
 }
 
 // Quarter-turn items of the work queue: tile (tx, ty, tz) of first-quadrant columns.
-template <int FAMILY, class Q>
-__device__ __noinline__ void queue_sym_tile(const BpItem &it, const BpArgs &a, int tx, int ty, int tz, int tid,
-                                            int mode, float4 *s_coef, float4 *s_w, int *s_cls)
+template <int FAMILY, class Q, int ZPT>
+__device__ __noinline__ void queue_sym_tile_z(const BpItem &it, const BpArgs &a, int tx, int ty, int tz, int tid,
+                                              int mode, float4 *s_coef, float4 *s_w, int *s_cls)
 {
-    sym_tile<FAMILY, Q, kSymQueueZpt>(a, tx * it.bx, ty * it.by, tz * kSymQueueZpt, it.bx, it.by, tid, kQueueThreads,
-                                      mode, s_coef, s_w, s_cls);
+    sym_tile<FAMILY, Q, ZPT>(a, tx * it.bx, ty * it.by, tz * ZPT, it.bx, it.by, tid, kQueueThreads, mode, s_coef, s_w,
+                             s_cls);
+}
+template <int FAMILY, class Q>
+__device__ __forceinline__ void queue_sym_tile(const BpItem &it, const BpArgs &a, int tx, int ty, int tz, int tid,
+                                               int mode, float4 *s_coef, float4 *s_w, int *s_cls)
+{
+    if (it.zpt == 1) queue_sym_tile_z<FAMILY, Q, 1>(it, a, tx, ty, tz, tid, mode, s_coef, s_w, s_cls);
+    else queue_sym_tile_z<FAMILY, Q, 8>(it, a, tx, ty, tz, tid, mode, s_coef, s_w, s_cls);
 }
 
 template <class Q>

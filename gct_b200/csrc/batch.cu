@@ -38,8 +38,9 @@ BpItem make_item(const gct_fdk_plan *p, const StackRef &st, float *vol, const Ti
     it.bx = c.bx;
     it.by = c.by;
     it.vps = c.vps;
-    if (st.quarter) {  // quarter-turn item: tiles of first-quadrant columns, kSymQueueZpt deep
-        if (c.zpt != kSymQueueZpt) fail(GCT_ERR_INVALID_ARG, "quarter-turn queue tiles hold 8 voxels per thread");
+    if (st.quarter) {  // quarter-turn item: tiles of first-quadrant columns
+        if (!sym_queue_zpt_ok(c.zpt))
+            fail(GCT_ERR_INVALID_ARG, "quarter-turn queue tiles hold 8 voxels per thread (1 for 2D images)");
         it.a.sym = p->sym;
         it.a.v_count = st.quarter;
         it.tiles_x = (p->kx / 2 + c.bx - 1) / c.bx;
@@ -68,9 +69,9 @@ TileConfig default_config(const gct_fdk_plan *p, bool quarter_turn)
 {
     TileConfig c;
     if (quarter_turn) {
-        c.zpt = kSymQueueZpt;
-        c.bx = 8;
-        c.by = 32;
+        c.zpt = vol3d(p) ? 8 : 1;
+        c.bx = vol3d(p) ? 8 : 16;
+        c.by = vol3d(p) ? 32 : 16;
     } else if (p->ky == 1 && vol3d(p)) {  // one row of columns (the transposed 1D parallel kind)
         c.bx = 256;
         c.by = 1;
@@ -91,7 +92,7 @@ std::vector<TileConfig> shape_candidates(bool three_d, bool one_row, bool quarte
     std::vector<TileConfig> c;
     if (quarter_turn) {
         for (auto b : {std::make_pair(8, 32), std::make_pair(4, 64), std::make_pair(16, 16), std::make_pair(32, 8)})
-            c.push_back({kSymQueueZpt, b.first, b.second, 32});
+            c.push_back({three_d ? 8 : 1, b.first, b.second, 32});
     } else if (one_row) {
         for (int zpt : {8, 16}) c.push_back({zpt, 256, 1, 32});
     } else if (three_d) {

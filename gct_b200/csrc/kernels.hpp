@@ -118,10 +118,10 @@ inline bool queue_zpt_ok(int zpt) { return zpt == 1 || zpt == 4 || zpt == 8 || z
 // one voxel per thread along z (2D images; needs many resident warps to hide its gather latency),
 // class 1 tiles of 4, 8 or 16 (volumes; needs registers for its accumulators), class 2 the tiles
 // of quarter-turn items (BpArgs.sym set, interleaved partner stacks): first-quadrant columns,
-// kSymQueueZpt voxels per thread along z, view ranges counted in base views.
+// 8 voxels per thread along z (1 for 2D images), view ranges counted in base views.
 constexpr int kQueueClasses = 3;
 constexpr int kQueueSymClass = 2;
-constexpr int kSymQueueZpt = 8;
+inline bool sym_queue_zpt_ok(int zpt) { return zpt == 1 || zpt == 8; }
 inline int queue_class(int zpt) { return zpt == 1 ? 0 : 1; }
 // Blocks of a queue kernel resident per SM for the storage type (0 f32, 1 f16) and depth class.
 int queue_blocks_per_sm(int storage, int zclass);

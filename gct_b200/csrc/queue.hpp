@@ -26,7 +26,7 @@ bool vol3d(const gct_fdk_plan *p);
 // Fails unless bx * by == kQueueThreads and zpt is a queue shape: every thread of a block owns
 // one column of its tile, and tiles must not overlap (accumulating entries would add twice).
 // A stack in the quarter-turn layout (st.quarter > 0) makes a quarter-turn item: tiles over the
-// first quadrant of columns, kSymQueueZpt deep, views counted in base views.
+// first quadrant of columns, 8 voxels deep (1 for 2D images), views counted in base views.
 BpItem make_item(const gct_fdk_plan *p, const StackRef &st, float *vol, const TileConfig &c);
 long long item_tiles(const BpItem &it);
 // Views that work entries of the item count (base views for quarter-turn items) and its queue

@@ -69,7 +69,7 @@ struct Request {
     float *proj_dev = nullptr, *vol_dev = nullptr;
     StackRef st;
     gct::TileConfig cfg;
-    int chunk = 0, next_view = 0;
+    int chunk = 0, next_view = 0;  // views per round and the next view (base views for quarter-turn stacks)
     uint32_t rounds = 0;
     gct_req_state state = GCT_REQ_QUEUED;
     gct_status status = GCT_OK;
@@ -142,11 +142,14 @@ size_t footprint(const gct_fdk_plan *p, size_t *proj_bytes, size_t *vol_bytes)
 }
 
 // Views per round of a request: about round_updates voxel-view updates, at least 16 views.
-int chunk_views(const gct_fdk_plan *p, double round_updates)
+// Views per round (at least 16) for about round_updates voxel-view updates; for a quarter-turn
+// stack the views of a round are base views, each worth four.
+int chunk_views(const gct_fdk_plan *p, const StackRef &st, double round_updates)
 {
-    const double vox = static_cast<double>(p->vol.nx) * p->vol.ny * p->vol.nz;
+    const double vox = static_cast<double>(p->vol.nx) * p->vol.ny * p->vol.nz * (st.quarter ? 4 : 1);
     const double v = std::floor(round_updates / std::max(vox, 1.0));
-    return static_cast<int>(std::max(16.0, std::min(static_cast<double>(p->nv), v)));
+    const int views = gct::item_views(p, st);
+    return static_cast<int>(std::max(st.quarter ? 4.0 : 16.0, std::min(static_cast<double>(views), v)));
 }
 
 void finish(gct_fdk_server *s, Request *r, gct_req_state state, gct_status status)
@@ -197,23 +200,25 @@ void start(gct_fdk_server *s, Request *r)
     r->proj_dev = reinterpret_cast<float *>(base);
     unsigned char *ws = base + gct::Arena::round_up(r->proj_bytes);
     r->vol_dev = reinterpret_cast<float *>(ws + gct::Arena::round_up(r->plan->workspace_bytes()));
-    r->st = stack_of(r->plan, ws, true);
+    // quarter-turn plans keep their interleaved partner stacks (the quarter-turn queue class)
+    r->st = stack_of(r->plan, ws, false);
     for (cudaEvent_t *e : {&r->e_in, &r->e_prep, &r->e_out})
         cuda_check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "request event");
     cuda_check(cudaMemcpyAsync(r->proj_dev, r->proj_host, r->proj_bytes, cudaMemcpyHostToDevice, s->s_in),
                "projection upload");
     cuda_check(cudaEventRecord(r->e_in, s->s_in), "event record");
     cuda_check(cudaStreamWaitEvent(s->s_prep, r->e_in, 0), "stream wait");
-    prepare(r->plan, r->proj_dev, r->st, 0, r->plan->nv, s->s_prep);
+    if (r->st.quarter) prepare_partners(r->plan, r->proj_dev, r->st, 0, r->st.quarter, s->s_prep);
+    else prepare(r->plan, r->proj_dev, r->st, 0, r->plan->nv, s->s_prep);
     cuda_check(cudaEventRecord(r->e_prep, s->s_prep), "event record");
-    r->chunk = chunk_views(r->plan, s->round_updates);
+    r->chunk = chunk_views(r->plan, r->st, s->round_updates);
 }
 
 void activate(gct_fdk_server *s, Request *r)
 {
     cuda_check(cudaStreamWaitEvent(s->s_bp, r->e_prep, 0), "stream wait");
     r->cfg = s->autotune ? gct::autotune(r->plan, r->st, r->vol_dev, s->num_sms, s->s_bp).cfg
-                         : gct::default_config(r->plan);
+                         : gct::default_config(r->plan, r->st.quarter > 0);
     s->active.push_back(r);
 }
 
@@ -228,8 +233,8 @@ void run_round(gct_fdk_server *s)
     std::vector<std::pair<Request *, int>> advanced;
     for (Request *r : s->active) {
         const int q = (r->plan->opts.storage == GCT_STORAGE_F16 ? 1 : 0) * gct::kQueueClasses +
-                      gct::queue_class(r->cfg.zpt);
-        const int vb = r->next_view, vc = std::min(r->chunk, r->plan->nv - vb);
+                      gct::item_class(r->st, r->cfg);
+        const int vb = r->next_view, vc = std::min(r->chunk, gct::item_views(r->plan, r->st) - vb);
         const gct::BpItem it = gct::make_item(r->plan, r->st, r->vol_dev, r->cfg);
         const int idx = static_cast<int>(items[q].size());
         items[q].push_back(it);
@@ -283,7 +288,7 @@ void run_round(gct_fdk_server *s)
         Request *r = a.first;
         r->next_view += a.second;
         ++r->rounds;
-        if (r->next_view < r->plan->nv) {
+        if (r->next_view < gct::item_views(r->plan, r->st)) {
             still.push_back(r);
             continue;
         }

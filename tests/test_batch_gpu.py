@@ -147,7 +147,7 @@ def test_batch_quarter_turn_items():
                 assert rel_rms(got, _alone(plan, dproj, case.vg.shape)) <= 1e-5, case.name
                 ref = orc.fdk(case.og, case.ov, proj).reshape(got.shape)
                 assert rel_rms(got, ref) <= 1e-3, case.name
-                assert batch.item_config(i)["z_per_thread"] == 8
+                assert batch.item_config(i)["z_per_thread"] == (1 if case.name == "fan_arc" else 8)
     for p, *_ in items:
         p.close()
     case = make_case("cone_flat", nv=240)

@@ -132,3 +132,36 @@ def test_poisson_arrivals_report_latency():
         assert st["p99_ms"] >= st["p50_ms"] > 0
     for _, p, _ in reqs:
         p.close()
+
+
+def test_quarter_turn_requests_alone_and_in_mix():
+    # FP16 plans of full scans keep their interleaved partner stacks in the server and run in the
+    # quarter-turn queue: identical alone and in a mix, and against execute() of the same plan (the
+    # quarter-turn kernel, same per-thread sums in another chunking) within rounding
+    def request(kind, scale=1.0, **kw):
+        case = make_case(kind, **kw)
+        proj = (oracle_projections(case) * np.float32(scale)).astype(np.float32)
+        plan = g.FdkPlan(case.cg, case.vg, opts=g.FdkOptions(storage=g.STORAGE_F16))
+        assert plan.quarter_turn != 0
+        return case, plan, proj
+
+    a_case, a_plan, a_proj = request("cone_cyl", nv=240)
+    others = [request("fan_arc"), request("cone_flat", scale=2.0), request("cone_parallel")]
+    with g.FdkServer(512 * MB, round_updates=2e5) as srv:
+        alone = np.empty(a_case.vg.shape, np.float32)
+        t = srv.submit(a_plan, a_proj, alone)
+        srv.wait(t)
+        assert srv.info(t)["rounds"] > 1
+        outs = [np.empty(c.vg.shape, np.float32) for c, _, _ in others]
+        mixed = np.empty(a_case.vg.shape, np.float32)
+        tickets = [srv.submit(p, pr, o) for (c, p, pr), o in zip(others[:2], outs[:2])]
+        tm = srv.submit(a_plan, a_proj, mixed)
+        tickets += [srv.submit(p, pr, o) for (c, p, pr), o in zip(others[2:], outs[2:])]
+        for tk in tickets + [tm]:
+            srv.wait(tk)
+        assert np.array_equal(alone, mixed)
+        assert rel_rms(alone, _execute(a_plan, a_case, a_proj)) <= 1e-5
+        for (c, p, pr), o in zip(others, outs):
+            assert rel_rms(o, _execute(p, c, pr)) <= 1e-5, c.name
+    for _, p, _ in [(a_case, a_plan, a_proj)] + others:
+        p.close()
