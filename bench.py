@@ -69,7 +69,7 @@ BATCH48_LABEL = ("48 uneven reconstructions in one persistent launch: 24 x 2D pa
 # Serving mix (C5): 70 % 2D fan (line detector, 768 cells at 1.0 mm, SOD 570, SDD 1040, 720 views ->
 # 512^2 at 0.8 mm), 25 % cylindrical cone (the C4 geometry -> 512 x 512 x 64), 5 % flat cone 512^3
 # (the cone512 workload); 80 GB budget, mixed precision (FP16 quads; the flat cone with the
-# four-term Toeplitz filter, the others with the FFT filter).
+# FP16-split Toeplitz filter, the others with the FFT filter).
 SERVE_LABEL = ("Poisson arrivals, mix 70/25/5: 2D fan 512^2 x 720 views / cylindrical cone 512x512x64 x 1152 "
                "views / flat cone 512^3 x 720 views, 80 GB budget, mixed precision")
 EXTRA_CONFIGS = ["batch48", "serve"]
@@ -87,8 +87,9 @@ def parse_args():
                     help="arrival rates as fractions of the measured capacity (serve)")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--zpt", type=int, default=0, help="backprojection z per thread (0 = default)")
-    ap.add_argument("--mixed-filter", choices=["gemm4", "gemm3", "fft"], default="gemm4",
-                    help="ramp filter of the mixed path: split-BF16 Toeplitz GEMM on tcgen05 in the four-term "
+    ap.add_argument("--mixed-filter", choices=["gemm16", "gemm4", "gemm3", "fft"], default="gemm16",
+                    help="ramp filter of the mixed path: split Toeplitz GEMM on tcgen05 with rows in two FP16 "
+                         "pieces (one full term + three over the diagonal band), split-BF16 in the four-term "
                          "form (three pieces of rows and central taps) or three terms, or the FFT")
     ap.add_argument("--symmetry", choices=["auto", "off", "on"], default="auto",
                     help="quarter-turn backprojection: auto (FP16 storage, when the scan has it), off, on")
@@ -380,8 +381,8 @@ def run_gct(args, cfg, rank, world, local_rank):
     updates = nx * ny * nz * cg.num_views
     proj = make_projections(cg, cfg, args.seed + rank, device)
     stream = torch.cuda.current_stream()
-    mixed_filter = {"gemm4": g.FILTER_TOEPLITZ_BF16X4, "gemm3": g.FILTER_TOEPLITZ_BF16X3,
-                    "fft": g.FILTER_FFT}[args.mixed_filter]
+    mixed_filter = {"gemm16": g.FILTER_TOEPLITZ_F16X2, "gemm4": g.FILTER_TOEPLITZ_BF16X4,
+                    "gemm3": g.FILTER_TOEPLITZ_BF16X3, "fft": g.FILTER_FFT}[args.mixed_filter]
     sym = {"auto": g.SYMMETRY_AUTO, "off": g.SYMMETRY_OFF, "on": g.SYMMETRY_ON}[args.symmetry]
     plans = {
         "mixed": g.FdkPlan(cg, vg, opts=g.FdkOptions(filter=mixed_filter, storage=g.STORAGE_F16,
@@ -486,9 +487,13 @@ def run_gct(args, cfg, rank, world, local_rank):
         "cpu_baseline": cpu,
         "e2e": e2e,
         "clocks": clocks,
-        # per mixed step: view max, view scale, (split, GEMM, quads | FFT filter), backprojection
-        "gpu_launches": (4 if args.mixed_filter == "fft" else 6) * args.steps,
-        "mixed_filter": {"gemm4": "split-BF16 Toeplitz GEMM on tcgen05, 3 full terms + 2 banded (rows and central "
+        # per mixed step: GEMM forms split (with the view maxima), view scales, GEMM, quads,
+        # backprojection; FFT: view maxima, view scales, FFT filter, (partner quads), backprojection
+        "gpu_launches": (5 if args.mixed_filter != "fft" or mixed_quarter_turn else 4) * args.steps,
+        "mixed_filter": {"gemm16": "split-FP16 Toeplitz GEMM on tcgen05, 1 full term + 3 banded (rows scaled per row "
+                                   "in two FP16 pieces, central taps in three, far taps' dropped parts folded into "
+                                   "the central tap)",
+                         "gemm4": "split-BF16 Toeplitz GEMM on tcgen05, 3 full terms + 2 banded (rows and central "
                                   "taps in three BF16 pieces)",
                          "gemm3": "split-BF16 Toeplitz GEMM on tcgen05, 3 terms",
                          "fft": "shared-memory FFT"}[args.mixed_filter],
@@ -659,7 +664,7 @@ def run_serve(args, rank, world, local_rank):
                              n=(512, 512, 1), vox=0.8, voxz=1.0, n_ell=10), g.FILTER_FFT, 64),
         ("cyl", 0.25, cyl_item(), g.FILTER_FFT, 24),
         ("flat", 0.05, dict(kind="cone_flat", nv=720, nc=1024, nr=768, du=0.4, dv=0.4, sod=750.0, sdd=1200.0,
-                            n=(512, 512, 512), vox=0.5, voxz=0.5, n_ell=16), g.FILTER_TOEPLITZ_BF16X4, 6),
+                            n=(512, 512, 512), vox=0.5, voxz=0.5, n_ell=16), g.FILTER_TOEPLITZ_F16X2, 6),
     ]
     cls = []
     for i, (name, frac, c, filt, nbuf) in enumerate(kinds):

@@ -9,7 +9,8 @@ from .geometry import (ApodFunc, AxialCTGeom, ConeBeamProjGeomParams, CTGeom, De
                        Parallel2DProjGeomParams, ProjectionMatrix, ProjectionStack, ProjGeom, ProjGeomFactory,
                        ReconImg, ReconImgGeom, RotationGeom, RotationParams, RotDir, SpiralCTGeom,
                        is_valid_axial_recon, kind_of, map_point, parker_weights, ramp_filter_taps, VIEW_DTYPE)
-from .recon import (FILTER_FFT, FILTER_TOEPLITZ_BF16X3, FILTER_TOEPLITZ_BF16X4, SCAN_AXIAL, SCAN_SPIRAL, STORAGE_F16,
+from .recon import (FILTER_FFT, FILTER_TOEPLITZ_BF16X3, FILTER_TOEPLITZ_BF16X4, FILTER_TOEPLITZ_F16X2,
+                    SCAN_AXIAL, SCAN_SPIRAL, STORAGE_F16,
                     STORAGE_F32, SYMMETRY_AUTO, SYMMETRY_OFF, SYMMETRY_ON, FdkBatch, FdkOptions, FdkPlan, FdkServer,
                     FiltParams, forward_project, phantom_project, reconstruct)
 

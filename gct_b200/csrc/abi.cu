@@ -1,6 +1,7 @@
 // C ABI of the FDK engine (include/gct_fdk.h): plans, execution, stage entry points and the
 // host geometry functions. All failures become a gct_status plus a thread-local message.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -47,6 +48,53 @@ bool orthonormal(const double *a, const double *b, double tol)
 
 namespace {
 
+// FP16 value of x as the 16-bit pattern the GEMM buffers hold; `back` gets its value.
+__nv_bfloat16 f16_bits(double x, double &back)
+{
+    const __half h = __float2half_rn(static_cast<float>(x));
+    back = static_cast<double>(__half2float(h));
+    __nv_bfloat16 b;
+    std::memcpy(&b, &h, sizeof(b));
+    return b;
+}
+
+// Tap pieces of the FP16 form (filter_gemm.cu): taps scaled by a power of two so that the largest
+// is below 2^14; within the band |c - k| <= kGemmBand three FP16 pieces, beyond it the hi piece
+// alone, and per output column c the parts dropped beyond the band added to its central tap (before
+// that tap is split), so every column's sum of taps keeps its exact value.
+void toeplitz_f16(gct_fdk_plan *p, const std::vector<double> &taps, std::vector<__nv_bfloat16> &bh,
+                  std::vector<__nv_bfloat16> &bl, std::vector<__nv_bfloat16> &bll)
+{
+    double tmax = 0.0;
+    for (double t : taps) tmax = std::max(tmax, std::fabs(t));
+    int e = 0;
+    if (tmax > 0.0) std::frexp(tmax, &e);  // tmax < 2^e
+    const int sh = tmax > 0.0 ? std::min(100, std::max(-100, 14 - e)) : 0;
+    const double st = std::ldexp(1.0, sh);
+    p->tap_inv = static_cast<float>(std::ldexp(1.0, -sh));
+    const int nc = p->nc, band = gct::kGemmBand;
+    for (int n = 0; n < nc; ++n) {
+        double comp = 0.0, back;
+        for (int k = 0; k < nc; ++k) {
+            const int m = n - k + nc / 2;
+            if (m < 0 || m >= nc || std::abs(n - k) <= band) continue;
+            const double t = taps[m] * st;
+            bh[static_cast<size_t>(n) * p->Kp + k] = f16_bits(t, back);
+            comp += t - back;
+        }
+        for (int k = std::max(0, n - band); k <= std::min(nc - 1, n + band); ++k) {
+            const int m = n - k + nc / 2;
+            if (m < 0 || m >= nc) continue;
+            const double t = taps[m] * st + (k == n ? comp : 0.0);
+            const size_t at = static_cast<size_t>(n) * p->Kp + k;
+            double h, l, ll;
+            bh[at] = f16_bits(t, h);
+            bl[at] = f16_bits(t - h, l);
+            bll[at] = f16_bits(t - h - l, ll);
+        }
+    }
+}
+
 void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
                 const gct_filt_params *filt, const gct_fdk_opts *opts)
 {
@@ -63,7 +111,7 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
     p->filt = filt ? *filt : gct_filt_params{1.0, GCT_APOD_NONE};
     if (opts) p->opts = *opts;
     if (p->opts.filter != GCT_FILTER_FFT && p->opts.filter != GCT_FILTER_TOEPLITZ_BF16X3 &&
-        p->opts.filter != GCT_FILTER_TOEPLITZ_BF16X4)
+        p->opts.filter != GCT_FILTER_TOEPLITZ_BF16X4 && p->opts.filter != GCT_FILTER_TOEPLITZ_F16X2)
         gct::fail(GCT_ERR_INVALID_ARG, "unknown filter option");
     if (p->opts.storage != GCT_STORAGE_F32 && p->opts.storage != GCT_STORAGE_F16)
         gct::fail(GCT_ERR_INVALID_ARG, "unknown storage option");
@@ -166,29 +214,35 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
         p->Kp = gct::gemm_pad_k(p->nc);
         p->Np = gct::gemm_pad_n(p->nc);
         const bool four = p->opts.filter == GCT_FILTER_TOEPLITZ_BF16X4;
+        const bool f16 = p->opts.filter == GCT_FILTER_TOEPLITZ_F16X2;
         std::vector<__nv_bfloat16> bh(static_cast<size_t>(p->Np) * p->Kp, __float2bfloat16(0.f)), bl(bh), bll;
-        if (four) bll = bh;
-        for (int n = 0; n < p->nc; ++n)
-            for (int k = 0; k < p->nc; ++k) {
-                const int m = n - k + p->nc / 2;
-                if (m < 0 || m >= p->nc) continue;
-                const double t = taps[m];
-                const __nv_bfloat16 hi = __float2bfloat16(static_cast<float>(t));
-                const double r1 = t - static_cast<double>(__bfloat162float(hi));
-                const __nv_bfloat16 lo = __float2bfloat16(static_cast<float>(r1));
-                const size_t at = static_cast<size_t>(n) * p->Kp + k;
-                bh[at] = hi;
-                bl[at] = lo;
-                if (four && std::abs(n - k) <= gct::kGemmBand)
-                    bll[at] = __float2bfloat16(static_cast<float>(r1 - static_cast<double>(__bfloat162float(lo))));
-            }
+        if (four || f16) bll = bh;
+        if (f16) {
+            toeplitz_f16(p, taps, bh, bl, bll);
+        } else {
+            for (int n = 0; n < p->nc; ++n)
+                for (int k = 0; k < p->nc; ++k) {
+                    const int m = n - k + p->nc / 2;
+                    if (m < 0 || m >= p->nc) continue;
+                    const double t = taps[m];
+                    const __nv_bfloat16 hi = __float2bfloat16(static_cast<float>(t));
+                    const double r1 = t - static_cast<double>(__bfloat162float(hi));
+                    const __nv_bfloat16 lo = __float2bfloat16(static_cast<float>(r1));
+                    const size_t at = static_cast<size_t>(n) * p->Kp + k;
+                    bh[at] = hi;
+                    bl[at] = lo;
+                    if (four && std::abs(n - k) <= gct::kGemmBand)
+                        bll[at] = __float2bfloat16(static_cast<float>(r1 - static_cast<double>(__bfloat162float(lo))));
+                }
+        }
         p->th.upload(bh.data(), bh.size(), "Toeplitz matrix (hi)");
         p->tl.upload(bl.data(), bl.size(), "Toeplitz matrix (lo)");
-        if (four) p->tll.upload(bll.data(), bll.size(), "Toeplitz matrix (third piece, central band)");
+        if (four || f16) p->tll.upload(bll.data(), bll.size(), "Toeplitz matrix (third piece, central band)");
         const size_t rows = static_cast<size_t>(p->nv) * p->nr;
         p->xh.alloc(rows * p->Kp, "GEMM rows (hi)");
         p->xl.alloc(rows * p->Kp, "GEMM rows (lo)");
         if (four) p->xll.alloc(rows * p->Kp, "GEMM rows (third piece)");
+        if (f16) p->grinv.alloc(rows, "GEMM row scales");
         p->ybuf.alloc(rows * p->nc, "GEMM filtered rows");
         p->gemm_err.alloc(1, "GEMM status");
         cuda_check(cudaMemset(p->gemm_err.p, 0, sizeof(int)), "GEMM status reset");
@@ -268,6 +322,8 @@ void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float 
     sa.xl = p->xl.p;
     sa.xll = p->xll.p;
     sa.amax = fused_scales ? fused_scales->amax : nullptr;
+    sa.rinv = p->grinv.p;
+    sa.tap_inv = p->tap_inv;
     gct::launch_split(sa, p->num_sms, s);
     cuda_check(cudaGetLastError(), "split kernel launch");
     if (fused_scales) {  // the split found the view maxima: scales before the quads are written
@@ -280,7 +336,10 @@ void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float 
     gl.xl = p->xl.p;
     gl.xll = p->xll.p;
     gl.tll = p->tll.p;
-    gl.terms = p->opts.filter == GCT_FILTER_TOEPLITZ_BF16X4 ? 4 : 3;
+    gl.form = p->opts.filter == GCT_FILTER_TOEPLITZ_BF16X4 ? gct::kGemmBf16x4
+              : p->opts.filter == GCT_FILTER_TOEPLITZ_F16X2  ? gct::kGemmF16x2
+                                                             : gct::kGemmBf16x3;
+    gl.rinv = p->grinv.p;
     gl.a_rows = static_cast<long long>(p->nv) * p->nr;
     gl.th = p->th.p;
     gl.tl = p->tl.p;

@@ -3,34 +3,40 @@
 // The reference filters each detector row by FFT convolution (src/cuda/recon/ramp_filtering_fft.cuh:
 // 208-219). A row convolution with N taps is also the product of the row with an N x N Toeplitz
 // matrix T[k][c] = g(c - k), so a whole projection stack is one GEMM Y = X T with
-// M = views x rows, K = N = detector columns. Here it runs as a 3-term split-precision BF16 GEMM
-// with FP32 accumulation:
-//     X = Xh + Xl, T = Th + Tl (BF16 hi/lo parts),  Y = Xh Th + Xh Tl + Xl Th
-// (the dropped Xl Tl term is ~2^-16 relative), or in a four-term form with three pieces of X
-// and of the central taps:
-//     X = Xh + Xl + Xll,  Y = Xh Th + Xh Tl + Xl Th + Xll Th + Xh Tll,
-// where Tll is kept for |c - k| <= kBand only, and the Xll Th term also runs over that band only
-// (Xll is rounding noise 2^-16 below the values, so the far taps add nothing it carries): the
-// last two terms cover the few K blocks around each output tile's diagonal. Two BF16 pieces hold
-// a value to about 2^-17 relative, and ramp
-// filtering removes the large smooth part of a projection, so residuals of that part are a large
-// fraction of the filtered value. The two-piece taps keep a DC response of about 1e-6 that
-// multiplies the smooth part of every view alike and adds up over views: 1.1e-3 relative RMS in
-// a 512^3 volume with noisy 720-view input, against 7.9e-5 with the four-term form. Stages:
-//   1. split_kernel: cosine x Parker weighting fused into the load, BF16 hi/lo split, zero padding
-//      of K to a multiple of 64;
+// M = views x rows, K = N = detector columns, FP32 accumulation in TMEM. Three split forms:
+//   * BF16, three terms: X = Xh + Xl, T = Th + Tl (BF16 hi/lo parts), Y = Xh Th + Xh Tl + Xl Th
+//     (the dropped Xl Tl term is ~2^-16 relative).
+//   * BF16, four terms: X = Xh + Xl + Xll, Y = Xh Th + Xh Tl + Xl Th + Xll Th + Xh Tll, where Tll
+//     is kept for |c - k| <= kBand only, and the Xll Th term also runs over the K blocks of that
+//     band only (Xll is rounding noise 2^-16 below the values, so the far taps add nothing it
+//     carries).
+//   * FP16, two pieces of the rows: each row scaled by a power of two so that its largest value
+//     is below 2^14, the taps likewise, X = Xh + Xl and T = Th + Tl + Tll in FP16 pieces, and
+//     Y = Xh Th + (Xh Tl + Xl Th + Xh Tll over the band). Away from the diagonal a tap is its FP16
+//     hi piece alone; what that drops is added to the central tap of the same output column, so
+//     every column's DC response is exact to FP32 rounding. One full K pass instead of three.
+// Two BF16 pieces hold a value to about 2^-17 relative, and ramp filtering removes the large
+// smooth part of a projection, so residuals of that part are a large fraction of the filtered
+// value: the two-piece BF16 taps keep a DC response error of about 1e-6 that multiplies the smooth
+// part of every view alike and adds up over views. Relative RMS in a 512^3 volume with noisy
+// 720-view input: three BF16 terms 1.1e-3 and four 7.9e-5 with FP16 quads; of that the filter
+// alone (FP64 emulation of the forms on the two central slices) 4.0e-5 for four BF16 terms and
+// 4.1e-6 for the FP16 form. Stages:
+//   1. split_kernel: cosine x Parker weighting fused into the load, split into pieces (FP16: with
+//      the row's scale, written beside the pieces), zero padding of K to a multiple of 64;
 //   2. toeplitz_gemm_kernel: persistent, warp-specialised tcgen05 GEMM. Warp 0 issues TMA loads of
 //      128 x 64 A tiles and 256 x 64 B tiles (128B swizzle) into a 4-stage shared-memory ring;
 //      one thread of warp 1 issues tcgen05.mma (M 128, N 256, K 16) into one of two TMEM
 //      accumulators of 256 FP32 columns; warps 2-5 drain the other accumulator with tcgen05.ld and
-//      store FP32 rows. The terms are one K loop of (3 x K/64) steps plus the band steps of the
-//      four-term form.
+//      store FP32 rows (FP16 form: times the row's inverse scale). An output tile's K loop is the
+//      full-K segments of its form followed by its band segments.
 //   3. quads_from_rows_kernel: the filtered rows become the backprojector's bilinear-coefficient
 //      quads (FP32 or FP16 with the per-view scale).
 // Every mbarrier wait is bounded (2 s of %globaltimer); on timeout the kernel records an error
 // code, stops issuing work, frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cudaTypedefs.h>
 
 #include "../../include/gct_fdk.h"
@@ -41,7 +47,7 @@ namespace gct {
 namespace {
 
 constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4, UMMA_K = 16;
-constexpr int kBand = kGemmBand;  // taps with |c - k| <= kBand carry a third BF16 piece (four-term form)
+constexpr int kBand = kGemmBand;  // taps with |c - k| <= kBand carry the band pieces
 constexpr uint32_t A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int TMEM_COLS = 512;  // two accumulators of BN FP32 columns
 constexpr unsigned long long kWaitNs = 2000000000ull;
@@ -101,16 +107,17 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr)
     return static_cast<uint64_t>((addr >> 4) & 0x3FFFu) | (1ull << 16) | (static_cast<uint64_t>(1024 >> 4) << 32) |
            (1ull << 46) | (2ull << 61);
 }
-// kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, M = 128, N = 256.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(BN >> 3) << 17) |
-                            (static_cast<uint32_t>(BM >> 4) << 24);
+// kind::f16 instruction descriptors: FP32 accumulator, A and B of one type (format 1 in both
+// fields for BF16, 0 for FP16), both K-major, M = 128, N = 256.
+constexpr uint32_t kIdescF16 = (1u << 4) | (static_cast<uint32_t>(BN >> 3) << 17) | (static_cast<uint32_t>(BM >> 4) << 24);
+constexpr uint32_t kIdescBF16 = kIdescF16 | (1u << 7) | (1u << 10);
 
-__device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate)
+__device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
 {
     asm volatile(
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
         " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(d_tmem),
-        "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
         : "memory");
 }
 __device__ __forceinline__ void umma_commit(uint32_t bar)
@@ -136,20 +143,52 @@ struct GemmParams {
     int m_tiles, n_tiles;
     float *Y;       // [M][ldy] FP32, row m_begin + i at Y + i * ldy
     int ldy;
-    int terms;      // 3, or 4 plus the banded Xh Tll term
+    int form;       // GemmForm
+    const float *rinv;  // FP16 form: per-row inverse scale, indexed like the A rows
     int *err;       // set non-zero on a timed-out wait
 };
 
-// K blocks of the banded Xh Tll term for the output tile starting at column n0: the rows k with
+// K blocks of the band segments for the output tile starting at column n0: the rows k with
 // |c - k| <= kBand for some c in [n0, n0 + BN).
 __device__ __forceinline__ void band_blocks(const GemmParams &p, int n0, int &kb0, int &kb1)
 {
-    if (p.terms != 4) {
+    if (p.form == kGemmBf16x3) {
         kb0 = kb1 = 0;
         return;
     }
     kb0 = max(0, (n0 - kBand) / BK);
     kb1 = min(p.num_kb, (n0 + BN + kBand + BK - 1) / BK);
+}
+
+// Full-K segments of a form, and its band segments per band K block.
+__device__ __forceinline__ int full_segments(int form) { return form == kGemmF16x2 ? 1 : 3; }
+__device__ __forceinline__ int band_segments(int form) { return form == kGemmF16x2 ? 3 : form == kGemmBf16x4 ? 2 : 0; }
+
+// Operands of K step ks of a tile: A piece (0 hi, 1 lo, 2 third) and B piece (likewise) and the K
+// block. Segments, full K then band:
+//   BF16 three/four terms: Xh Th, Xh Tl, Xl Th | Xll Th, Xh Tll
+//   FP16:                  Xh Th               | Xh Tl, Xl Th, Xh Tll
+__device__ __forceinline__ void step_operands(const GemmParams &p, int ks, int kb0, int nband, int &pa, int &pb,
+                                              int &kb)
+{
+    const int kfull = full_segments(p.form) * p.num_kb;
+    int seg;
+    if (ks < kfull) {
+        seg = ks / p.num_kb;
+        kb = ks - seg * p.num_kb;
+    } else {
+        const int bs = ks - kfull;
+        const int j = bs / nband;
+        kb = kb0 + (bs - j * nband);
+        seg = full_segments(p.form) + j;
+    }
+    if (p.form == kGemmF16x2) {
+        pa = seg == 2 ? 1 : 0;
+        pb = seg == 1 ? 1 : seg == 3 ? 2 : 0;
+    } else {
+        pa = seg == 2 ? 1 : seg == 3 ? 2 : 0;
+        pb = seg == 1 ? 1 : seg == 4 ? 2 : 0;
+    }
 }
 
 __global__ void __launch_bounds__(192, 1)
@@ -194,10 +233,8 @@ __global__ void __launch_bounds__(192, 1)
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
     const int total = p.m_tiles * p.n_tiles;
-    // three full-K segments (Xh Th, Xh Tl, Xl Th); the four-term form then adds Xll Th and Xh Tll over
-    // the K blocks of the diagonal band: the third pieces are 2^-16 of the values, so taps beyond
-    // the band add nothing they carry (Xll is rounding noise without a smooth part)
-    const int kfull = 3 * p.num_kb;
+    const int kfull = full_segments(p.form) * p.num_kb, nbseg = band_segments(p.form);
+    const uint32_t idesc = p.form == kGemmF16x2 ? kIdescF16 : kIdescBF16;
 
     if (warp == 0) {
         if (lane == 0) {  // TMA producer
@@ -208,26 +245,18 @@ __global__ void __launch_bounds__(192, 1)
                 int kb0, kb1;
                 band_blocks(p, n0, kb0, kb1);
                 const int nband = kb1 - kb0;
-                const int ksteps = kfull + 2 * nband;
+                const int ksteps = kfull + nbseg * nband;
                 for (int ks = 0; ks < ksteps; ++ks) {
-                    // segments: 0 Xh Th, 1 Xh Tl, 2 Xl Th (full K); then 3 Xll Th and 4 Xh Tll over the band
-                    int seg, kb;
-                    if (ks < kfull) {
-                        seg = ks / p.num_kb;
-                        kb = ks - seg * p.num_kb;
-                    } else {
-                        const int bs = ks - kfull;
-                        seg = bs < nband ? 3 : 4;
-                        kb = kb0 + (bs < nband ? bs : bs - nband);
-                    }
+                    int pa, pb, kb;
+                    step_operands(p, ks, kb0, nband, pa, pb, kb);
                     if (!mbar_wait(empty(stage), phase ^ 1)) {
                         atomicExch(&s_fail, 1);
                         break;
                     }
                     mbar_expect_tx(full(stage), STAGE_BYTES);
                     const uint32_t sa = smem_u32(smem + stage * STAGE_BYTES);
-                    tma_load_2d(sa, seg == 3 ? &mAll : seg == 2 ? &mAl : &mAh, kb * BK, m0, full(stage));
-                    tma_load_2d(sa + A_BYTES, seg == 4 ? &mBll : seg == 1 ? &mBl : &mBh, kb * BK, n0, full(stage));
+                    tma_load_2d(sa, pa == 2 ? &mAll : pa == 1 ? &mAl : &mAh, kb * BK, m0, full(stage));
+                    tma_load_2d(sa + A_BYTES, pb == 2 ? &mBll : pb == 1 ? &mBl : &mBh, kb * BK, n0, full(stage));
                     if (++stage == STAGES) {
                         stage = 0;
                         phase ^= 1;
@@ -248,7 +277,7 @@ __global__ void __launch_bounds__(192, 1)
                 const uint32_t d = tmem_base + static_cast<uint32_t>(acc * BN);
                 int kb0, kb1;
                 band_blocks(p, (t % p.n_tiles) * BN, kb0, kb1);
-                const int ksteps = kfull + 2 * (kb1 - kb0);
+                const int ksteps = kfull + nbseg * (kb1 - kb0);
                 bool ok = true;
                 for (int ks = 0; ks < ksteps; ++ks) {
                     if (!mbar_wait(full(stage), phase)) {
@@ -261,7 +290,7 @@ __global__ void __launch_bounds__(192, 1)
                     const uint64_t da = smem_desc(sa), db = smem_desc(sa + A_BYTES);
 #pragma unroll
                     for (int k = 0; k < BK / UMMA_K; ++k)  // +32 B along K per step: +2 in the address field
-                        umma(d, da + 2 * k, db + 2 * k, (ks > 0 || k > 0) ? 1u : 0u);
+                        umma(d, da + 2 * k, db + 2 * k, idesc, (ks > 0 || k > 0) ? 1u : 0u);
                     umma_commit(empty(stage));
                     if (++stage == STAGES) {
                         stage = 0;
@@ -289,6 +318,8 @@ __global__ void __launch_bounds__(192, 1)
             tc_fence_after();
             const int row = mt * BM + q * 32 + lane;  // relative to m_begin
             float *yrow = p.Y + static_cast<long long>(row) * p.ldy;
+            // FP16 form: undo the row and tap scales (powers of two, exact); 1 otherwise
+            const float rs = (p.rinv && row < p.M) ? __ldg(p.rinv + p.m_begin + row) : 1.0f;
 #pragma unroll 1
             for (int ch = 0; ch < BN / 32; ++ch) {
                 uint32_t r[32];
@@ -301,12 +332,12 @@ __global__ void __launch_bounds__(192, 1)
                         float4 *dst = reinterpret_cast<float4 *>(yrow + c0);
 #pragma unroll
                         for (int j = 0; j < 8; ++j)
-                            dst[j] = make_float4(__uint_as_float(r[4 * j]), __uint_as_float(r[4 * j + 1]),
-                                                 __uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3]));
+                            dst[j] = make_float4(rs * __uint_as_float(r[4 * j]), rs * __uint_as_float(r[4 * j + 1]),
+                                                 rs * __uint_as_float(r[4 * j + 2]), rs * __uint_as_float(r[4 * j + 3]));
                     } else {
 #pragma unroll
                         for (int j = 0; j < 32; ++j)
-                            if (c0 + j < p.N) yrow[c0 + j] = __uint_as_float(r[j]);
+                            if (c0 + j < p.N) yrow[c0 + j] = rs * __uint_as_float(r[j]);
                     }
                 }
             }
@@ -328,9 +359,11 @@ __global__ void __launch_bounds__(192, 1)
     }
 }
 
-// Cosine x Parker weighting and BF16 split of rows [row0, row0 + rows) into [rows][Kp]: two or
-// three pieces per value. One warp per row (per-row view/row indices and geometry), four columns
-// per lane step (one 16-byte load when rows are 16-byte aligned) stored as 8-byte bf16x4 words.
+// Cosine x Parker weighting and split of rows [row0, row0 + rows) into [rows][Kp]: two or three
+// BF16 pieces per value, or (rinv set) two FP16 pieces of the value times the row's power-of-two
+// scale, whose inverse times the tap scale's goes to rinv[row]. One warp per row (per-row
+// view/row indices and geometry), four columns per lane step (one 16-byte load when rows are
+// 16-byte aligned) stored as 8-byte words of four 16-bit pieces.
 // With `amax`, the row's largest raw |p| also goes into amax[view] (atomic max of the bit
 // pattern, non-negative floats), which replaces the separate view-maximum pass.
 __device__ __forceinline__ uint2 bf16x4(float a, float b, float c, float d)
@@ -344,6 +377,125 @@ __device__ __forceinline__ uint2 bf16x4(float a, float b, float c, float d)
 __device__ __forceinline__ float bf16_lo(unsigned w) { return __uint_as_float(w << 16); }
 __device__ __forceinline__ float bf16_hi(unsigned w) { return __uint_as_float(w & 0xffff0000u); }
 
+// Weighted values x of columns [k, k + 4) of one row (zero beyond nc); m takes the max |raw|.
+__device__ __forceinline__ void weighted4(const SplitArgs &a, const float *src, const float *pk, float4 gv, int r,
+                                          int k, bool vec, float (&x)[4], float &m)
+{
+    float raw[4], pw[4];
+    if (vec && k + 3 < a.nc) {
+        const float4 p4 = __ldg(reinterpret_cast<const float4 *>(src + k));
+        const float4 w4 = __ldg(reinterpret_cast<const float4 *>(pk + k));
+        raw[0] = p4.x, raw[1] = p4.y, raw[2] = p4.z, raw[3] = p4.w;
+        pw[0] = w4.x, pw[1] = w4.y, pw[2] = w4.z, pw[3] = w4.w;
+    } else {
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const bool in = k + h < a.nc;
+            raw[h] = in ? __ldg(src + k + h) : 0.f;
+            pw[h] = in ? __ldg(pk + k + h) : 0.f;
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+        m = fmaxf(m, fabsf(raw[h]));
+        x[h] = raw[h] * pw[h] * cos_weight_dev(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k + h, r);
+    }
+}
+
+__device__ __forceinline__ uint2 f16x4(float a, float b, float c, float d)
+{
+    const __half2 lo = __floats2half2_rn(a, b), hi = __floats2half2_rn(c, d);
+    uint2 u;
+    u.x = *reinterpret_cast<const unsigned *>(&lo);
+    u.y = *reinterpret_cast<const unsigned *>(&hi);
+    return u;
+}
+
+// Power-of-two scale that puts a row's largest |x| (xm, warp-uniform) in [2^13, 2^14); the row's
+// 1 / (row scale x tap scale) goes to rinv[row].
+__device__ __forceinline__ float row_scale_f16(const SplitArgs &a, long long row, float xm, int lane)
+{
+    int e = 0;
+    if (xm > 0.f) frexpf(xm, &e);  // xm < 2^e
+    const int sh = xm > 0.f ? min(100, max(-100, 14 - e)) : 0;
+    if (lane == 0) a.rinv[row] = ldexpf(a.tap_inv, -sh);
+    return ldexpf(1.0f, sh);
+}
+
+// x (already scaled) -> two FP16 pieces, stored at word k4 of the row
+__device__ __forceinline__ void store_f16_pieces(const float (&x)[4], uint2 *dh, uint2 *dl, int k4)
+{
+    const uint2 hi = f16x4(x[0], x[1], x[2], x[3]);
+    dh[k4] = hi;
+    const __half2 h01 = *reinterpret_cast<const __half2 *>(&hi.x), h23 = *reinterpret_cast<const __half2 *>(&hi.y);
+    // exact in FP32: x and its FP16 rounding are within one FP16 ulp
+    dl[k4] = f16x4(x[0] - __low2float(h01), x[1] - __high2float(h01), x[2] - __low2float(h23), x[3] - __high2float(h23));
+}
+
+// One row of the FP16 form. NCH > 0 (rows of a multiple of 4 columns): every 16-byte load of the
+// row is issued first (NCH words of four columns per lane, Kp <= 128 NCH) and the weighted values
+// stay in registers between finding the row maximum and splitting; NCH == 0: two passes over the
+// row, the second recomputing the weighted values.
+template <int NCH>
+__device__ __forceinline__ void split_f16_row(const SplitArgs &a, long long row, const float *src, const float *pk,
+                                              float4 gv, int r, bool vec, uint2 *dh, uint2 *dl, int lane, float &m)
+{
+    const int nk4 = a.Kp / 4;
+    float xm = 0.f;
+    if constexpr (NCH > 0) {
+        float4 p4[NCH], w4[NCH];
+#pragma unroll
+        for (int c = 0; c < NCH; ++c) {  // columns past nc (K padding) read as zero
+            const int k = 4 * (lane + 32 * c);
+            const bool in = k < a.nc;
+            p4[c] = in ? __ldg(reinterpret_cast<const float4 *>(src + k)) : make_float4(0.f, 0.f, 0.f, 0.f);
+            w4[c] = in ? __ldg(reinterpret_cast<const float4 *>(pk + k)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        float x[NCH][4];
+#pragma unroll
+        for (int c = 0; c < NCH; ++c) {
+            const int k = 4 * (lane + 32 * c);
+            const float raw[4] = {p4[c].x, p4[c].y, p4[c].z, p4[c].w}, pw[4] = {w4[c].x, w4[c].y, w4[c].z, w4[c].w};
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                m = fmaxf(m, fabsf(raw[h]));
+                x[c][h] = raw[h] * pw[h] * cos_weight_dev(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k + h, r);
+                xm = fmaxf(xm, fabsf(x[c][h]));
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) xm = fmaxf(xm, __shfl_xor_sync(0xffffffffu, xm, o));
+        const float sc = row_scale_f16(a, row, xm, lane);
+#pragma unroll
+        for (int c = 0; c < NCH; ++c) {
+            const int k4 = lane + 32 * c;
+            if (k4 < nk4) {
+#pragma unroll
+                for (int h = 0; h < 4; ++h) x[c][h] *= sc;
+                store_f16_pieces(x[c], dh, dl, k4);
+            }
+        }
+    } else {
+        for (int k4 = lane; k4 < nk4; k4 += 32) {
+            float x[4];
+            weighted4(a, src, pk, gv, r, 4 * k4, vec, x, m);
+#pragma unroll
+            for (int h = 0; h < 4; ++h) xm = fmaxf(xm, fabsf(x[h]));
+        }
+        for (int o = 16; o > 0; o >>= 1) xm = fmaxf(xm, __shfl_xor_sync(0xffffffffu, xm, o));
+        const float sc = row_scale_f16(a, row, xm, lane);
+        for (int k4 = lane; k4 < nk4; k4 += 32) {
+            float x[4], mm = 0.f;
+            weighted4(a, src, pk, gv, r, 4 * k4, vec, x, mm);
+#pragma unroll
+            for (int h = 0; h < 4; ++h) x[h] *= sc;
+            store_f16_pieces(x, dh, dl, k4);
+        }
+    }
+}
+
+// NCH < 0: BF16 pieces; NCH >= 0: FP16 pieces (split_f16_row<NCH>), one instance per register
+// footprint.
+template <int NCH>
 __global__ void split_kernel(SplitArgs a)
 {
     const int lane = threadIdx.x & 31;
@@ -360,36 +512,21 @@ __global__ void split_kernel(SplitArgs a)
         uint2 *dl = reinterpret_cast<uint2 *>(a.xl + row * a.Kp);
         uint2 *dll = a.xll ? reinterpret_cast<uint2 *>(a.xll + row * a.Kp) : nullptr;
         float m = 0.f;
-        for (int k4 = lane; k4 < a.Kp / 4; k4 += 32) {
-            const int k = 4 * k4;
-            float raw[4], pw[4];
-            if (vec && k + 3 < a.nc) {
-                const float4 p4 = __ldg(reinterpret_cast<const float4 *>(src + k));
-                const float4 w4 = __ldg(reinterpret_cast<const float4 *>(pk + k));
-                raw[0] = p4.x, raw[1] = p4.y, raw[2] = p4.z, raw[3] = p4.w;
-                pw[0] = w4.x, pw[1] = w4.y, pw[2] = w4.z, pw[3] = w4.w;
-            } else {
-#pragma unroll
-                for (int h = 0; h < 4; ++h) {
-                    const bool in = k + h < a.nc;
-                    raw[h] = in ? __ldg(src + k + h) : 0.f;
-                    pw[h] = in ? __ldg(pk + k + h) : 0.f;
-                }
+        if (NCH >= 0) {
+            split_f16_row<(NCH > 0 ? NCH : 0)>(a, row, src, pk, gv, r, vec, dh, dl, lane, m);
+        } else {
+            for (int k4 = lane; k4 < a.Kp / 4; k4 += 32) {
+                float x[4];
+                weighted4(a, src, pk, gv, r, 4 * k4, vec, x, m);
+                const uint2 hi = bf16x4(x[0], x[1], x[2], x[3]);
+                dh[k4] = hi;
+                const float r0 = x[0] - bf16_lo(hi.x), r1 = x[1] - bf16_hi(hi.x);  // exact in FP32
+                const float r2 = x[2] - bf16_lo(hi.y), r3 = x[3] - bf16_hi(hi.y);
+                const uint2 lo = bf16x4(r0, r1, r2, r3);
+                dl[k4] = lo;
+                if (dll)
+                    dll[k4] = bf16x4(r0 - bf16_lo(lo.x), r1 - bf16_hi(lo.x), r2 - bf16_lo(lo.y), r3 - bf16_hi(lo.y));
             }
-            float x[4];
-#pragma unroll
-            for (int h = 0; h < 4; ++h) {
-                m = fmaxf(m, fabsf(raw[h]));
-                x[h] = raw[h] * pw[h] * cos_weight_dev(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k + h, r);
-            }
-            const uint2 hi = bf16x4(x[0], x[1], x[2], x[3]);
-            dh[k4] = hi;
-            const float r0 = x[0] - bf16_lo(hi.x), r1 = x[1] - bf16_hi(hi.x);  // exact in FP32
-            const float r2 = x[2] - bf16_lo(hi.y), r3 = x[3] - bf16_hi(hi.y);
-            const uint2 lo = bf16x4(r0, r1, r2, r3);
-            dl[k4] = lo;
-            if (dll)
-                dll[k4] = bf16x4(r0 - bf16_lo(lo.x), r1 - bf16_hi(lo.x), r2 - bf16_lo(lo.y), r3 - bf16_hi(lo.y));
         }
         if (a.amax) {
             for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -522,8 +659,9 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
     return fn;
 }
 
-// 2D BF16 tensor [rows][cols] (cols contiguous), box cols_box x rows_box, 128B swizzle.
-bool make_map(CUtensorMap *m, const void *base, unsigned long long rows, unsigned long long cols, unsigned rows_box)
+// 2D 16-bit tensor [rows][cols] (cols contiguous), box cols_box x rows_box, 128B swizzle.
+bool make_map(CUtensorMap *m, CUtensorMapDataType dt, const void *base, unsigned long long rows,
+              unsigned long long cols, unsigned rows_box)
 {
     auto fn = encode_fn();
     if (!fn) return false;
@@ -531,7 +669,7 @@ bool make_map(CUtensorMap *m, const void *base, unsigned long long rows, unsigne
     const cuuint64_t strides[1] = {cols * 2};
     const cuuint32_t box[2] = {static_cast<cuuint32_t>(BK), rows_box};
     const cuuint32_t estr[2] = {1, 1};
-    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
+    return fn(m, dt, 2, const_cast<void *>(base), dims, strides, box, estr,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -546,7 +684,12 @@ void launch_split(const SplitArgs &a, int num_sms, cudaStream_t s)
 {
     long long grid = (a.rows + 7) / 8;  // 8 warps (rows) per block
     if (grid > static_cast<long long>(num_sms) * 16) grid = static_cast<long long>(num_sms) * 16;
-    split_kernel<<<static_cast<unsigned>(grid < 1 ? 1 : grid), 256, 0, s>>>(a);
+    const unsigned g = static_cast<unsigned>(grid < 1 ? 1 : grid);
+    const bool vec = (a.nc & 3) == 0;
+    if (!a.rinv) split_kernel<-1><<<g, 256, 0, s>>>(a);
+    else if (vec && a.Kp <= 128 * 8) split_kernel<8><<<g, 256, 0, s>>>(a);
+    else if (vec && a.Kp <= 128 * 16) split_kernel<16><<<g, 256, 0, s>>>(a);
+    else split_kernel<0><<<g, 256, 0, s>>>(a);
 }
 
 void launch_quads_from_rows(const QuadArgs &a, int mode, int num_sms, cudaStream_t s)
@@ -581,12 +724,15 @@ void launch_quads_partners(const QuadArgs &a, int mode, int num_sms, cudaStream_
 
 cudaError_t launch_toeplitz_gemm(const GemmLaunch &g, int num_sms, cudaStream_t s)
 {
-    if (g.terms != 3 && !(g.terms == 4 && g.xll && g.tll)) return cudaErrorInvalidValue;
+    const bool four = g.form == kGemmBf16x4, f16 = g.form == kGemmF16x2;
+    if (!(g.form == kGemmBf16x3 || (four && g.xll && g.tll) || (f16 && g.tll && g.rinv)))
+        return cudaErrorInvalidValue;
+    const CUtensorMapDataType dt = f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     CUtensorMap mAh, mAl, mAll, mBh, mBl, mBll;
-    if (!make_map(&mAh, g.xh, g.a_rows, g.Kp, BM) || !make_map(&mAl, g.xl, g.a_rows, g.Kp, BM) ||
-        !make_map(&mAll, g.terms == 4 ? g.xll : g.xl, g.a_rows, g.Kp, BM) ||
-        !make_map(&mBh, g.th, g.Np, g.Kp, BN) || !make_map(&mBl, g.tl, g.Np, g.Kp, BN) ||
-        !make_map(&mBll, g.terms == 4 ? g.tll : g.tl, g.Np, g.Kp, BN))
+    if (!make_map(&mAh, dt, g.xh, g.a_rows, g.Kp, BM) || !make_map(&mAl, dt, g.xl, g.a_rows, g.Kp, BM) ||
+        !make_map(&mAll, dt, four ? g.xll : g.xl, g.a_rows, g.Kp, BM) ||
+        !make_map(&mBh, dt, g.th, g.Np, g.Kp, BN) || !make_map(&mBl, dt, g.tl, g.Np, g.Kp, BN) ||
+        !make_map(&mBll, dt, g.form == kGemmBf16x3 ? g.tl : g.tll, g.Np, g.Kp, BN))
         return cudaErrorInvalidValue;
     GemmParams p;
     p.M = g.M;
@@ -597,7 +743,8 @@ cudaError_t launch_toeplitz_gemm(const GemmLaunch &g, int num_sms, cudaStream_t 
     p.n_tiles = g.Np / BN;
     p.Y = g.Y;
     p.ldy = g.ldy;
-    p.terms = g.terms;
+    p.form = g.form;
+    p.rinv = f16 ? g.rinv : nullptr;
     p.err = g.err;
     const int tiles = p.m_tiles * p.n_tiles;
     const int grid = tiles < num_sms ? tiles : num_sms;

@@ -8,7 +8,11 @@ namespace gct {
 
 int gemm_pad_k(int n);  // K padded to the 64-column tile
 int gemm_pad_n(int n);  // N padded to the 256-column tile
-constexpr int kGemmBand = 64;  // |c - k| of the taps with a third BF16 piece (four-term form)
+constexpr int kGemmBand = 64;  // |c - k| of the band of the four-term and FP16 forms
+// Split forms of the Toeplitz GEMM (filter_gemm.cu): three BF16 terms, four BF16 terms (third
+// pieces over the band), FP16 rows in two pieces with scaled rows and taps (lo and third tap
+// pieces over the band).
+enum GemmForm : int { kGemmF16x2 = 2, kGemmBf16x3 = 3, kGemmBf16x4 = 4 };
 size_t toeplitz_gemm_smem_bytes();
 
 struct SplitArgs {
@@ -20,19 +24,23 @@ struct SplitArgs {
     float du = 0.f, dv = 0.f;
     const float4 *fview = nullptr;
     const float *parker = nullptr;
-    __nv_bfloat16 *xh = nullptr, *xl = nullptr;  // [all rows][Kp]
+    // 16-bit pieces [all rows][Kp]: BF16, or FP16 bit patterns when rinv is set
+    __nv_bfloat16 *xh = nullptr, *xl = nullptr;
     __nv_bfloat16 *xll = nullptr;                // third piece (four-term GEMM), or NULL
     float *amax = nullptr;                       // per-view max |raw value| (zeroed by the caller), or NULL
+    float *rinv = nullptr;                       // FP16 form: per-row 1 / (row scale x tap scale), [all rows]
+    float tap_inv = 1.f;                         // FP16 form: 1 / tap scale (a power of two)
 };
 void launch_split(const SplitArgs &a, int num_sms, cudaStream_t s);
 
 struct GemmLaunch {
-    const __nv_bfloat16 *xh = nullptr, *xl = nullptr;  // A: [a_rows][Kp]
-    const __nv_bfloat16 *xll = nullptr;                // third piece of A (terms == 4)
-    int terms = 3;                                     // 3: Xh Th + Xh Tl + Xl Th; 4: + Xll Th + Xh Tll
+    const __nv_bfloat16 *xh = nullptr, *xl = nullptr;  // A: [a_rows][Kp] (FP16 bit patterns in the FP16 form)
+    const __nv_bfloat16 *xll = nullptr;                // third piece of A (four-term form)
+    int form = kGemmBf16x3;
     long long a_rows = 0;
     const __nv_bfloat16 *th = nullptr, *tl = nullptr;  // B = T^T: [Np][Kp]
-    const __nv_bfloat16 *tll = nullptr;                // third piece of B, central band (terms == 4)
+    const __nv_bfloat16 *tll = nullptr;                // third piece of B, central band (four-term, FP16 forms)
+    const float *rinv = nullptr;                       // FP16 form: per-row inverse scale, [a_rows]
     int Np = 0, Kp = 0;
     int m_begin = 0, M = 0, N = 0;
     float *Y = nullptr;  // row m_begin + i at Y + i * ldy

@@ -111,10 +111,13 @@ struct gct_fdk_plan {
     DevBuf<float2> H, tw;
     DevBuf<float> coefs;
     DevBuf<unsigned char> work;
-    // Toeplitz-GEMM filter: B = T^T split into BF16 hi/lo [Np][Kp], A rows [nv*nr][Kp], FP32 rows
+    // Toeplitz-GEMM filter: B = T^T split into 16-bit hi/lo pieces [Np][Kp] (BF16, or FP16 bit
+    // patterns in the FP16 form), A rows [nv*nr][Kp], FP32 rows
     int Kp = 0, Np = 0;
     DevBuf<__nv_bfloat16> th, tl, xh, xl;
-    DevBuf<__nv_bfloat16> xll, tll;  // four-term filter: third piece of the rows and of the central taps
+    DevBuf<__nv_bfloat16> xll, tll;  // four-term filter: third piece of the rows; third tap piece over the band
+    DevBuf<float> grinv;             // FP16 form: per-row inverse scale of the GEMM rows
+    float tap_inv = 1.f;             // FP16 form: inverse of the taps' power-of-two scale
     DevBuf<float> ybuf;
     DevBuf<int> gemm_err;
     // staging for gct_fdk_execute_host: projections, two device volumes (consecutive calls

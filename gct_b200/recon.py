@@ -23,6 +23,7 @@ from .geometry import ApodFunc, AxialCTGeom, ProjectionStack, ReconImg, ReconImg
 FILTER_FFT = 0
 FILTER_TOEPLITZ_BF16X3 = 1
 FILTER_TOEPLITZ_BF16X4 = 2
+FILTER_TOEPLITZ_F16X2 = 3
 STORAGE_F32 = 0
 STORAGE_F16 = 1
 SYMMETRY_AUTO = 0

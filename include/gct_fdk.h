@@ -147,9 +147,13 @@ typedef struct gct_geom_params {
 enum {
     GCT_FILTER_FFT = 0,             /* own row-batched shared-memory FFT, FP32 arithmetic */
     GCT_FILTER_TOEPLITZ_BF16X3 = 1, /* 3-term split BF16 Toeplitz GEMM on tcgen05, FP32 accumulate */
-    GCT_FILTER_TOEPLITZ_BF16X4 = 2  /* projections in three BF16 pieces and the central taps
+    GCT_FILTER_TOEPLITZ_BF16X4 = 2, /* projections in three BF16 pieces and the central taps
                                      * (|c - k| <= 64) in three: three full GEMM terms plus two over
                                      * the diagonal band; removes the two-piece taps' DC error */
+    GCT_FILTER_TOEPLITZ_F16X2 = 3   /* rows scaled per row into two FP16 pieces, taps in FP16: one
+                                     * full GEMM term (hi x hi) plus three over the diagonal band,
+                                     * the far taps' dropped parts folded into each column's
+                                     * central tap so its DC response stays exact */
 };
 enum {
     GCT_STORAGE_F32 = 0, /* filtered projections kept in FP32 */

@@ -39,7 +39,7 @@ def _run(plan, proj, vg):
 def test_sampled_voxels_and_linearity(config):
     import torch
     cfg, cg, vg, proj = _setup(config)
-    mixed = g.FdkOptions(filter=g.FILTER_TOEPLITZ_BF16X4, storage=g.STORAGE_F16)
+    mixed = g.FdkOptions(filter=g.FILTER_TOEPLITZ_F16X2, storage=g.STORAGE_F16)
     with g.FdkPlan(cg, vg) as p32, g.FdkPlan(cg, vg, opts=mixed) as p16:
         vols = {"fp32": _run(p32, proj, vg), "mixed": _run(p16, proj, vg)}
         errs, n = bench.oracle_errors(cg, cfg, proj, vols, 1234)
