@@ -89,6 +89,33 @@ __device__ __forceinline__ float cos_weight_dev(int kind, float c0, float r0, fl
     }
 }
 
+// cos_weight_dev along one detector row r, with the kind's row-invariant parts taken once:
+// w(c) = R cos(u) (arc, cylindrical) or S / sqrt(U2 u^2 + B) (line, flat, cone-parallel, parallel),
+// u = (c - c0) du. The same weights as cos_weight_dev up to the rounding of the hoisted terms.
+struct RowWeight {
+    bool arc;
+    float c0, du, S, U2, B, R;
+    __device__ __forceinline__ float at(int c) const
+    {
+        const float u = (static_cast<float>(c) - c0) * du;
+        return arc ? R * cosf(u) : S * rsqrtf(fmaf(U2 * u, u, B));
+    }
+};
+__device__ __forceinline__ RowWeight row_weight(int kind, float c0, float r0, float sdd, float du, float dv, int r)
+{
+    const float v = (static_cast<float>(r) - r0) * dv;
+    RowWeight w{false, c0, du, 1.f, 0.f, 1.f, 1.f};
+    switch (kind) {
+        case GCT_GEOM_FAN_ARC: w.arc = true; break;
+        case GCT_GEOM_FAN_LINE: w.S = sdd, w.U2 = 1.f, w.B = sdd * sdd; break;
+        case GCT_GEOM_CONE_PARALLEL: w.S = sdd, w.B = v * v + sdd * sdd; break;
+        case GCT_GEOM_CONE_CYL: w.arc = true, w.R = sdd * rsqrtf(v * v + sdd * sdd); break;
+        case GCT_GEOM_CONE_FLAT: w.S = sdd, w.U2 = 1.f, w.B = v * v + sdd * sdd; break;
+        default: break;  // parallel kinds: 1 / sqrt(1) = 1
+    }
+    return w;
+}
+
 __device__ __forceinline__ float rcp_approx(float x)
 {
     float r;

@@ -378,7 +378,7 @@ __device__ __forceinline__ float bf16_lo(unsigned w) { return __uint_as_float(w 
 __device__ __forceinline__ float bf16_hi(unsigned w) { return __uint_as_float(w & 0xffff0000u); }
 
 // Weighted values x of columns [k, k + 4) of one row (zero beyond nc); m takes the max |raw|.
-__device__ __forceinline__ void weighted4(const SplitArgs &a, const float *src, const float *pk, float4 gv, int r,
+__device__ __forceinline__ void weighted4(const SplitArgs &a, const float *src, const float *pk, const RowWeight &rw,
                                           int k, bool vec, float (&x)[4], float &m)
 {
     float raw[4], pw[4];
@@ -398,7 +398,7 @@ __device__ __forceinline__ void weighted4(const SplitArgs &a, const float *src, 
 #pragma unroll
     for (int h = 0; h < 4; ++h) {
         m = fmaxf(m, fabsf(raw[h]));
-        x[h] = raw[h] * pw[h] * cos_weight_dev(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k + h, r);
+        x[h] = raw[h] * pw[h] * rw.at(k + h);
     }
 }
 
@@ -438,7 +438,7 @@ __device__ __forceinline__ void store_f16_pieces(const float (&x)[4], uint2 *dh,
 // row, the second recomputing the weighted values.
 template <int NCH>
 __device__ __forceinline__ void split_f16_row(const SplitArgs &a, long long row, const float *src, const float *pk,
-                                              float4 gv, int r, bool vec, uint2 *dh, uint2 *dl, int lane, float &m)
+                                              const RowWeight &rw, bool vec, uint2 *dh, uint2 *dl, int lane, float &m)
 {
     const int nk4 = a.Kp / 4;
     float xm = 0.f;
@@ -459,7 +459,7 @@ __device__ __forceinline__ void split_f16_row(const SplitArgs &a, long long row,
 #pragma unroll
             for (int h = 0; h < 4; ++h) {
                 m = fmaxf(m, fabsf(raw[h]));
-                x[c][h] = raw[h] * pw[h] * cos_weight_dev(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k + h, r);
+                x[c][h] = raw[h] * pw[h] * rw.at(k + h);
                 xm = fmaxf(xm, fabsf(x[c][h]));
             }
         }
@@ -477,7 +477,7 @@ __device__ __forceinline__ void split_f16_row(const SplitArgs &a, long long row,
     } else {
         for (int k4 = lane; k4 < nk4; k4 += 32) {
             float x[4];
-            weighted4(a, src, pk, gv, r, 4 * k4, vec, x, m);
+            weighted4(a, src, pk, rw, 4 * k4, vec, x, m);
 #pragma unroll
             for (int h = 0; h < 4; ++h) xm = fmaxf(xm, fabsf(x[h]));
         }
@@ -485,7 +485,7 @@ __device__ __forceinline__ void split_f16_row(const SplitArgs &a, long long row,
         const float sc = row_scale_f16(a, row, xm, lane);
         for (int k4 = lane; k4 < nk4; k4 += 32) {
             float x[4], mm = 0.f;
-            weighted4(a, src, pk, gv, r, 4 * k4, vec, x, mm);
+            weighted4(a, src, pk, rw, 4 * k4, vec, x, mm);
 #pragma unroll
             for (int h = 0; h < 4; ++h) x[h] *= sc;
             store_f16_pieces(x, dh, dl, k4);
@@ -506,6 +506,7 @@ __global__ void split_kernel(SplitArgs a)
         const long long row = a.row0 + rl;
         const int v = static_cast<int>(row / a.nr), r = static_cast<int>(row - static_cast<long long>(v) * a.nr);
         const float4 gv = __ldg(&a.fview[v]);
+        const RowWeight rw = row_weight(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, r);
         const float *src = a.proj + row * a.nc;
         const float *pk = a.parker + static_cast<long long>(v) * a.nc;
         uint2 *dh = reinterpret_cast<uint2 *>(a.xh + row * a.Kp);
@@ -513,11 +514,11 @@ __global__ void split_kernel(SplitArgs a)
         uint2 *dll = a.xll ? reinterpret_cast<uint2 *>(a.xll + row * a.Kp) : nullptr;
         float m = 0.f;
         if (NCH >= 0) {
-            split_f16_row<(NCH > 0 ? NCH : 0)>(a, row, src, pk, gv, r, vec, dh, dl, lane, m);
+            split_f16_row<(NCH > 0 ? NCH : 0)>(a, row, src, pk, rw, vec, dh, dl, lane, m);
         } else {
             for (int k4 = lane; k4 < a.Kp / 4; k4 += 32) {
                 float x[4];
-                weighted4(a, src, pk, gv, r, 4 * k4, vec, x, m);
+                weighted4(a, src, pk, rw, 4 * k4, vec, x, m);
                 const uint2 hi = bf16x4(x[0], x[1], x[2], x[3]);
                 dh[k4] = hi;
                 const float r0 = x[0] - bf16_lo(hi.x), r1 = x[1] - bf16_hi(hi.x);  // exact in FP32

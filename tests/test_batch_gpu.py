@@ -111,9 +111,10 @@ def test_batch_graph_and_direct_issue_agree():
         p.close()
 
 
-def test_batch_toeplitz_filter_items():
+@pytest.mark.parametrize("filt", [g.FILTER_TOEPLITZ_BF16X4, g.FILTER_TOEPLITZ_F16X2])
+def test_batch_toeplitz_filter_items(filt):
     case = make_case("cone_flat")
-    plan, dproj, vol, proj = _dev(case, storage=g.STORAGE_F16, filt=g.FILTER_TOEPLITZ_BF16X4)
+    plan, dproj, vol, proj = _dev(case, storage=g.STORAGE_F16, filt=filt)
     with g.FdkBatch([(plan, dproj, vol)]) as batch:
         batch.launch()
         plan.check()

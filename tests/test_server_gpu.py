@@ -13,18 +13,19 @@ import pytest
 import gct_b200 as g
 from cases import make_case, oracle_projections
 from conftest import rel_rms
+from oracle import oracle as orc
 
 pytestmark = pytest.mark.gpu
 
 MB = 1 << 20
 
 
-def _request(kind, storage=g.STORAGE_F16, scale=1.0, **kw):
+def _request(kind, storage=g.STORAGE_F16, scale=1.0, filt=g.FILTER_FFT, **kw):
     case = make_case(kind, **kw)
     proj = (oracle_projections(case) * np.float32(scale)).astype(np.float32)
     # the server runs the work-queue kernel; execute() of a plan with the quarter-turn form off runs
     # the same per-column arithmetic, which the 1e-6 comparisons below rely on
-    plan = g.FdkPlan(case.cg, case.vg, opts=g.FdkOptions(storage=storage, symmetry=g.SYMMETRY_OFF))
+    plan = g.FdkPlan(case.cg, case.vg, opts=g.FdkOptions(storage=storage, symmetry=g.SYMMETRY_OFF, filter=filt))
     return case, plan, proj
 
 
@@ -66,6 +67,24 @@ def test_alone_and_in_mix_are_identical():
         assert st["peak_active"] >= 2
         assert st["p50_ms"] > 0 and st["p99_ms"] >= st["p50_ms"]
     for _, p, _ in others + [(a_case, a_plan, a_proj)]:
+        p.close()
+
+
+def test_toeplitz_filter_requests():
+    # requests whose plans filter with the Toeplitz GEMM forms: the server filters their view
+    # chunks one at a time (the FP16 form's row scales are per row, so chunking changes nothing)
+    reqs = [_request("cone_flat", nv=120, filt=g.FILTER_TOEPLITZ_F16X2),
+            _request("cone_cyl", filt=g.FILTER_TOEPLITZ_BF16X4), _request("fan_line")]
+    with g.FdkServer(512 * MB, round_updates=2e5) as srv:
+        outs = [np.empty(c.vg.shape, np.float32) for c, _, _ in reqs]
+        tickets = [srv.submit(p, pr, o) for (c, p, pr), o in zip(reqs, outs)]
+        for tk in tickets:
+            srv.wait(tk)
+        assert srv.info(tickets[0])["rounds"] > 1
+    for (c, p, pr), o in zip(reqs, outs):
+        assert rel_rms(o, _execute(p, c, pr)) <= 1e-5, c.name
+        ref = orc.fdk(c.og, c.ov, pr).reshape(o.shape)
+        assert rel_rms(o, ref) <= 1e-3, c.name
         p.close()
 
 
