@@ -25,7 +25,6 @@ import argparse
 import json
 import math
 import os
-import re
 import subprocess
 import sys
 import tempfile
@@ -51,7 +50,7 @@ CONFIGS = {
                      label="flat-panel cone-beam short scan (pi + fan), 512x512x384, 496 views, 1240x960 at 0.3 mm, "
                            "SOD 785, SDD 1200"),
     "fan256": dict(kind="fan_line", nv=360, nc=512, nr=1, du=1.2, dv=1.0, sod=570.0, sdd=1040.0,
-                   n=(256, 256, 1), vox=1.0, range=2 * math.pi, n_ell=10, i0=None,
+                   n=(256, 256, 1), vox=1.0, range=2 * math.pi, n_ell=10, i0=None, phantom="water_disk",
                    label="fan-beam line detector full scan, 256^2 at 1 mm, 360 views, 512 cells at 1.2 mm, "
                          "SOD 570, SDD 1040"),
 }
@@ -73,6 +72,9 @@ BATCH48_LABEL = ("48 uneven reconstructions in one persistent launch: 24 x 2D pa
 SERVE_LABEL = ("Poisson arrivals, mix 70/25/5: 2D fan 512^2 x 720 views / cylindrical cone 512x512x64 x 1152 "
                "views / flat cone 512^3 x 720 views, 80 GB budget, mixed precision")
 EXTRA_CONFIGS = ["batch48", "serve"]
+
+# The headline metric, identical on both arms (the GPU arm and --impl reference).
+METRIC = "FDK backprojection GUPS & recons/s, mixed-precision vs plain FP32 at stated FP64 error"
 
 
 def parse_args():
@@ -96,6 +98,9 @@ def parse_args():
     ap.add_argument("--no-error", action="store_true", help="skip the FP64 oracle error check")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-path", choices=["mixed", "fp32"], default=None,
+                    help="profiling run: build and time only this path's plan (a smaller device footprint for "
+                         "ncu captures) and print its stage times instead of the benchmark line")
     return ap.parse_args()
 
 
@@ -125,8 +130,32 @@ def make_geometry(cfg):
     return cg, vg
 
 
+# Water disk of the fan-beam workload: radius 120 mm (the configuration's "120 mm water disk" read
+# as a radius, the only reading in which its ellipses of semi-axes up to 100 mm fit inside), water
+# at 0.0193 / mm (about 70 keV).
+WATER_DISK_RADIUS_MM = 120.0
+WATER_MU_PER_MM = 0.0193
+
+
+def water_disk_ellipses(n_ell, seed):
+    """Seeded 2D phantom: a water disk plus n_ell ellipses with semi-axes U[5, 100] mm, added
+    attenuation U[0.01, 0.05] / mm and random rotation, each inside the disk."""
+    rs = np.random.RandomState(seed)
+    R = WATER_DISK_RADIUS_MM
+    ell = [(0.0, 0.0, 0.0, R, R, 1.0, 0.0, WATER_MU_PER_MM)]
+    for _ in range(n_ell):
+        a, b = rs.uniform(5.0, 100.0, size=2)
+        room = max(R - max(a, b), 0.0)
+        r, t = room * math.sqrt(rs.uniform()), rs.uniform(0, 2 * math.pi)
+        ell.append((r * math.cos(t), r * math.sin(t), 0.0, a, b, 1.0, rs.uniform(0, math.pi), rs.uniform(0.01, 0.05)))
+    return ell
+
+
 def make_ellipsoids(cfg, seed):
-    """Seeded phantom: a water-like body plus random inner ellipsoids (mm, 1/mm)."""
+    """Seeded phantom (mm, 1/mm): the water disk with ellipses for the fan-beam workload, else a
+    water-like body plus random inner ellipsoids."""
+    if cfg.get("phantom") == "water_disk":
+        return water_disk_ellipses(cfg["n_ell"], seed)
     rs = np.random.RandomState(seed)
     nx, ny, nz = cfg["n"]
     half = 0.5 * cfg["vox"] * min(nx, ny)
@@ -167,23 +196,36 @@ def sample_rows(nr: int) -> tuple:
     return lo, min(nr, lo + 16)
 
 
+def oracle_geometry(cfg, row_lo: int = 0, row_hi: int | None = None):
+    """The workload's geometry built by the FP64 oracle's own view factory (no gct_b200), with the
+    detector cut to rows [row_lo, row_hi) (a shifted row centre; identical for voxels whose
+    projections stay inside those rows)."""
+    from oracle import oracle as orc
+    nv, nc, nr = cfg["nv"], cfg["nc"], cfg["nr"]
+    rng = cfg["range"]
+    if rng is None:  # short scan: pi + full fan angle
+        rng = math.pi + 2.0 * math.atan(nc * cfg["du"] / 2.0 / cfg["sdd"])
+    kind = orc.KIND[cfg["kind"]]
+    row_hi = nr if row_hi is None else row_hi
+    views = orc.make_views(kind, nv, (nc - 1) / 2.0, (nr - 1) / 2.0 - row_lo, cfg["sdd"], cfg["sod"], 1, 0.0,
+                           rng / nv)
+    if kind >= 3:
+        return orc.Geometry(kind, nc, cfg["du"], views, row_hi - row_lo, cfg["dv"])
+    return orc.Geometry(kind, nc, cfg["du"], views)
+
+
 def oracle_sample(cfg, seed, proj_rows=None):
     """Bounded CPU sample: FP64 oracle FDK of the two central z-slices (all x, y) over all views.
 
     The detector is cut to the rows those slices project onto (geometry with a shifted row
     centre, identical for these voxels). Projections are the given device rows, or generated by
-    the FP64 oracle phantom with numpy Poisson noise when None."""
+    the FP64 oracle phantom with numpy Poisson noise when None. Uses the oracle alone."""
     from oracle import oracle as orc
-    import gct_b200 as g
-    cg, _ = make_geometry(cfg)
     nx, ny, nz = cfg["n"]
     k0 = nz // 2 - 1
-    r_lo, r_hi = sample_rows(cg.num_rows)
-    views = cg.views.copy()
-    if cg.is_3d:
-        views["det_col_center"] -= r_lo
-    og = orc.Geometry(int(cg.kind), cg.num_cols, cg.det_geom()[0].sampling_width, views,
-                      (r_hi - r_lo) if cg.is_3d else 1, cg.det_geom()[1].sampling_width if cg.is_3d else 1.0)
+    is3d = orc.KIND[cfg["kind"]] >= 3
+    r_lo, r_hi = sample_rows(cfg["nr"]) if is3d else (0, 1)
+    og = oracle_geometry(cfg, r_lo, r_hi)
     if proj_rows is None:
         p = orc.phantom(og, np.array(make_ellipsoids(cfg, seed)))
         if cfg["i0"]:
@@ -200,9 +242,10 @@ def oracle_sample(cfg, seed, proj_rows=None):
     t = time.perf_counter()
     orc.fdk(og, ov, proj_rows, voxels=vox, use_fft=True, threads=threads)
     dt = time.perf_counter() - t
-    updates = len(vox) * cg.num_views
-    sample = (f"FP64 oracle FDK of {nslab} central z-slice(s) ({nx}x{ny}x{nslab} voxels) over all {cg.num_views} "
-              f"views, detector rows {r_lo}-{r_hi - 1} (the rows those slices touch), {threads} threads")
+    updates = len(vox) * og.nv
+    sample = (f"FP64 oracle FDK of {nslab} central z-slice(s) ({nx}x{ny}x{nslab} voxels) over all {og.nv} "
+              f"views" + (f", detector rows {r_lo}-{r_hi - 1} (the rows those slices touch)" if is3d else "")
+              + f", {threads} threads")
     return updates / dt / 1e9, threads, sample, (r_lo, r_hi)
 
 
@@ -220,7 +263,7 @@ def run_reference(args, cfg, rank):
     value = float(np.median(vals))
     nx, ny, nz = cfg["n"]
     line = {
-        "impl": "reference", "metric": "FDK backprojection GUPS (voxel x view updates / s)", "value": value,
+        "impl": "reference", "metric": METRIC, "value": value,
         "unit": "GUPS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * wall / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -283,13 +326,53 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(name: str):
-    """DRAM bytes per launch recorded from an ncu capture summary under profiles/ (or None)."""
-    p = REPO / "profiles" / name
-    if not p.exists():
-        return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
-    return float(m.group(1)) if m else None
+# DRAM bytes per voxel-view update of the backprojectors, from ncu captures (dram__bytes_read.sum +
+# dram__bytes_write.sum of one launch on the cone256 profiling case, divided by its updates). These
+# are recorded figures, not measured by this run; the summary file names the command.
+NCU_DRAM_BYTES_PER_UPDATE = {
+    "bp_sym_kernel f16": (0.55, "profiles/backproject_sym_cone512_f16.md"),
+}
+
+
+def rooflines(cfg, updates, mixed, fp32, quarter, hbm, peak_kind, sm_mhz, num_sms, workload):
+    """Roofline entries of the timed kernels.
+
+    Backprojectors: the four bilinear taps of an update (8 B in FP16 quads, 16 B in FP32 quads)
+    come through the SM's L1 data path from L1 and L2 (each quad is reused along rays), so the
+    bound is that path, 128 B per clock per SM (nominal), not HBM; their compulsory HBM bytes
+    (filtered stack read once, volume written once) are reported beside it.
+    FFT filter: HBM-bound; algorithmic bytes 4 B read per detector pixel plus the padded quads
+    written (16 B FP32). All achieved figures are per-launch bytes over the CUDA-event time of the
+    stage on the launching stream."""
+    nx, ny, nz = cfg["n"]
+    nv, nc, nr = cfg["nv"], cfg["nc"], cfg["nr"]
+    l1_peak = 128.0 * num_sms * sm_mhz * 1e6 / 1e9
+    vox_bytes = 4.0 * nx * ny * nz
+    quads = float(nv) * (nr + 4) * (nc + 4)  # padded quad grid per view
+    out = {}
+    for name, res, b_upd, kern in (("backproject_mixed", mixed, 8,
+                                    "bp_sym_kernel (quarter-turn partners, FP16 quads)" if quarter
+                                    else "bp_kernel (FP16 quads)"),
+                                   ("backproject_fp32", fp32, 16, "bp_kernel (FP32 quads)")):
+        t = res["bp_ms"] / 1000.0
+        ach = updates * b_upd / t / 1e9
+        comp = quads * b_upd + vox_bytes
+        e = {"bound": "l1", "kernel": kern, "achieved": ach, "peak": l1_peak, "unit": "GB/s",
+             "frac": ach / l1_peak, "peak_source": "nominal 128 B/clk per SM x SMs x median SM clock under load",
+             "algorithmic_bytes_per_update": b_upd, "traffic": None,
+             "hbm_compulsory": {"bytes": comp, "achieved": comp / t / 1e9, "peak": hbm, "unit": "GB/s",
+                                "frac": comp / t / 1e9 / hbm, "peak_source": peak_kind}}
+        key = "bp_sym_kernel f16" if (name == "backproject_mixed" and quarter) else None
+        if key in NCU_DRAM_BYTES_PER_UPDATE and workload in ("cone512", "cone256"):
+            per, src = NCU_DRAM_BYTES_PER_UPDATE[key]
+            e["traffic_ncu"] = {"bytes_per_launch": per * updates, "bytes_per_update": per, "source": src}
+        out[name] = e
+    t = fp32["filt_ms"] / 1000.0
+    fb = float(nv) * nr * nc * 4 + quads * 16
+    out["filter_fft_fp32"] = {"bound": "hbm", "kernel": "filter_fft_kernel (FP32 quads)", "achieved": fb / t / 1e9,
+                              "peak": hbm, "unit": "GB/s", "frac": fb / t / 1e9 / hbm, "peak_source": peak_kind,
+                              "algorithmic_bytes": fb, "traffic": None}
+    return out
 
 
 def sample_voxels(cfg, seed):
@@ -384,12 +467,21 @@ def run_gct(args, cfg, rank, world, local_rank):
     mixed_filter = {"gemm16": g.FILTER_TOEPLITZ_F16X2, "gemm4": g.FILTER_TOEPLITZ_BF16X4,
                     "gemm3": g.FILTER_TOEPLITZ_BF16X3, "fft": g.FILTER_FFT}[args.mixed_filter]
     sym = {"auto": g.SYMMETRY_AUTO, "off": g.SYMMETRY_OFF, "on": g.SYMMETRY_ON}[args.symmetry]
-    plans = {
-        "mixed": g.FdkPlan(cg, vg, opts=g.FdkOptions(filter=mixed_filter, storage=g.STORAGE_F16,
-                                                     z_per_thread=args.zpt, symmetry=sym)),
-        "fp32": g.FdkPlan(cg, vg, opts=g.FdkOptions(filter=g.FILTER_FFT, storage=g.STORAGE_F32,
-                                                    z_per_thread=args.zpt, symmetry=sym)),
-    }
+    opts = {"mixed": g.FdkOptions(filter=mixed_filter, storage=g.STORAGE_F16, z_per_thread=args.zpt, symmetry=sym),
+            "fp32": g.FdkOptions(filter=g.FILTER_FFT, storage=g.STORAGE_F32, z_per_thread=args.zpt, symmetry=sym)}
+    if args.profile_path:
+        plan = g.FdkPlan(cg, vg, opts=opts[args.profile_path])
+        vol = torch.empty(vg.shape, dtype=torch.float32, device=device)
+        total, filt_ms, bp_ms = time_plan(plan, proj, vol, args.steps, args.warmup, stream, dist)
+        plan.check()
+        if rank == 0:
+            print(json.dumps({"profile_path": args.profile_path, "workload": args.config, "steps": args.steps,
+                              "ms_per_step": 1000.0 * total / args.steps, "stages_ms": {"filter": filt_ms,
+                                                                                         "backproject": bp_ms},
+                              "quarter_turn": plan.quarter_turn}), flush=True)
+        plan.close()
+        return
+    plans = {k: g.FdkPlan(cg, vg, opts=o) for k, o in opts.items()}
     mixed_quarter_turn = plans["mixed"].quarter_turn
     vols = {k: torch.empty(vg.shape, dtype=torch.float32, device=device) for k in plans}
     for k, p in plans.items():
@@ -452,21 +544,17 @@ def run_gct(args, cfg, rank, world, local_rank):
         return
     hbm, peak_kind = measured_peaks()
     mixed = results["mixed"]
-    bytes_per_update = 8  # four FP16 bilinear taps
-    achieved = updates * bytes_per_update / (mixed["bp_ms"] / 1000.0) / 1e9
-    quarter = mixed_quarter_turn
-    bp_label = ("backproject, quarter-turn partners (FP16 quads, bp_sym_kernel)" if quarter
-                else "backproject (FP16 quads, bp_kernel)")
-    traffic = profiled_traffic(f"backproject_{'sym_' if quarter else ''}{args.config}_f16.md")
-    sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
-    l1_peak = 128 * torch.cuda.get_device_properties(local_rank).multi_processor_count * sm_mhz * 1e6 / 1e9
+    rl = rooflines(cfg, updates, mixed, results["fp32"], mixed_quarter_turn, hbm, peak_kind,
+                   (clocks or {}).get("sm_mhz") or 1965.0,
+                   torch.cuda.get_device_properties(local_rank).multi_processor_count, args.config)
     line = {
-        "metric": "FDK backprojection GUPS (voxel x view updates / s), mixed precision", "value": mixed["gups"],
+        "metric": METRIC, "value": mixed["gups"], "precision": "mixed (FP16 filtered storage, FP32 accumulation)",
         "unit": "GUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * mixed["total"] / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32-accumulate/f16-storage", "data": "synthetic",
         "config": {"workload": args.config, "description": cfg["label"], "volume": list(cfg["n"]),
-                   "views": cfg["nv"], "detector": [cfg["nc"], cfg["nr"]], "phantom": f"{cfg['n_ell']} seeded ellipsoids",
+                   "views": cfg["nv"], "detector": [cfg["nc"], cfg["nr"]], "phantom": (f"{cfg['n_ell']} seeded ellipses in a {WATER_DISK_RADIUS_MM:g} mm radius water disk"
+                               if cfg.get("phantom") == "water_disk" else f"{cfg['n_ell']} seeded ellipsoids"),
                    "noise": f"Poisson I0={cfg['i0']:g}" if cfg["i0"] else "none", "l2": "inputs larger than L2, no flush",
                    "parallelism": f"replicas x{world}"},
         "recons_per_s": world * args.steps / mixed["total"],
@@ -477,13 +565,8 @@ def run_gct(args, cfg, rank, world, local_rank):
                  "stages_ms": {"filter": results["fp32"]["filt_ms"], "backproject": results["fp32"]["bp_ms"]}},
         "speedup_mixed_vs_fp32": mixed["gups"] / results["fp32"]["gups"],
         "error_vs_fp64_oracle": ({"voxels": nsamp, **errors} if errors else None),
-        "roofline": {"bound": "hbm", "kernel": bp_label, "achieved": achieved, "peak": hbm,
-                     "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_update": bytes_per_update,
-                     "traffic": traffic,
-                     # the taps come through the SM's L1 data path, which bounds this kernel
-                     "l1_data_path": {"achieved": achieved, "peak": l1_peak, "unit": "GB/s", "frac": achieved / l1_peak,
-                                      "peak_source": "nominal 128 B/clk per SM x SMs x median SM clock under load"}},
+        "roofline": rl["backproject_mixed"],
+        "rooflines": {k: v for k, v in rl.items() if k != "backproject_mixed"},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "clocks": clocks,

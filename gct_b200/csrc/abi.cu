@@ -670,6 +670,11 @@ struct PlanHolder {
 
 }  // namespace
 
+namespace {
+// Device address of the allocation-free path's scratch array on `dev` (defined below).
+unsigned char *noalloc_scratch(int dev);
+}  // namespace
+
 extern "C" {
 
 int32_t gct_abi_version(void) { return GCT_FDK_ABI_VERSION; }
@@ -889,6 +894,10 @@ gct_status gct_fdk_plan_create(const gct_ct_geom *geom, const gct_vol_geom *vol,
         PlanHolder h;
         h.p = new gct_fdk_plan();
         build_plan(h.p, geom, vol, filt, opts);
+        // The allocation-free path's scratch array sits in this file's module, which the CUDA
+        // runtime loads lazily: looking its address up here commits it on the plan's device at
+        // plan creation, so gct_fdk_execute_noalloc never loads it.
+        noalloc_scratch(h.p->device);
         *out = h.p;
         h.p = nullptr;
     });

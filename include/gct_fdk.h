@@ -368,11 +368,15 @@ gct_status gct_fdk_execute_host_budget(gct_fdk_plan *plan, const float *proj_hos
  * The filtered projections go through a fixed scratch array of GCT_NOALLOC_SCRATCH_BYTES
  * (64 MiB) that the library holds on every device that loads it, until the process exits; the
  * views are processed in chunks that fit it. A geometry whose single view needs more than that
- * is rejected with GCT_ERR_BUDGET. The first call on a device looks up the scratch address
- * (cudaGetSymbolAddress) with that device current; make that first call before any stream
- * capture. All calls share the one scratch array: calls whose GPU work overlaps (other streams,
- * other threads, other plans) race on it and must be serialised by the caller. Nothing in it
- * needs to start at zero; each call overwrites what it reads. */
+ * is rejected with GCT_ERR_BUDGET. gct_fdk_plan_create looks up the scratch address
+ * (cudaGetSymbolAddress) on the plan's device; the CUDA runtime loads the module that holds the
+ * array lazily, so its 64 MiB are committed then, at plan creation, and never inside this call.
+ * Kernel code is loaded by the CUDA driver at a kernel's first launch (lazy module loading, the
+ * default since CUDA 12.2): a caller that must see no device allocation at all after start-up
+ * makes one call at start-up, or sets CUDA_MODULE_LOADING=EAGER. All calls share the one scratch
+ * array: calls whose GPU work overlaps (other streams, other threads, other plans) race on it and
+ * must be serialised by the caller. Nothing in it needs to start at zero; each call overwrites
+ * what it reads. Plans with the quarter-turn form run the plain backprojector on this path. */
 #define GCT_NOALLOC_SCRATCH_BYTES (64ull << 20)
 gct_status gct_fdk_execute_noalloc(gct_fdk_plan *plan, const float *proj_dev, float *vol_dev,
                                    void *stream);

@@ -17,12 +17,19 @@
 # by a kernel). The Eigen-dependent sources (geom_math.cpp, eigen_utils.cpp, projection_matrix.cpp,
 # proj_geom_cb_factory.cpp) are not compiled; ref_fdk_main.cu defines the two functions of theirs
 # the FDK links against.
+#
+# The reference tree is GCT_REFERENCE_DIR, else the read-only checkout this recipe was written for.
+# With --if-present the recipe exits 0 without building when that tree is absent (a machine that
+# only runs the prebuilt files).
 set -euo pipefail
 REF="${GCT_REFERENCE_DIR:-/root/reference}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 OUT="$HERE/_ref"
 if [ ! -d "$REF/src" ]; then
-    echo "build_ref.sh: reference tree not found at $REF" >&2
+    if [ "${1:-}" = "--if-present" ]; then
+        exit 0
+    fi
+    echo "build_ref.sh: reference tree not found at $REF (set GCT_REFERENCE_DIR)" >&2
     exit 1
 fi
 mkdir -p "$OUT"

@@ -717,58 +717,68 @@ double or_proj_mapping(const or_geom *g, unsigned v, const double *X, double *u,
 
 /* ---- analytic phantom --------------------------------------------------------------------- */
 
-/* ellipsoids: 8 doubles each (cx, cy, cz, ax, ay, az, phi, mu). out [nv][nr][nc]. */
-void or_phantom(const or_geom *g, const double *ell, unsigned ne, double *out)
+/* Ray of detector pixel (v, r, c): origin o and (unnormalised) direction d, in the geometry's
+ * own convention (the inverse of projMapping + DCSToPCS, src/cuda/geom/coord_trans_proj.cuh:
+ * 142-345): parallel kinds start on the detector line through the isocentre, the others at the
+ * source and pass through the pixel. */
+static void pixel_ray(const or_geom *g, unsigned v, unsigned r, unsigned c, double *o, double *d)
 {
     const int k = g->kind;
+    const or_view *pv = &g->views[v];
+    const double u = ((double)c - pv->det_row_center) * g->du;
+    const double t = is2d(k) ? ((double)r - pv->det_col_center) * g->dv : 0.0;
+    for (int i = 0; i < 3; ++i) o[i] = d[i] = 0.0;
+    if (is_parallel(k)) {
+        const double th = pv->rot_ang;
+        o[0] = -sin(th) * u;
+        o[1] = cos(th) * u;
+        o[2] = k == K_PAR2 ? -t : k == K_REBIN ? -t * pv->src_iso_dist / pv->src_det_dist : 0.0;
+        d[0] = cos(th);
+        d[1] = sin(th);
+        return;
+    }
+    const int fan = !is2d(k);
+    double S[3] = {pv->src_pos[0], pv->src_pos[1], fan ? 0.0 : pv->src_pos[2]};
+    double eu[3] = {pv->det_row_dir[0], pv->det_row_dir[1], fan ? 0.0 : pv->det_row_dir[2]};
+    double ev[3] = {0, 0, 0}, ew[3];
+    if (k == K_FLAT || k == K_CYL)
+        for (int i = 0; i < 3; ++i) ev[i] = pv->det_col_dir[i];
+    if (k == K_LINE) {
+        ew[0] = -eu[1];
+        ew[1] = eu[0];
+        ew[2] = 0.0;
+    } else if (k == K_FLAT) {
+        ew[0] = eu[1] * ev[2] - eu[2] * ev[1];
+        ew[1] = eu[2] * ev[0] - eu[0] * ev[2];
+        ew[2] = eu[0] * ev[1] - eu[1] * ev[0];
+    } else {
+        ew[0] = pv->iso_ray_dir[0];
+        ew[1] = pv->iso_ray_dir[1];
+        ew[2] = fan ? 0.0 : pv->iso_ray_dir[2];
+    }
+    for (int i = 0; i < 3; ++i) o[i] = S[i];
+    if (k == K_LINE || k == K_FLAT) {
+        for (int i = 0; i < 3; ++i) d[i] = pv->src_det_dist * ew[i] + u * eu[i] + t * ev[i];
+    } else {
+        for (int i = 0; i < 3; ++i) d[i] = cos(u) * ew[i] + sin(u) * eu[i] + (t / pv->src_det_dist) * ev[i];
+    }
+}
+
+/* ellipsoids: 8 doubles each (cx, cy, cz, ax, ay, az, phi, mu). out [nv][nr][nc]. 1D-detector
+ * kinds integrate the ellipses' cross-sections in the plane z = 0 (planar rays). */
+void or_phantom(const or_geom *g, const double *ell, unsigned ne, double *out)
+{
+    const int planar = !is2d(g->kind);
     for (unsigned v = 0; v < g->nv; ++v) {
-        const or_view *pv = &g->views[v];
         for (unsigned r = 0; r < g->nr; ++r) {
             for (unsigned c = 0; c < g->nc; ++c) {
-                const double u = ((double)c - pv->det_row_center) * g->du;
-                const double t = is2d(k) ? ((double)r - pv->det_col_center) * g->dv : 0.0;
-                double o[3] = {0, 0, 0}, d[3] = {0, 0, 0};
-                if (is_parallel(k)) {
-                    const double th = pv->rot_ang;
-                    o[0] = -sin(th) * u;
-                    o[1] = cos(th) * u;
-                    o[2] = k == K_PAR2 ? -t : k == K_REBIN ? -t * pv->src_iso_dist / pv->src_det_dist : 0.0;
-                    d[0] = cos(th);
-                    d[1] = sin(th);
-                } else {
-                    const int fan = !is2d(k);
-                    double S[3] = {pv->src_pos[0], pv->src_pos[1], fan ? 0.0 : pv->src_pos[2]};
-                    double eu[3] = {pv->det_row_dir[0], pv->det_row_dir[1], fan ? 0.0 : pv->det_row_dir[2]};
-                    double ev[3] = {0, 0, 0}, ew[3];
-                    if (k == K_FLAT || k == K_CYL)
-                        for (int i = 0; i < 3; ++i) ev[i] = pv->det_col_dir[i];
-                    if (k == K_LINE) {
-                        ew[0] = -eu[1];
-                        ew[1] = eu[0];
-                        ew[2] = 0.0;
-                    } else if (k == K_FLAT) {
-                        ew[0] = eu[1] * ev[2] - eu[2] * ev[1];
-                        ew[1] = eu[2] * ev[0] - eu[0] * ev[2];
-                        ew[2] = eu[0] * ev[1] - eu[1] * ev[0];
-                    } else {
-                        ew[0] = pv->iso_ray_dir[0];
-                        ew[1] = pv->iso_ray_dir[1];
-                        ew[2] = fan ? 0.0 : pv->iso_ray_dir[2];
-                    }
-                    for (int i = 0; i < 3; ++i) o[i] = S[i];
-                    if (k == K_LINE || k == K_FLAT) {
-                        for (int i = 0; i < 3; ++i) d[i] = pv->src_det_dist * ew[i] + u * eu[i] + t * ev[i];
-                    } else {
-                        for (int i = 0; i < 3; ++i)
-                            d[i] = cos(u) * ew[i] + sin(u) * eu[i] + (t / pv->src_det_dist) * ev[i];
-                    }
-                }
+                double o[3], d[3];
+                pixel_ray(g, v, r, c, o, d);
                 const double dn = sqrt(dot3(d, d));
                 double sum = 0.0;
                 for (unsigned e = 0; e < ne; ++e) {
                     const double *E = ell + 8 * e;
                     const double cp = cos(E[6]), sp = sin(E[6]);
-                    const int planar = !is2d(k);
                     const double p0 = o[0] - E[0], p1 = o[1] - E[1], p2 = planar ? 0.0 : o[2] - E[2];
                     const double q2 = planar ? 0.0 : d[2];
                     const double px = (cp * p0 + sp * p1) / E[3], py = (-sp * p0 + cp * p1) / E[4], pz = p2 / E[5];
@@ -777,6 +787,37 @@ void or_phantom(const or_geom *g, const double *ell, unsigned ne, double *out)
                     const double C = px * px + py * py + pz * pz - 1.0;
                     const double disc = B * B - A * C;
                     if (disc > 0.0) sum += E[7] * 2.0 * sqrt(disc) / A * dn;
+                }
+                out[((size_t)v * g->nr + r) * g->nc + c] = sum;
+            }
+        }
+    }
+}
+
+/* Isotropic Gaussian blobs: 5 doubles each (cx, cy, cz, sigma, amplitude), density
+ * a exp(-|x - c|^2 / (2 sigma^2)). The line integral of a blob along a line whose closest
+ * approach to its centre is dist is a sigma sqrt(2 pi) exp(-dist^2 / (2 sigma^2)); 1D-detector
+ * kinds integrate 2D blobs in the plane z = 0 (the same formula with the in-plane distance).
+ * A smooth phantom with exact line integrals, for checking a projector that samples a voxel
+ * grid. out [nv][nr][nc]. */
+void or_gauss_project(const or_geom *g, const double *blobs, unsigned nb, double *out)
+{
+    const int planar = !is2d(g->kind);
+    for (unsigned v = 0; v < g->nv; ++v) {
+        for (unsigned r = 0; r < g->nr; ++r) {
+            for (unsigned c = 0; c < g->nc; ++c) {
+                double o[3], d[3];
+                pixel_ray(g, v, r, c, o, d);
+                if (planar) o[2] = d[2] = 0.0;
+                const double dn = sqrt(dot3(d, d));
+                const double e[3] = {d[0] / dn, d[1] / dn, d[2] / dn};
+                double sum = 0.0;
+                for (unsigned b = 0; b < nb; ++b) {
+                    const double *B = blobs + 5 * b;
+                    const double w[3] = {B[0] - o[0], B[1] - o[1], planar ? 0.0 : B[2] - o[2]};
+                    const double along = dot3(w, e);
+                    const double d2 = fmax(dot3(w, w) - along * along, 0.0);
+                    sum += B[4] * B[3] * sqrt(2.0 * OR_PI) * exp(-d2 / (2.0 * B[3] * B[3]));
                 }
                 out[((size_t)v * g->nr + r) * g->nc + c] = sum;
             }

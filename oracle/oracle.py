@@ -28,6 +28,10 @@ VIEW_DTYPE = np.dtype([
     ("det_row_dir", "<f8", 3), ("det_col_dir", "<f8", 3), ("iso_ray_dir", "<f8", 3),
 ])
 
+# The texture unit's position rule that lerp_bits=8 emulates, named as ref_fdk --bp names it:
+# "q8round" (sample position snapped to the nearest 1/256 texel) or "q8floor" (snapped down).
+TEXTURE_RULE = "q8round"
+
 KIND = {"parallel_1d": 0, "fan_arc": 1, "fan_line": 2, "parallel_2d": 3, "cone_parallel": 4,
         "cone_cyl": 5, "cone_flat": 6}
 
@@ -83,6 +87,8 @@ def load() -> C.CDLL:
             lib.or_proj_mapping.restype = C.c_double
             lib.or_phantom.argtypes = [C.POINTER(_Geom), dp, C.c_uint, dp]
             lib.or_phantom.restype = None
+            lib.or_gauss_project.argtypes = [C.POINTER(_Geom), dp, C.c_uint, dp]
+            lib.or_gauss_project.restype = None
             _lib = lib
     return _lib
 
@@ -270,4 +276,26 @@ def phantom(g: Geometry, ellipsoids) -> np.ndarray:
     e = np.ascontiguousarray(np.asarray(ellipsoids, dtype=np.float64).reshape(-1, 8))
     out = np.zeros(g.shape)
     load().or_phantom(C.byref(g._s), _dp(e), len(e), _dp(out))
+    return out
+
+
+def gauss_project(g: Geometry, blobs) -> np.ndarray:
+    """Exact line integrals of isotropic Gaussian blobs (cx, cy, cz, sigma, amplitude)."""
+    b = np.ascontiguousarray(np.asarray(blobs, dtype=np.float64).reshape(-1, 5))
+    out = np.zeros(g.shape)
+    load().or_gauss_project(C.byref(g._s), _dp(b), len(b), _dp(out))
+    return out
+
+
+def gauss_volume(vol: Volume, blobs, planar: bool = False) -> np.ndarray:
+    """The blobs' density sampled at the voxel centres ([z][y][x]); planar: the z = 0 plane."""
+    b = np.asarray(blobs, dtype=np.float64).reshape(-1, 5)
+    x = vol.mid[0] - (vol.nx - 1) * vol.dx / 2.0 + np.arange(vol.nx) * vol.dx
+    y = vol.mid[1] - (vol.ny - 1) * vol.dy / 2.0 + np.arange(vol.ny) * vol.dy
+    z = np.zeros(1) if planar else vol.mid[2] - (vol.nz - 1) * vol.dz / 2.0 + np.arange(vol.nz) * vol.dz
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    out = np.zeros(Z.shape)
+    for cx, cy, cz, s, a in b:
+        r2 = (X - cx) ** 2 + (Y - cy) ** 2 + (0.0 if planar else (Z - cz) ** 2)
+        out += a * np.exp(-r2 / (2.0 * s * s))
     return out

@@ -82,3 +82,28 @@ def test_spiral_plans_are_not_batched():
         v = torch.zeros(case.vg.shape, device="cuda")
         with pytest.raises(g.GctError, match="spiral"):
             g.FdkBatch([(p, d, v)])
+
+
+def test_spiral_matches_the_reference(tmp_path):
+    """Against the reference's own spiral FDK (oracle/_ref/ref_fdk --spiral: its stage functions in
+    the order of src/cuda/recon/fdk_spiral.cuh:33-94 on a cylindrical detector). The reference
+    samples through the texture unit (1/256-texel positions) and the engine exactly: the whole gap
+    must be the reference's own distance from the FP64 oracle (the texture's quantisation), within
+    the bound measured on the axial cases (1.5e-4)."""
+    import test_reference_gpu as tr
+    if not tr.REF_FDK.exists():
+        pytest.skip("oracle/_ref/ref_fdk not built")
+    case = make_spiral_case("cone_cyl")
+    proj = spiral_projections(case)
+    with _plan(case) as p:
+        got = _execute(p, case, proj)
+    ref = tr.run_reference(case, proj, tmp_path, "--spiral")
+    on = np.array([w is not None for w in orc.spiral_windows(case.og, case.ov)])
+    # the same slices are reconstructed and the same ones left zero
+    assert np.array_equal(np.any(ref != 0, axis=(1, 2)), on)
+    exact = orc.fdk_spiral(case.og, case.ov, proj)
+    e_ref, e_ref_oracle = rel_rms(got[on], ref[on]), rel_rms(ref[on], exact[on])
+    print(f"spiral: engine-ref {e_ref:.2e}  ref-oracle {e_ref_oracle:.2e}  "
+          f"engine-oracle {rel_rms(got[on], exact[on]):.2e}")
+    assert e_ref <= 1.5e-4
+    assert abs(e_ref - e_ref_oracle) <= 0.05 * e_ref_oracle + 2e-6
