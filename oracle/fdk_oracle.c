@@ -22,8 +22,9 @@
  *   final scale          src/cuda/recon/fdk_axial.cuh:196-199
  *   spiral scans         src/cuda/recon/fdk_spiral.cuh:33-94 (no Parker weights: or_filter_np;
  *                        the per-slice view windows are restated in oracle.py)
- * The texture unit's 8-bit fractional lerp weights can be emulated (lerp_bits = 8) to quantify
- * that difference separately from the exact bilinear interpolation (lerp_bits = 0).
+ * The texture unit's linear filter can be emulated (lerp_bits = 8: sample positions and the
+ * bilinear corner weight on a 1/256 grid, as measured through the reference's texture objects)
+ * to quantify that difference separately from the exact bilinear interpolation (lerp_bits = 0).
  */
 #include <math.h>
 #include <pthread.h>
@@ -493,6 +494,18 @@ static double quant(double a, int bits)
     return floor(a * s + 0.5) / s;
 }
 
+/* Bilinear value of texels t00 = T[r][c], t01 = T[r][c+1], t10 = T[r+1][c], t11 = T[r+1][c+1] at
+ * fractions ac (along a row) and ar (across rows). lerp_bits = 0: exact weights. lerp_bits = 8:
+ * the texture unit's linear filter as measured through the reference's own texture objects
+ * (golden vectors tests/golden/tex_probe.npz): both fractions snap to the nearest 1/256 (the
+ * callers snap them), the corner weight ac ar snaps to the nearest 1/256 too, and the other three
+ * weights follow from it so that all four sum to one. A 1D fetch is the case ar = 0. */
+static double bilerp(double t00, double t01, double t10, double t11, double ac, double ar, int lerp_bits)
+{
+    const double w11 = quant(ac * ar, lerp_bits);
+    return (1.0 - ac - ar + w11) * t00 + (ac - w11) * t01 + (ar - w11) * t10 + w11 * t11;
+}
+
 /* bilinear sample of one filtered view at pixel coordinates with border 0 */
 static double sample(const double *(*rowp)(void *, unsigned, long), void *ctx, unsigned v, const or_geom *g,
                      double col, double row, int lerp_bits)
@@ -504,21 +517,38 @@ static double sample(const double *(*rowp)(void *, unsigned, long), void *ctx, u
         const double *p = rowp(ctx, v, 0);
         const double a = (ic >= 0 && ic < (long)g->nc) ? p[ic] : 0.0;
         const double b = (ic + 1 >= 0 && ic + 1 < (long)g->nc) ? p[ic + 1] : 0.0;
-        return (1.0 - ac) * a + ac * b;
+        return bilerp(a, b, 0.0, 0.0, ac, 0.0, lerp_bits);
     }
     const double fr = floor(row);
     const long ir = (long)fr;
     const double ar = quant(row - fr, lerp_bits);
-    double val[2] = {0.0, 0.0};
+    double t[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
     for (int dr = 0; dr < 2; ++dr) {
         const long rr = ir + dr;
         if (rr < 0 || rr >= (long)g->nr) continue;
         const double *p = rowp(ctx, v, rr);
-        const double a = (ic >= 0 && ic < (long)g->nc) ? p[ic] : 0.0;
-        const double b = (ic + 1 >= 0 && ic + 1 < (long)g->nc) ? p[ic + 1] : 0.0;
-        val[dr] = (1.0 - ac) * a + ac * b;
+        t[dr][0] = (ic >= 0 && ic < (long)g->nc) ? p[ic] : 0.0;
+        t[dr][1] = (ic + 1 >= 0 && ic + 1 < (long)g->nc) ? p[ic + 1] : 0.0;
     }
-    return (1.0 - ar) * val[0] + ar * val[1];
+    return bilerp(t[0][0], t[0][1], t[1][0], t[1][1], ac, ar, lerp_bits);
+}
+
+/* The oracle's texture fetch on its own: texels [h][w], texture coordinates (x, y) as passed to
+ * tex2D (texel centres at integer + 0.5; y = 0.5 for a one-row texture), border 0. Lets the
+ * golden probe vectors pin the emulation used by or_fdk / or_backproject. */
+double or_tex_fetch(const double *tex, unsigned w, unsigned h, double x, double y, int lerp_bits)
+{
+    const double px = x - 0.5, py = y - 0.5;
+    const double fx = floor(px), fy = floor(py);
+    const long i = (long)fx, j = (long)fy;
+    const double ac = quant(px - fx, lerp_bits), ar = quant(py - fy, lerp_bits);
+    double t[2][2];
+    for (int dr = 0; dr < 2; ++dr)
+        for (int dc = 0; dc < 2; ++dc) {
+            const long r = j + dr, c = i + dc;
+            t[dr][dc] = (r >= 0 && r < (long)h && c >= 0 && c < (long)w) ? tex[(size_t)r * w + (size_t)c] : 0.0;
+        }
+    return bilerp(t[0][0], t[0][1], t[1][0], t[1][1], ac, ar, lerp_bits);
 }
 
 typedef struct {

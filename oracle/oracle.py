@@ -28,9 +28,9 @@ VIEW_DTYPE = np.dtype([
     ("det_row_dir", "<f8", 3), ("det_col_dir", "<f8", 3), ("iso_ray_dir", "<f8", 3),
 ])
 
-# The texture unit's position rule that lerp_bits=8 emulates, named as ref_fdk --bp names it:
-# "q8round" (sample position snapped to the nearest 1/256 texel) or "q8floor" (snapped down).
-TEXTURE_RULE = "q8round"
+# lerp_bits=8 emulates the texture unit's linear filter as measured through the reference's own
+# texture objects (tests/golden/tex_probe.npz): sample positions snap to the nearest 1/256 texel
+# and the bilinear corner weight a b to the nearest 1/256; ref_fdk --bp texture is the same rule.
 
 KIND = {"parallel_1d": 0, "fan_arc": 1, "fan_line": 2, "parallel_2d": 3, "cone_parallel": 4,
         "cone_cyl": 5, "cone_flat": 6}
@@ -87,6 +87,8 @@ def load() -> C.CDLL:
             lib.or_proj_mapping.restype = C.c_double
             lib.or_phantom.argtypes = [C.POINTER(_Geom), dp, C.c_uint, dp]
             lib.or_phantom.restype = None
+            lib.or_tex_fetch.argtypes = [dp, C.c_uint, C.c_uint, C.c_double, C.c_double, C.c_int]
+            lib.or_tex_fetch.restype = C.c_double
             lib.or_gauss_project.argtypes = [C.POINTER(_Geom), dp, C.c_uint, dp]
             lib.or_gauss_project.restype = None
             _lib = lib
@@ -299,3 +301,12 @@ def gauss_volume(vol: Volume, blobs, planar: bool = False) -> np.ndarray:
         r2 = (X - cx) ** 2 + (Y - cy) ** 2 + (0.0 if planar else (Z - cz) ** 2)
         out += a * np.exp(-r2 / (2.0 * s * s))
     return out
+
+
+def tex_fetch(texels: np.ndarray, xy: np.ndarray, lerp_bits: int = 8) -> np.ndarray:
+    """The oracle's bilinear fetch of texels [h][w] at texture coordinates xy (n x 2, texel
+    centres at integer + 0.5), border 0; lerp_bits=8 is the texture unit's rule."""
+    t = np.ascontiguousarray(texels, dtype=np.float64)
+    h, w = t.shape
+    lib = load()
+    return np.array([lib.or_tex_fetch(_dp(t), w, h, float(x), float(y), lerp_bits) for x, y in np.asarray(xy)])

@@ -14,10 +14,10 @@
 //                                             and view, view by view), except that the texture fetch
 //                                             of backProjKern (back_proj.cuh:16-79) is replaced by a
 //                                             bilinear interpolation of the same filtered view in
-//                                             global memory: MODE exact (FP32 weights), q8round or
-//                                             q8floor (the coordinate snapped to 1/256 of a texel,
-//                                             to nearest or down). This isolates the texture unit's
-//                                             weight quantisation from everything else.
+//                                             global memory: MODE exact (FP32 weights) or texture
+//                                             (the texture unit's 1/256 weight rule, see lerp2).
+//                                             This isolates the texture unit's weight quantisation
+//                                             from everything else.
 //   ref_fdk --texprobe in.bin out.bin         fetches through the reference's own texture objects
 //                                             (NDArrayTexture, nd_array_texture.cuh:33-56, filled by
 //                                             copyDevToDevTexture) at given coordinates. Input: int32
@@ -108,33 +108,35 @@ struct Input {
 
 
 // ---- bilinear interpolation in place of the texture fetch (--bp) ------------------------------
-enum BpMode { kBpExact = 0, kBpQ8Round = 1, kBpQ8Floor = 2 };
+enum BpMode { kBpExact = 0, kBpTexture = 1 };
 
-// Texel-space position of a fetch at coordinate t (the value passed to tex1D / tex2D, which
-// includes the reference's +0.5): the linear filter interpolates between texels floor(t - 0.5)
-// and floor(t - 0.5) + 1. The quantised modes snap that position to 1/256 of a texel.
-__device__ __forceinline__ float texel_pos(float t, int mode)
-{
-    float x = t - 0.5f;
-    if (mode == kBpQ8Round) x = floorf(x * 256.f + 0.5f) * (1.f / 256.f);
-    else if (mode == kBpQ8Floor) x = floorf(x * 256.f) * (1.f / 256.f);
-    return x;
-}
+__device__ __forceinline__ float q256(float v) { return floorf(v * 256.f + 0.5f) * (1.f / 256.f); }
 
 __device__ __forceinline__ float texel(const float *img, int w, int h, int i, int j)
 {
     return (i >= 0 && i < w && j >= 0 && j < h) ? img[static_cast<size_t>(j) * w + i] : 0.f;  // border 0
 }
 
+// Bilinear sample at texture coordinates (tx, ty) (the values passed to tex1D / tex2D, which
+// include the reference's +0.5: the linear filter interpolates between texels floor(t - 0.5) and
+// floor(t - 0.5) + 1). kBpExact: FP32 weights. kBpTexture: the texture unit's rule as measured
+// through the reference's own texture objects (tests/golden/tex_probe.npz): the sample position
+// snaps to the nearest 1/256 of a texel on each axis, and the corner weight a b also snaps to the
+// nearest 1/256, the other three weights being a - w11, b - w11 and 1 - a - b + w11.
 __device__ float lerp2(const float *img, int w, int h, float tx, float ty, int mode)
 {
-    const float x = texel_pos(tx, mode), y = texel_pos(ty, mode);
+    float x = tx - 0.5f, y = ty - 0.5f;
+    if (mode == kBpTexture) {
+        x = q256(x);
+        y = q256(y);
+    }
     const float fx = floorf(x), fy = floorf(y);
     const int i = static_cast<int>(fx), j = static_cast<int>(fy);
     const float a = x - fx, b = y - fy;
-    const float r0 = (1.f - a) * texel(img, w, h, i, j) + a * texel(img, w, h, i + 1, j);
-    const float r1 = (1.f - a) * texel(img, w, h, i, j + 1) + a * texel(img, w, h, i + 1, j + 1);
-    return (1.f - b) * r0 + b * r1;
+    const float w11 = mode == kBpTexture ? q256(a * b) : a * b;
+    const float w01 = a - w11, w10 = b - w11, w00 = 1.f - a - b + w11;
+    return w00 * texel(img, w, h, i, j) + w01 * texel(img, w, h, i + 1, j) + w10 * texel(img, w, h, i, j + 1) +
+           w11 * texel(img, w, h, i + 1, j + 1);
 }
 
 // backProjKern (back_proj.cuh:16-42) with the fetch replaced by lerp2 on the view in memory.
@@ -426,14 +428,14 @@ int main(int argc, char **argv)
                 opt.repeat = std::max(1, std::atoi(argv[++a]));
             } else if (o == "--bp" && a + 1 < argc) {
                 const std::string m = argv[++a];
-                opt.bp_mode = m == "exact" ? kBpExact : m == "q8round" ? kBpQ8Round : m == "q8floor" ? kBpQ8Floor : -2;
+                opt.bp_mode = m == "exact" ? kBpExact : m == "texture" ? kBpTexture : -2;
                 if (opt.bp_mode < 0) throw std::runtime_error("unknown --bp mode " + m);
             } else {
                 throw std::runtime_error("unknown option " + o);
             }
         }
         if (argc - a != 2) {
-            std::fprintf(stderr, "usage: %s [--texprobe | --spiral | --bp exact|q8round|q8floor] [--repeat K] "
+            std::fprintf(stderr, "usage: %s [--texprobe | --spiral | --bp exact|texture] [--repeat K] "
                                  "input.bin output.bin\n", argv[0]);
             return 2;
         }
