@@ -1,8 +1,8 @@
-// Row-batched ramp filter: cosine and Parker weights fused into the load, a Stockham radix-4/2
-// FFT convolution with the ramp spectrum in shared memory, and an epilogue that writes either
-// plain FP32 rows or the padded bilinear-coefficient quads read by the backprojector. Two
-// detector rows share one complex FFT (row a in the real part, row b in the imaginary part): the
-// ramp taps are real, so the two convolutions stay separated.
+// Row-batched ramp filter: cosine and Parker weights fused into the load, an FFT convolution with
+// the ramp spectrum done in registers with radix-16 passes, and an epilogue that writes either
+// plain FP32 rows or the padded bilinear-coefficient quads read by the backprojector. Two detector
+// rows share one complex FFT (row a in the real part, row b in the imaginary part): the ramp taps
+// are real, so the two convolutions stay separated.
 //
 // Replaces runCosWeighting (src/cuda/recon/cos_weighting.cuh:225-263), runParkerWeighting
 // (src/cuda/recon/parker_weighting.cuh:202-230) and RampFilteringFFT::runFiltering
@@ -11,126 +11,305 @@
 // the crop disappears, the shortest alias-free power of two (> 1.5 N) is used, and each row is
 // read once and written once.
 //
-// Work split: one CTA per (view, segment of rows). A CTA walks its rows in order, keeps the
-// previous filtered row in shared memory and writes the quad of row r once rows r and r + 1 are
-// known, so every quad is written whole by one CTA. Each segment filters one extra row (the first
-// row of the next segment) to close its last quad.
+// Transform of length L = 2^LOG2L by T = L / 16 threads, 16 points per thread. Thread t holds
+// x[t + T m], m = 0..15, in registers. The transform is a Stockham decomposition into passes of
+// radix 16 (the last one radix 2^(LOG2L mod 4), or 16): a pass of radix R and span Ns takes, for
+// butterfly j, the inputs x[j + r L / R] (r < R), multiplies input r by W_{R Ns}^{r (j mod Ns)} and
+// writes its R-point DFT to y[(j - j mod Ns) R + (j mod Ns) + k Ns]. Each pass's butterflies run
+// in one thread's registers; passes exchange through one shared-memory buffer (padded by one
+// float2 per 16 so the strided accesses are bank-conflict free). The last pass leaves thread t
+// with X[t + T m] in natural order, which is exactly the input set of the first pass of the next
+// transform: the spectrum product and the inverse transform (a forward transform of the
+// conjugate) follow without an exchange. Per row pair: four exchanges, no twiddle tables (each
+// pass's twiddles are powers of one per-thread base computed at start).
+//
+// Work split: one CTA per (view, segment of quad rows) (or, for one-row detectors, per pair of
+// views). A CTA walks its rows in pairs, keeps the filtered rows of the previous pair in shared
+// memory and writes each quad row whole once its two detector rows are known.
 #include "../../include/gct_fdk.h"
 #include "common.cuh"
 #include "kernels.hpp"
+
+#ifndef GCT_FFT_MINB
+#define GCT_FFT_MINB 4
+#endif
 
 namespace gct {
 namespace {
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2(a.y, -a.x); }  // times -i
 
-// Shared-memory index with one float2 of padding per 16: strided Stockham writes then spread
-// over all banks.
+// Shared-memory index with one float2 of padding per 16 entries.
 __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
 
-// One Stockham stage (Govindaraju et al., SC'08). Butterfly j reads x[j + r L/R], multiplies by
-// the twiddle W_{R Ns}^(r (j mod Ns)) and writes its R-point DFT to
-// y[(j / Ns) Ns R + (j mod Ns) + r Ns]; after all stages the output is in natural order.
-// Twiddles of a stage with span Ns live contiguously at tw[Ns + k], k < Ns.
-// LAST fuses the pointwise product with the spectrum H and the conjugation that turns the next
-// forward FFT into the inverse.
-template <int L, int NT, bool LAST>
-__device__ __forceinline__ void stage_r4(const float2 *src, float2 *dst, const float2 *tw, const float2 *H,
-                                         int Ns, int tid)
+// x times W_16^M = exp(-2 pi i M / 16) for a compile-time M (the exact constants cos(pi/8),
+// sin(pi/8) and sqrt(1/2); multiples of a quarter turn are swaps and negations).
+template <int M>
+__device__ __forceinline__ float2 tw16(float2 x)
 {
-    for (int j = tid; j < L / 4; j += NT) {
-        const int k = j & (Ns - 1);
-        float2 v0 = src[pad(j)], v1 = src[pad(j + L / 4)], v2 = src[pad(j + L / 2)], v3 = src[pad(j + 3 * L / 4)];
-        if (Ns > 1) {
-            const float2 w1 = tw[Ns + k];
-            const float2 w2 = cmul(w1, w1);
-            v1 = cmul(v1, w1);
-            v2 = cmul(v2, w2);
-            v3 = cmul(v3, cmul(w2, w1));
-        }
-        const float2 t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3);
-        const float2 d = csub(v1, v3);
-        const float2 t3 = make_float2(d.y, -d.x);  // -i * (v1 - v3)
-        const int idx = (j - k) * 4 + k;
-        float2 y[4] = {cadd(t0, t2), cadd(t1, t3), csub(t0, t2), csub(t1, t3)};
+    constexpr int m = ((M % 16) + 16) % 16;
+    constexpr float c1 = 0.923879532511286756f, s1 = 0.382683432365089772f, h = 0.707106781186547524f;
+    if constexpr (m == 0) return x;
+    else if constexpr (m == 4) return mul_mi(x);
+    else if constexpr (m == 8) return make_float2(-x.x, -x.y);
+    else if constexpr (m == 12) return make_float2(-x.y, x.x);
+    else if constexpr (m == 2) return make_float2(h * (x.x + x.y), h * (x.y - x.x));
+    else if constexpr (m == 6) return make_float2(h * (x.y - x.x), -h * (x.x + x.y));
+    else if constexpr (m == 10) return make_float2(-h * (x.x + x.y), h * (x.x - x.y));
+    else if constexpr (m == 14) return make_float2(h * (x.x - x.y), h * (x.x + x.y));
+    else {
+        // W = cos(2 pi m / 16) - i sin(2 pi m / 16)
+        constexpr float cs = (m == 1 || m == 15) ? c1 : (m == 3 || m == 13) ? s1 : (m == 5 || m == 11) ? -s1 : -c1;
+        constexpr float sn = (m == 1 || m == 7) ? s1 : (m == 3 || m == 5) ? c1 : (m == 9 || m == 15) ? -s1 : -c1;
+        return make_float2(fmaf(x.x, cs, x.y * sn), fmaf(x.y, cs, -x.x * sn));
+    }
+}
+
+// In-place DFTs with natural-order output.
+__device__ __forceinline__ void dft2(float2 *x)
+{
+    const float2 a = x[0], b = x[1];
+    x[0] = cadd(a, b);
+    x[1] = csub(a, b);
+}
+
+__device__ __forceinline__ void dft4v(float2 a0, float2 a1, float2 a2, float2 a3, float2 &y0, float2 &y1, float2 &y2,
+                                      float2 &y3)
+{
+    const float2 t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = mul_mi(csub(a1, a3));
+    y0 = cadd(t0, t2);
+    y1 = cadd(t1, t3);
+    y2 = csub(t0, t2);
+    y3 = csub(t1, t3);
+}
+
+__device__ __forceinline__ void dft4(float2 *x) { dft4v(x[0], x[1], x[2], x[3], x[0], x[1], x[2], x[3]); }
+
+// 8 = 4 x 2: inner DFT4 over x[2 n1 + n2], twiddle W_8^(n2 k1), outer DFT2.
+__device__ __forceinline__ void dft8(float2 *x)
+{
+    float2 a0, a1, a2, a3, b0, b1, b2, b3;
+    dft4v(x[0], x[2], x[4], x[6], a0, a1, a2, a3);
+    dft4v(x[1], x[3], x[5], x[7], b0, b1, b2, b3);
+    b1 = tw16<2>(b1);
+    b2 = tw16<4>(b2);
+    b3 = tw16<6>(b3);
+    x[0] = cadd(a0, b0);
+    x[4] = csub(a0, b0);
+    x[1] = cadd(a1, b1);
+    x[5] = csub(a1, b1);
+    x[2] = cadd(a2, b2);
+    x[6] = csub(a2, b2);
+    x[3] = cadd(a3, b3);
+    x[7] = csub(a3, b3);
+}
+
+// 16 = 4 x 4: inner DFT4 over x[4 n1 + n2], twiddle W_16^(n2 k1), outer DFT4 over n2.
+__device__ __forceinline__ void dft16(float2 *x)
+{
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            float2 o = y[r];
-            if (LAST) {
-                o = cmul(o, __ldg(H + idx + r * Ns));
-                o.y = -o.y;
+    for (int n2 = 0; n2 < 4; ++n2) dft4v(x[n2], x[4 + n2], x[8 + n2], x[12 + n2], x[n2], x[4 + n2], x[8 + n2], x[12 + n2]);
+    // x[n2 + 4 k1] now holds inner output k1 of column n2
+    x[5] = tw16<1>(x[5]);
+    x[9] = tw16<2>(x[9]);
+    x[13] = tw16<3>(x[13]);
+    x[6] = tw16<2>(x[6]);
+    x[10] = tw16<4>(x[10]);
+    x[14] = tw16<6>(x[14]);
+    x[7] = tw16<3>(x[7]);
+    x[11] = tw16<6>(x[11]);
+    x[15] = tw16<9>(x[15]);
+    float2 y[16];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1)
+        dft4v(x[4 * k1], x[4 * k1 + 1], x[4 * k1 + 2], x[4 * k1 + 3], y[k1], y[k1 + 4], y[k1 + 8], y[k1 + 12]);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) x[k] = y[k];
+}
+
+// DFT16 of x whose entries 8..15 are zero: X[2k] = DFT8(x)[k], X[2k + 1] = DFT8(x[n] W_16^n)[k].
+__device__ __forceinline__ void dft16_half(float2 *x)
+{
+    float2 e[8], o[8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) e[n] = x[n];
+    o[0] = x[0];
+    o[1] = tw16<1>(x[1]);
+    o[2] = tw16<2>(x[2]);
+    o[3] = tw16<3>(x[3]);
+    o[4] = tw16<4>(x[4]);
+    o[5] = tw16<5>(x[5]);
+    o[6] = tw16<6>(x[6]);
+    o[7] = tw16<7>(x[7]);
+    dft8(e);
+    dft8(o);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        x[2 * k] = e[k];
+        x[2 * k + 1] = o[k];
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void dft(float2 *x)
+{
+    if constexpr (R == 16) dft16(x);
+    else if constexpr (R == 8) dft8(x);
+    else if constexpr (R == 4) dft4(x);
+    else dft2(x);
+}
+
+// x[r] *= w^r, r = 1..R-1 (powers by squaring and products: at most five roundings deep).
+template <int R>
+__device__ __forceinline__ void twiddle(float2 *x, float2 w)
+{
+    if constexpr (R >= 2) x[1] = cmul(x[1], w);
+    if constexpr (R >= 4) {
+        const float2 w2 = cmul(w, w), w3 = cmul(w2, w);
+        x[2] = cmul(x[2], w2);
+        x[3] = cmul(x[3], w3);
+        if constexpr (R >= 8) {
+            const float2 w4 = cmul(w2, w2), w5 = cmul(w4, w), w6 = cmul(w4, w2), w7 = cmul(w4, w3);
+            x[4] = cmul(x[4], w4);
+            x[5] = cmul(x[5], w5);
+            x[6] = cmul(x[6], w6);
+            x[7] = cmul(x[7], w7);
+            if constexpr (R >= 16) {
+                const float2 w8 = cmul(w4, w4);
+                x[8] = cmul(x[8], w8);
+                x[9] = cmul(x[9], cmul(w8, w));
+                x[10] = cmul(x[10], cmul(w8, w2));
+                x[11] = cmul(x[11], cmul(w8, w3));
+                x[12] = cmul(x[12], cmul(w8, w4));
+                x[13] = cmul(x[13], cmul(w8, w5));
+                x[14] = cmul(x[14], cmul(w8, w6));
+                x[15] = cmul(x[15], cmul(w8, w7));
             }
-            dst[pad(idx + r * Ns)] = o;
         }
     }
 }
 
-template <int L, int NT, bool LAST>
-__device__ __forceinline__ void stage_r2(const float2 *src, float2 *dst, const float2 *tw, const float2 *H,
-                                         int Ns, int tid)
-{
-    for (int j = tid; j < L / 2; j += NT) {
-        const int k = j & (Ns - 1);
-        float2 v0 = src[pad(j)], v1 = src[pad(j + L / 2)];
-        if (Ns > 1) v1 = cmul(v1, tw[Ns + k]);
-        const int idx = (j - k) * 2 + k;
-        float2 y0 = cadd(v0, v1), y1 = csub(v0, v1);
-        if (LAST) {
-            y0 = cmul(y0, __ldg(H + idx));
-            y0.y = -y0.y;
-            y1 = cmul(y1, __ldg(H + idx + Ns));
-            y1.y = -y1.y;
-        }
-        dst[pad(idx)] = y0;
-        dst[pad(idx + Ns)] = y1;
-    }
-}
+// Pass structure of a transform of length 2^LOG2L.
+template <int LOG2L>
+struct Fft {
+    static constexpr int L = 1 << LOG2L;
+    static constexpr int T = L / 16;                  // threads per transform
+    static constexpr int NPASS = (LOG2L + 3) / 4;
+    static constexpr int RLAST = 1 << (LOG2L - 4 * (NPASS - 1));
+    static constexpr int LP = L + L / 16;             // padded exchange buffer (float2)
+    static constexpr int radix(int p) { return p < NPASS - 1 ? 16 : RLAST; }
+    static constexpr int span(int p) { return 1 << (4 * p); }
+};
 
-// Remaining stages of an L-point FFT whose first radix-4 stage (Ns = 1) is already in `a`.
-// Ping-pongs between a and b; returns the buffer holding the result.
-template <int LOG2L, int NT, bool FUSE_H>
-__device__ __forceinline__ float2 *fft_rest(float2 *a, float2 *b, const float2 *tw, const float2 *H, int tid)
-{
-    constexpr int L = 1 << LOG2L;
-    constexpr int NR4 = LOG2L / 2;
-    float2 *src = a, *dst = b;
-    int Ns = 4;
+// Per-thread twiddle bases: pass p >= 1 multiplies input r of butterfly 0 by base_p^r with
+// base_p = W_{R Ns}^(t mod Ns); butterfly i of a last pass with several butterflies per thread
+// uses base_p W_16^i (its j = t + i T is below Ns there).
+template <int LOG2L>
+struct Bases {
+    float2 w[Fft<LOG2L>::NPASS];
+    __device__ __forceinline__ void init(int t)
+    {
+        using F = Fft<LOG2L>;
+        w[0] = make_float2(1.f, 0.f);
 #pragma unroll
-    for (int s = 1; s < NR4; ++s) {
-        const bool last = (s == NR4 - 1) && !(LOG2L & 1);
-        if (FUSE_H && last)
-            stage_r4<L, NT, true>(src, dst, tw, H, Ns, tid);
-        else
-            stage_r4<L, NT, false>(src, dst, tw, H, Ns, tid);
-        __syncthreads();
-        float2 *t = src;
-        src = dst;
-        dst = t;
-        Ns *= 4;
+        for (int p = 1; p < F::NPASS; ++p) {
+            const int ns = F::span(p), rn = F::radix(p) * ns;
+            float s, c;
+            // exp(-2 pi i k / (R Ns)) = cos - i sin of pi (2 k / (R Ns)); 2 k / (R Ns) is exact
+            sincospif(2.0f * static_cast<float>(t & (ns - 1)) / static_cast<float>(rn), &s, &c);
+            w[p] = make_float2(c, -s);
+        }
     }
-    if (LOG2L & 1) {
-        if (FUSE_H)
-            stage_r2<L, NT, true>(src, dst, tw, H, Ns, tid);
-        else
-            stage_r2<L, NT, false>(src, dst, tw, H, Ns, tid);
-        __syncthreads();
-        float2 *t = src;
-        src = dst;
-        dst = t;
-    }
-    return src;
+};
+
+// Twiddles and DFT of butterflies I.. of pass P, whose inputs are in x (butterfly-major).
+template <int LOG2L, int P, int I>
+__device__ __forceinline__ void butterflies(float2 (&x)[16], float2 base)
+{
+    constexpr int R = Fft<LOG2L>::radix(P);
+    twiddle<R>(x + I * R, tw16<I>(base));  // butterfly I's base: base W_16^I
+    dft<R>(x + I * R);
+    if constexpr (I + 1 < 16 / R) butterflies<LOG2L, P, I + 1>(x, base);
 }
 
-// First radix-4 stage of the inverse transform (input already conjugated in smem).
-template <int L, int NT>
-__device__ __forceinline__ void first_stage_smem(const float2 *src, float2 *dst, int tid)
+// One pass p >= 1: read inputs from the exchange buffer, twiddle, DFT. x is butterfly-major:
+// x[i R + r] = input r of butterfly i, then output k at x[i R + k].
+template <int LOG2L, int P>
+__device__ __forceinline__ void pass_in(const float2 *buf, float2 (&x)[16], int t, float2 base)
 {
-    stage_r4<L, NT, false>(src, dst, nullptr, nullptr, 1, tid);
+    using F = Fft<LOG2L>;
+    constexpr int R = F::radix(P), B = 16 / R, L = F::L, T = F::T;
+#pragma unroll
+    for (int i = 0; i < B; ++i)
+#pragma unroll
+        for (int r = 0; r < R; ++r) x[i * R + r] = buf[pad(t + i * T + r * (L / R))];
+    butterflies<LOG2L, P, 0>(x, base);
+}
+
+// Writes the outputs of pass p (not the last) to the exchange buffer at their Stockham places.
+template <int LOG2L, int P>
+__device__ __forceinline__ void pass_out(float2 *buf, const float2 (&x)[16], int t)
+{
+    using F = Fft<LOG2L>;
+    constexpr int R = F::radix(P), B = 16 / R, T = F::T, NS = F::span(P);
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        const int j = t + i * T;
+        const int kk = j & (NS - 1);
+        const int o = (j - kk) * R + kk;
+#pragma unroll
+        for (int k = 0; k < R; ++k) buf[pad(o + k * NS)] = x[i * R + k];
+    }
+}
+
+// Natural order after the last pass: butterfly i's output k is X[t + T (i + k B)].
+template <int LOG2L>
+__device__ __forceinline__ void last_to_natural(float2 (&x)[16])
+{
+    constexpr int R = Fft<LOG2L>::RLAST, B = 16 / R;
+    if constexpr (B > 1) {
+        float2 y[16];
+#pragma unroll
+        for (int i = 0; i < B; ++i)
+#pragma unroll
+            for (int k = 0; k < R; ++k) y[i + k * B] = x[i * R + k];
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = y[m];
+    }
+}
+
+// Full transform of x (natural order in: x[m] = v[t + T m]; natural order out). The first pass
+// runs on the registers; HALF: x[8..15] are zero on entry.
+template <int LOG2L, bool HALF>
+__device__ __forceinline__ void transform(float2 (&x)[16], float2 *buf, int t, const Bases<LOG2L> &bs)
+{
+    using F = Fft<LOG2L>;
+    static_assert(F::NPASS >= 2, "transforms of at least 64 points");
+    if constexpr (HALF) dft16_half(x);
+    else dft16(x);
+    pass_out<LOG2L, 0>(buf, x, t);
+    __syncthreads();
+    pass_in<LOG2L, 1>(buf, x, t, bs.w[1]);
+    if constexpr (F::NPASS > 2) {
+        __syncthreads();
+        pass_out<LOG2L, 1>(buf, x, t);
+        __syncthreads();
+        pass_in<LOG2L, 2>(buf, x, t, bs.w[2]);
+    }
+    if constexpr (F::NPASS > 3) {
+        __syncthreads();
+        pass_out<LOG2L, 2>(buf, x, t);
+        __syncthreads();
+        pass_in<LOG2L, 3>(buf, x, t, bs.w[3]);
+    }
+    __syncthreads();  // every thread is done reading the buffer before the next transform writes it
+    last_to_natural<LOG2L>(x);
 }
 
 // Quad of rows (top, bot) at column c in the storage form of MODE (quad_f32 / quad_f16).
@@ -143,170 +322,287 @@ __device__ __forceinline__ void store_quad(void *out, long long qidx, float p00,
         static_cast<uint2 *>(out)[qidx] = quad_f16(p00, p01, p10, p11);
 }
 
-// Writes quad row `r` (detector row r, padded index r + kQuadPad) of view v from the filtered
-// rows `top` (row r) and `bot` (row r + 1); either may be NULL for a zero row. Values are scaled
-// by `sc`. Rows read from the FFT buffer use its padded indexing and sign.
+// Quad row qr (detector rows qr and qr + 1) of view v (stack index) from two shared rows stored
+// with two zero entries before column 0 and a zero tail (row[c + 2] = y[c]); NULL = zero row.
 template <int MODE>
-__device__ __forceinline__ void write_quad_row(const FilterArgs &a, int v, int r, const float *top,
-                                               const float2 *bot, bool bot_imag, float sc, int tid, int nthr)
+__device__ __forceinline__ void write_quad_row(const FilterArgs &a, int v, int qr, const float *top, const float *bot,
+                                               int t, int nthr)
 {
-    const int nc = a.nc;
-    const int qpitch = nc + 2 * kQuadPad;
+    const int qpitch = a.nc + 2 * kQuadPad;
     long long first;
     int step;
-    quad_layout(a.v0 + v, static_cast<long long>(a.nr + 2 * kQuadPad) * qpitch, a.quarter, first, step);
-    const long long row0 = first + static_cast<long long>(r + kQuadPad) * qpitch * step;
-    auto tv = [&](int c) -> float { return (top && c >= 0 && c < nc) ? top[c] : 0.0f; };
-    auto bv = [&](int c) -> float {
-        if (!bot || c < 0 || c >= nc) return 0.0f;
-        const float2 z = bot[pad(c)];
-        return sc * (bot_imag ? -z.y : z.x);
-    };
-    for (int cq = tid; cq < qpitch; cq += nthr) {
-        const int c = cq - kQuadPad;
-        store_quad<MODE>(a.out, row0 + static_cast<long long>(cq) * step, tv(c), tv(c + 1), bv(c), bv(c + 1));
+    quad_layout(v, static_cast<long long>(a.nr + 2 * kQuadPad) * qpitch, a.quarter, first, step);
+    const long long row0 = first + static_cast<long long>(qr + kQuadPad) * qpitch * step;
+    for (int cq = t; cq < qpitch; cq += nthr) {
+        const float p00 = top ? top[cq] : 0.f, p01 = top ? top[cq + 1] : 0.f;
+        const float p10 = bot ? bot[cq] : 0.f, p11 = bot ? bot[cq + 1] : 0.f;
+        store_quad<MODE>(a.out, row0 + static_cast<long long>(cq) * step, p00, p01, p10, p11);
     }
 }
 
-// Transposed quad grid of view v of a one-row detector from its filtered, scaled row y (shared).
+// Transposed quad grid of view v of a one-row detector from its filtered row y (shared, padded
+// as above).
 template <int MODE>
-__device__ __forceinline__ void write_quads_t1d(const FilterArgs &a, int v, const float *y, int tid, int nthr)
+__device__ __forceinline__ void write_quads_t1d(const FilterArgs &a, int v, const float *y, int t, int nthr)
 {
     const int nc = a.nc, rows = nc + 2 * kQuadPad;
-    const long long base = static_cast<long long>(a.v0 + v) * rows * kT1dPitch;
-    auto yv = [&](int r) -> float { return (r >= 0 && r < nc) ? y[r] : 0.0f; };
-    for (int e = tid; e < rows * kT1dPitch; e += nthr) {
-        const int r = e / kT1dPitch - kQuadPad, c = e % kT1dPitch - kQuadPad;
-        const float t = yv(r), b = yv(r + 1);
+    const long long base = static_cast<long long>(v) * rows * kT1dPitch;
+    for (int e = t; e < rows * kT1dPitch; e += nthr) {
+        const int r = e / kT1dPitch, c = e % kT1dPitch - kQuadPad;  // y[r - 2] is shared entry r
+        const float tp = y[r], bt = y[r + 1];
         if (c == 0)
-            store_quad<MODE>(a.out, base + e, t, 0.0f, b, 0.0f);
+            store_quad<MODE>(a.out, base + e, tp, 0.0f, bt, 0.0f);
         else if (c == -1)
-            store_quad<MODE>(a.out, base + e, 0.0f, t, 0.0f, b);
+            store_quad<MODE>(a.out, base + e, 0.0f, tp, 0.0f, bt);
         else
             store_quad<MODE>(a.out, base + e, 0.0f, 0.0f, 0.0f, 0.0f);
     }
 }
 
-template <int LOG2L, int MODE>
-__global__ void __launch_bounds__(256) filter_fft_kernel(FilterArgs a, int seg_rows, int nseg)
+// Loads, weights and packs detector rows a (real part) and b (imaginary part) at columns t + T m;
+// NULL rows are zero. Columns at or past nc are zero.
+template <int LOG2L, bool HALF>
+__device__ __forceinline__ void load_pair(const FilterArgs &a, float2 (&x)[16], const float *pa, const float *pb,
+                                          const RowWeight &wa, const RowWeight &wb, const float *ka, const float *kb,
+                                          int t)
 {
-    constexpr int L = 1 << LOG2L;
-    constexpr int NT = (L / 4 < 256) ? L / 4 : 256;
-    constexpr int LP = L + L / 16;
-    extern __shared__ float2 smem[];
-    float2 *tw = smem, *b0 = smem + L, *b1 = smem + L + LP;
-    float *yprev = reinterpret_cast<float *>(smem + L + 2 * LP);
-    const int tid = threadIdx.x;
-    for (int m = tid; m < L; m += NT) tw[m] = a.twiddle[m];
-
-    const int nc = a.nc, nr = a.nr;
-    for (long long blk = blockIdx.x; blk < static_cast<long long>(a.nv) * nseg; blk += gridDim.x) {
-        const int v = static_cast<int>(blk / nseg), s = static_cast<int>(blk - static_cast<long long>(v) * nseg);
-        const int r0 = s * seg_rows, r1 = min(r0 + seg_rows, nr);
-        const bool quads = MODE != kOutPlainF32;
-        const int last_row = (quads && r1 < nr) ? r1 : r1 - 1;  // quads: one extra row closes the segment
-        const float4 gv = __ldg(&a.fview[v]);
-        const float *wpk = a.parker + static_cast<long long>(v) * nc;
-        const float sc = (quads && a.vscale) ? a.vscale[v] : 1.0f;
-        int prev_row = r0 - 1;
-        bool have_prev = false;
-        if (quads && s == 0 && !a.t1d) {
-            write_quad_row<MODE>(a, v, -2, nullptr, nullptr, false, sc, tid, NT);
-            for (int c = tid; c < nc; c += NT) yprev[c] = 0.0f;  // row -1 is zero
-            have_prev = true;
-        }
-        __syncthreads();
-        for (int ra = r0; ra <= last_row; ra += 2) {
-            const bool has_b = ra + 1 <= last_row;
-            const float *pa = a.proj + (static_cast<long long>(v) * nr + ra) * nc;
-            const float *pb = pa + nc;
-            // load, weight and first radix-4 stage straight from global memory
-            for (int j = tid; j < L / 4; j += NT) {
-                float2 x[4];
+    constexpr int T = Fft<LOG2L>::T;
+    constexpr int MZ = HALF ? 8 : 11;  // nc <= L / 1.5 < 11 T
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int k = j + q * (L / 4);
-                    x[q] = make_float2(0.f, 0.f);
-                    if (k < nc) {
-                        const float w = __ldg(wpk + k);
-                        x[q].x = __ldg(pa + k) * w * cos_weight_dev(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k, ra);
-                        if (has_b) x[q].y = __ldg(pb + k) * w * cos_weight_dev(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, k, ra + 1);
+    for (int m = 0; m < 16; ++m) x[m] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int m = 0; m < MZ; ++m) {
+        const int c = t + T * m;
+        if (c < a.nc) {
+            const float k = __ldg(ka + c);
+            if (pa) x[m].x = __ldg(pa + c) * (wa.at(c) * k);
+            if (pb) x[m].y = __ldg(pb + c) * (wb.at(c) * (kb == ka ? k : __ldg(kb + c)));
+        }
+    }
+}
+
+// Spectrum product and the conjugation that turns the next forward transform into the inverse:
+// x <- conj(x H), H already scaled by 1 / L.
+template <int LOG2L>
+__device__ __forceinline__ void spectrum(float2 (&x)[16], const float2 *__restrict__ H, int t)
+{
+    constexpr int T = Fft<LOG2L>::T;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const float2 h = __ldg(H + t + T * m);
+        const float2 z = cmul(x[m], h);
+        x[m] = make_float2(z.x, -z.y);
+    }
+}
+
+// Filters the detector rows (ra, rb) of views (va, vb) (rows beyond the detector, or a view < 0,
+// are zero) and leaves the filtered rows in natural order: row a in x[m].x, row b in -x[m].y at
+// columns t + T m.
+template <int LOG2L, bool HALF>
+__device__ __forceinline__ void filter_pair(const FilterArgs &a, float2 (&x)[16], float2 *buf, int t,
+                                            const Bases<LOG2L> &bs, int va, int ra, int vb, int rb)
+{
+    const bool has_a = va >= 0 && ra >= 0 && ra < a.nr, has_b = vb >= 0 && rb >= 0 && rb < a.nr;
+    const long long pix = static_cast<long long>(a.nr) * a.nc;
+    const int ua = has_a ? va : 0, ub = has_b ? vb : ua;
+    const float *pa = has_a ? a.proj + ua * pix + static_cast<long long>(ra) * a.nc : nullptr;
+    const float *pb = has_b ? a.proj + ub * pix + static_cast<long long>(rb) * a.nc : nullptr;
+    const float4 ga = __ldg(&a.fview[ua]), gb = __ldg(&a.fview[ub]);
+    const RowWeight wa = row_weight(a.kind, ga.x, ga.y, ga.z, a.du, a.dv, ra);
+    const RowWeight wb = row_weight(a.kind, gb.x, gb.y, gb.z, a.du, a.dv, rb);
+    const float *ka = a.parker + static_cast<long long>(ua) * a.nc;
+    const float *kb = a.parker + static_cast<long long>(ub) * a.nc;
+    load_pair<LOG2L, HALF>(a, x, pa, pb, wa, wb, ka, kb, t);
+    transform<LOG2L, HALF>(x, buf, t, bs);
+    spectrum<LOG2L>(x, a.H, t);
+    transform<LOG2L, false>(x, buf, t, bs);
+}
+
+// Writes the filtered rows held in x into two shared rows (padded: row[c + 2] = y[c]), scaled.
+template <int LOG2L>
+__device__ __forceinline__ void stage_rows(const float2 (&x)[16], float *ya, float *yb, float sa, float sb, int nc,
+                                           int t)
+{
+    constexpr int T = Fft<LOG2L>::T;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const int c = t + T * m;
+        if (c < nc) {
+            ya[c + 2] = sa * x[m].x;
+            yb[c + 2] = -sb * x[m].y;
+        }
+    }
+}
+
+// Resident blocks per SM asked of the compiler (caps registers at 65536 / (T * MINB)).
+template <int LOG2L>
+constexpr int fft_min_blocks()
+{
+    return Fft<LOG2L>::T >= 512 ? 1 : Fft<LOG2L>::T >= 256 ? 2 : Fft<LOG2L>::T >= 128 ? GCT_FFT_MINB : 8;
+}
+
+template <int LOG2L, int MODE, bool HALF, bool ONE_ROW>
+__global__ void __launch_bounds__(Fft<LOG2L>::T, fft_min_blocks<LOG2L>())
+    filter_fft_kernel(FilterArgs a, int seg, int nseg)
+{
+    using F = Fft<LOG2L>;
+    constexpr int T = F::T;
+    extern __shared__ float2 smem[];
+    float2 *buf = smem;
+    const int rpitch = (a.nc + 2 * kQuadPad + 4) & ~3;  // padded shared row: 2 zeros, nc values, zeros
+    float *rows = reinterpret_cast<float *>(smem + F::LP);
+    const int t = threadIdx.x;
+    Bases<LOG2L> bs;
+    bs.init(t);
+    for (int e = t; e < 3 * rpitch; e += T) rows[e] = 0.f;
+    __syncthreads();
+    float2 x[16];
+    constexpr bool quads = MODE != kOutPlainF32;
+
+    if constexpr (ONE_ROW) {
+        // one-row detectors: rows of views (2 i, 2 i + 1) share a transform; each view's grid is
+        // written whole from its own row
+        const int npair = (a.nv + 1) / 2;
+        for (int pi = blockIdx.x; pi < npair; pi += gridDim.x) {
+            const int va = 2 * pi, vb = (2 * pi + 1 < a.nv) ? 2 * pi + 1 : -1;
+            filter_pair<LOG2L, HALF>(a, x, buf, t, bs, va, 0, vb, 0);
+            if constexpr (!quads) {
+#pragma unroll
+                for (int m = 0; m < 16; ++m) {
+                    const int c = t + T * m;
+                    if (c < a.nc) {
+                        static_cast<float *>(a.out)[static_cast<long long>(va) * a.nc + c] = x[m].x;
+                        if (vb >= 0) static_cast<float *>(a.out)[static_cast<long long>(vb) * a.nc + c] = -x[m].y;
                     }
                 }
-                const float2 t0 = cadd(x[0], x[2]), t1 = csub(x[0], x[2]), t2 = cadd(x[1], x[3]);
-                const float2 d = csub(x[1], x[3]);
-                const float2 t3 = make_float2(d.y, -d.x);
-                b0[pad(4 * j)] = cadd(t0, t2);
-                b0[pad(4 * j + 1)] = cadd(t1, t3);
-                b0[pad(4 * j + 2)] = csub(t0, t2);
-                b0[pad(4 * j + 3)] = csub(t1, t3);
-            }
-            __syncthreads();
-            float2 *spec = fft_rest<LOG2L, NT, true>(b0, b1, tw, a.H, tid);  // conj(FFT(x) H)
-            float2 *other = (spec == b0) ? b1 : b0;
-            first_stage_smem<L, NT>(spec, other, tid);
-            __syncthreads();
-            float2 *res = fft_rest<LOG2L, NT, false>(other, spec, tw, a.H, tid);  // conj of the filtered rows
-            // rows: ra in .x, ra + 1 in -.y
-            for (int h = 0; h < (has_b ? 2 : 1); ++h) {
-                const int rr = ra + h;
-                if (!quads) {
-                    if (rr < r1) {
-                        float *out = static_cast<float *>(a.out) + (static_cast<long long>(v) * nr + rr) * nc;
-                        for (int c = tid; c < nc; c += NT) out[c] = h ? -res[pad(c)].y : res[pad(c)].x;
+            } else {
+                float *ya = rows, *yb = rows + rpitch;
+                const float sa = a.vscale ? a.vscale[va] : 1.f, sb = (a.vscale && vb >= 0) ? a.vscale[vb] : 1.f;
+                stage_rows<LOG2L>(x, ya, yb, sa, sb, a.nc, t);
+                __syncthreads();
+                for (int h = 0; h < 2; ++h) {
+                    const int v = h ? vb : va;
+                    if (v < 0) continue;
+                    const float *y = h ? yb : ya;
+                    if (a.t1d) {
+                        write_quads_t1d<MODE>(a, a.v0 + v, y, t, T);
+                    } else {
+                        write_quad_row<MODE>(a, a.v0 + v, -2, nullptr, nullptr, t, T);
+                        write_quad_row<MODE>(a, a.v0 + v, -1, nullptr, y, t, T);
+                        write_quad_row<MODE>(a, a.v0 + v, 0, y, nullptr, t, T);
+                        write_quad_row<MODE>(a, a.v0 + v, 1, nullptr, nullptr, t, T);
+                        write_quad_row<MODE>(a, a.v0 + v, 2, nullptr, nullptr, t, T);
                     }
-                    continue;
                 }
-                if (have_prev) write_quad_row<MODE>(a, v, prev_row, yprev, res, h == 1, sc, tid, NT);
-                __syncthreads();
-                for (int c = tid; c < nc; c += NT) yprev[c] = sc * (h ? -res[pad(c)].y : res[pad(c)].x);
-                prev_row = rr;
-                have_prev = true;
-                __syncthreads();
+                __syncthreads();  // the shared rows are rewritten by the next pair
             }
-            __syncthreads();
         }
-        if (quads && a.t1d) {  // one-row detector: the transposed grid from the filtered row
-            write_quads_t1d<MODE>(a, v, yprev, tid, NT);
-        } else if (quads && r1 == nr) {  // last segment: rows nr-1 (bottom neighbour zero), nr and nr+1
-            write_quad_row<MODE>(a, v, nr - 1, yprev, nullptr, false, sc, tid, NT);
-            write_quad_row<MODE>(a, v, nr, nullptr, nullptr, false, sc, tid, NT);
-            write_quad_row<MODE>(a, v, nr + 1, nullptr, nullptr, false, sc, tid, NT);
+        return;
+    } else {
+    const long long items = static_cast<long long>(a.nv) * nseg;
+    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+        const int v = static_cast<int>(it / nseg), s = static_cast<int>(it - static_cast<long long>(v) * nseg);
+        if constexpr (!quads) {
+            // plain rows [r0, r1) of view v
+            const int r0 = s * seg, r1 = min(r0 + seg, a.nr);
+            for (int ra = r0; ra < r1; ra += 2) {
+                const int rb = ra + 1 < r1 ? ra + 1 : -1;
+                filter_pair<LOG2L, HALF>(a, x, buf, t, bs, v, ra, rb >= 0 ? v : -1, rb);
+                float *out = static_cast<float *>(a.out) + (static_cast<long long>(v) * a.nr + ra) * a.nc;
+#pragma unroll
+                for (int m = 0; m < 16; ++m) {
+                    const int c = t + T * m;
+                    if (c < a.nc) {
+                        out[c] = x[m].x;
+                        if (rb >= 0) out[a.nc + c] = -x[m].y;
+                    }
+                }
+            }
+        } else {
+            // quad rows [q0, q1) of view v: quad row q needs detector rows q and q + 1
+            const int q0 = -kQuadPad + s * seg, q1 = min(q0 + seg, a.nr + kQuadPad);
+            const float sc = a.vscale ? a.vscale[v] : 1.f;
+            const int sv = a.v0 + v;
+            int prev = 0, sa = 1, sb = 2;  // shared row slots: previous pair's row b, this pair's a and b
+            for (int ra = q0; ra <= q1; ra += 2) {
+                const int rb = ra + 1;
+                float *ya = rows + sa * rpitch, *yb = rows + sb * rpitch;
+                if ((ra >= 0 && ra < a.nr) || (rb >= 0 && rb < a.nr)) {
+                    filter_pair<LOG2L, HALF>(a, x, buf, t, bs, v, ra, v, rb);  // holds barriers
+                    stage_rows<LOG2L>(x, ya, yb, sc, sc, a.nc, t);
+                } else {
+                    __syncthreads();  // the previous pair's quad rows have been read from these slots
+                    for (int c = t; c < a.nc; c += T) ya[c + 2] = yb[c + 2] = 0.f;
+                }
+                __syncthreads();
+                if (ra - 1 >= q0 && ra - 1 < q1) write_quad_row<MODE>(a, sv, ra - 1, rows + prev * rpitch, ya, t, T);
+                if (ra < q1) write_quad_row<MODE>(a, sv, ra, ya, yb, t, T);
+                // the next pair writes its rows into the slots of this pair's previous row and row a,
+                // after the barriers of its transforms
+                const int np = sb;
+                sb = sa;
+                sa = prev;
+                prev = np;
+            }
         }
-        __syncthreads();
+        __syncthreads();  // the next item's first pair rewrites the shared rows
+    }
     }
 }
 
 template <int LOG2L>
 size_t smem_bytes_log2(int nc)
 {
-    constexpr int L = 1 << LOG2L;
-    return (static_cast<size_t>(L) + 2 * (L + L / 16)) * sizeof(float2) + static_cast<size_t>(nc) * sizeof(float);
+    const int rpitch = (nc + 2 * kQuadPad + 4) & ~3;
+    return static_cast<size_t>(Fft<LOG2L>::LP) * sizeof(float2) + 3 * static_cast<size_t>(rpitch) * sizeof(float);
+}
+
+template <int LOG2L, int MODE>
+void launch_mode(const FilterArgs &a, int num_sms, cudaStream_t s)
+{
+    using F = Fft<LOG2L>;
+    const size_t smem = smem_bytes_log2<LOG2L>(a.nc);
+    const bool half = a.nc <= F::L / 2;
+    long long items;
+    int seg = 0, nseg = 1;
+    if (a.nr == 1) {
+        items = (a.nv + 1) / 2;
+    } else {
+        // segments of about 64 rows (quad segments filter one extra pair to close their last quad
+        // row); shorter segments when views are few; balanced lengths, even for quads
+        const int rows = MODE == kOutPlainF32 ? a.nr : a.nr + 2 * kQuadPad;
+        seg = 64;
+        while (seg > 4 && static_cast<long long>(a.nv) * ((rows + seg - 1) / seg) < 8LL * num_sms) seg /= 2;
+        nseg = (rows + seg - 1) / seg;
+        seg = (rows + nseg - 1) / nseg;
+        if (MODE != kOutPlainF32) seg = (seg + 1) & ~1;
+        nseg = (rows + seg - 1) / seg;
+        items = static_cast<long long>(a.nv) * nseg;
+    }
+    long long grid = items;
+    const long long cap = static_cast<long long>(num_sms) * 32;
+    if (grid > cap) grid = cap;
+    if (grid < 1) grid = 1;
+    auto go = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        kern<<<static_cast<unsigned>(grid), F::T, smem, s>>>(a, seg, nseg);
+    };
+    if (a.nr == 1) {
+        if (half) go(filter_fft_kernel<LOG2L, MODE, true, true>);
+        else go(filter_fft_kernel<LOG2L, MODE, false, true>);
+    } else {
+        if (half) go(filter_fft_kernel<LOG2L, MODE, true, false>);
+        else go(filter_fft_kernel<LOG2L, MODE, false, false>);
+    }
 }
 
 template <int LOG2L>
 void launch_log2(const FilterArgs &a, int num_sms, cudaStream_t s)
 {
-    constexpr int L = 1 << LOG2L;
-    constexpr int NT = (L / 4 < 256) ? L / 4 : 256;
-    const size_t smem = smem_bytes_log2<LOG2L>(a.nc);
-    // segments of about 64 rows (one extra filtered row each); shorter segments when views are few
-    int seg_rows = 64;
-    while (seg_rows > 2 && static_cast<long long>(a.nv) * ((a.nr + seg_rows - 1) / seg_rows) < 4LL * num_sms)
-        seg_rows /= 2;
-    if (seg_rows > a.nr) seg_rows = a.nr;
-    const int nseg = (a.nr + seg_rows - 1) / seg_rows;
-    long long grid = static_cast<long long>(a.nv) * nseg;
-    const long long cap = static_cast<long long>(num_sms) * 64;
-    if (grid > cap) grid = cap;
-    auto go = [&](auto kern) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        kern<<<static_cast<unsigned>(grid), NT, smem, s>>>(a, seg_rows, nseg);
-    };
     switch (a.mode) {
-        case kOutPlainF32: go(filter_fft_kernel<LOG2L, kOutPlainF32>); break;
-        case kOutQuadF32: go(filter_fft_kernel<LOG2L, kOutQuadF32>); break;
-        default: go(filter_fft_kernel<LOG2L, kOutQuadF16>); break;
+        case kOutPlainF32: launch_mode<LOG2L, kOutPlainF32>(a, num_sms, s); break;
+        case kOutQuadF32: launch_mode<LOG2L, kOutQuadF32>(a, num_sms, s); break;
+        default: launch_mode<LOG2L, kOutQuadF16>(a, num_sms, s); break;
     }
 }
 
