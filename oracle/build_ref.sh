@@ -9,7 +9,10 @@
 #                       calls) for sm_100a, driven by oracle/ref_fdk_main.cu, for the GPU parity
 #                       tests against the reference itself;
 #   libgct_ref_io.so    the reference's array-file readers and writers (src/cpp/io) behind the C
-#                       entry points of oracle/ref_io.cpp, for the IO golden files.
+#                       entry points of oracle/ref_io.cpp, for the IO golden files;
+#   ref_wrappers        the reference's reconstruct() overloads on its own types, defined by this
+#                       repository's include/gct_recon_wrappers.hpp over gct_b200/libgct_fdk.so
+#                       (built first), driven by oracle/ref_wrappers_main.cpp.
 #
 # The reference's Eigen submodule is empty in its tree. The translation units used here compile
 # without it except for declarations in src/cpp/geom/projection_matrix.h, which
@@ -68,4 +71,9 @@ IO=(cpp/io/file_reader/meta_img_reader.cpp cpp/io/file_reader/array_file_reader.
     cpp/io/string_utils.cpp cpp/io/file_writer/meta_img_file_writer.cpp)
 g++ -std=c++20 -O2 -fPIC -w -I "$REF/src" -shared -o "$OUT/libgct_ref_io.so" "$HERE/ref_io.cpp" \
     "${IO[@]/#/$REF/src/}"
-echo "$OUT/libgct_ref_host.so $OUT/ref_fdk $OUT/libgct_ref_io.so"
+# the drop-in overloads on the reference's types, over this repository's library
+REPO="$(cd "$HERE/.." && pwd)"
+g++ -std=c++20 -O2 -w -I "$REF/src" -I "$REPO/include" -I "$HERE" -o "$OUT/ref_wrappers" "$HERE/ref_wrappers_main.cpp" \
+    "$OUT/rotation_geom.o" "$OUT/vec_wcs.o" "$OUT/proj_meta_info.o" -L "$REPO/gct_b200" -lgct_fdk \
+    -Wl,-rpath,'$ORIGIN/../../gct_b200'
+echo "$OUT/libgct_ref_host.so $OUT/ref_fdk $OUT/libgct_ref_io.so $OUT/ref_wrappers"

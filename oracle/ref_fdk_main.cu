@@ -25,10 +25,7 @@
 //                                             [height][width]; float32 n (x, y) coordinates as passed
 //                                             to tex1D / tex2D. Output: n float32 fetched values.
 //
-// Input file (little endian): int32 kind, nc, nr, nv, nx, ny, nz; float32 du, dv, dx, dy, dz, mx,
-// my, mz; nv records of 17 float32 (rot_ang, det_row_center, det_col_center, src_det_dist,
-// src_iso_dist, src_pos[3], det_row_dir[3], det_col_dir[3], iso_ray_dir[3]); nv*nr*nc float32
-// projections. Output file: nz*ny*nx float32 (nz = 1 for 2D images).
+// Input file: the format of ref_input.hpp. Output file: nz*ny*nx float32 (nz = 1 for 2D images).
 //
 // The reference composes a projection matrix per flat-detector view (ct_geom_dev.cu:421-441) that no
 // kernel reads; its constructor needs Eigen, so this harness defines it as leaving the matrix zero.
@@ -46,6 +43,7 @@
 #include "cpp/recon/check_validity.h"
 #include "cuda/recon/recon_wrappers.cuh"
 #include "cuda/recon/fdk_axial.cuh"
+#include "ref_input.hpp"
 
 #include <chrono>
 #include <cstring>
@@ -67,45 +65,7 @@ VecWCS<3u> crossProduct(VecWCS<3u> const &a, VecWCS<3u> const &b)
 }  // namespace GCT::Geom
 
 namespace {
-struct Rec {
-    float rot, rc, cc, sdd, sid, s[3], ru[3], rv[3], iso[3];
-};
-VecWCS<2u> v2(const float *p) { return VecWCS<2u>{p[0], p[1]}; }
-VecWCS<3u> v3(const float *p) { return VecWCS<3u>{p[0], p[1], p[2]}; }
-Units::MilliMeters mm(float x) { return Units::MilliMeters{x}; }
-Units::DetPixels px(float x) { return Units::DetPixels{x}; }
-
-template <class PG>
-PG make(const Rec &r);
-template <> ProjGeom<DetParallel> make(const Rec &r) { return {Units::Radians{r.rot}, px(r.rc)}; }
-template <> ProjGeom<DetFanArc> make(const Rec &r) { return {mm(r.sdd), px(r.rc), v2(r.s), v2(r.ru), v2(r.iso)}; }
-template <> ProjGeom<DetFanLine> make(const Rec &r) { return {mm(r.sdd), px(r.rc), v2(r.s), v2(r.ru)}; }
-template <> ProjGeom<DetParallel, DetParallel> make(const Rec &r) { return {Units::Radians{r.rot}, px(r.rc), px(r.cc)}; }
-template <> ProjGeom<DetParallel, DetFanLine> make(const Rec &r)
-{
-    return {mm(r.sdd), mm(r.sid), Units::Radians{r.rot}, px(r.rc), px(r.cc)};
-}
-template <> ProjGeom<DetFanArc, DetFanLine> make(const Rec &r)
-{
-    return {mm(r.sdd), px(r.rc), px(r.cc), v3(r.s), v3(r.ru), v3(r.rv), v3(r.iso)};
-}
-template <> ProjGeom<DetFanLine, DetFanLine> make(const Rec &r)
-{
-    return {mm(r.sdd), px(r.rc), px(r.cc), v3(r.s), v3(r.ru), v3(r.rv)};
-}
-
-template <class Det> Det det(unsigned n, float w);
-template <> DetParallel det(unsigned n, float w) { return DetParallel{EqDistSampler{n, mm(w)}}; }
-template <> DetFanLine det(unsigned n, float w) { return DetFanLine{EqDistSampler{n, mm(w)}}; }
-template <> DetFanArc det(unsigned n, float w) { return DetFanArc{EqAngSampler{n, Units::Radians{w}}}; }
-
-struct Input {
-    int kind, nc, nr, nv, nx, ny, nz;
-    float du, dv, dx, dy, dz, mx, my, mz;
-    std::vector<Rec> recs;
-    std::vector<float> proj;
-};
-
+using namespace ref_input;
 
 // ---- bilinear interpolation in place of the texture fetch (--bp) ------------------------------
 enum BpMode { kBpExact = 0, kBpTexture = 1 };
@@ -440,20 +400,7 @@ int main(int argc, char **argv)
             return 2;
         }
         if (probe) return texprobe(argv[a], argv[a + 1]);
-        std::ifstream f(argv[a], std::ios::binary);
-        Input in{};
-        int32_t hdr[7];
-        float fl[8];
-        f.read(reinterpret_cast<char *>(hdr), sizeof(hdr));
-        f.read(reinterpret_cast<char *>(fl), sizeof(fl));
-        in.kind = hdr[0], in.nc = hdr[1], in.nr = hdr[2], in.nv = hdr[3], in.nx = hdr[4], in.ny = hdr[5], in.nz = hdr[6];
-        in.du = fl[0], in.dv = fl[1], in.dx = fl[2], in.dy = fl[3], in.dz = fl[4], in.mx = fl[5], in.my = fl[6],
-        in.mz = fl[7];
-        in.recs.resize(in.nv);
-        f.read(reinterpret_cast<char *>(in.recs.data()), sizeof(Rec) * in.nv);
-        in.proj.resize(static_cast<size_t>(in.nv) * in.nr * in.nc);
-        f.read(reinterpret_cast<char *>(in.proj.data()), sizeof(float) * in.proj.size());
-        if (!f) throw std::runtime_error("short input file");
+        const Input in = read_input(argv[a]);
         if (opt.spiral && in.kind != 5) throw std::runtime_error("--spiral needs kind 5 (cylindrical detector)");
         std::vector<float> out;
         switch (in.kind) {
