@@ -407,6 +407,37 @@ def oracle_errors(cg, cfg, proj_dev, vols, seed):
     return out, len(vox)
 
 
+def sampled_oracle_error(cg, c, proj, vol, seed, nvox=2000):
+    """relRMS / max error of one reconstruction (host arrays) against the FP64 oracle on nvox
+    sampled voxels (3D volumes: the two central slices, detector cut to the rows those slices
+    project onto), with the oracle's time for them as a CPU rate (voxel x view updates / s)."""
+    from oracle import oracle as orc
+    nx, ny, nz = c["n"]
+    rs = np.random.RandomState(seed)
+    is3d = cg.is_3d
+    k = np.full(nvox, 0) if nz <= 1 else (nz // 2 - 1 + (np.arange(nvox) % 2))
+    vox = np.stack([rs.randint(0, nx, nvox), rs.randint(0, ny, nvox), k], 1).astype(np.uint32)
+    views = cg.views.copy()
+    r_lo, r_hi = (sample_rows(cg.num_rows) if is3d else (0, 1))
+    if is3d:
+        views["det_col_center"] -= r_lo
+    det = cg.det_geom()
+    og = orc.Geometry(int(cg.kind), cg.num_cols, det[0].sampling_width, views, (r_hi - r_lo) if is3d else 1,
+                      det[1].sampling_width if is3d else 1.0)
+    vz = c.get("voxz", c["vox"])
+    ov = orc.Volume(nx, ny, max(nz, 1), c["vox"], c["vox"], vz, (0.0, 0.0, 0.0))
+    rows = np.ascontiguousarray(proj[:, r_lo:r_hi, :]) if is3d else proj
+    threads = os.cpu_count() or 1
+    t = time.perf_counter()
+    ref = orc.fdk(og, ov, rows, voxels=vox, use_fft=True, threads=threads)
+    dt = time.perf_counter() - t
+    flat = (vox[:, 2].astype(np.int64) * ny + vox[:, 1]) * nx + vox[:, 0]
+    got = np.asarray(vol, dtype=np.float64).reshape(-1)[flat]
+    err = {"voxels": int(nvox), "rel_rms": float(np.sqrt(np.mean((got - ref) ** 2) / np.mean(ref ** 2))),
+           "max_rel": float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))}
+    return err, len(vox) * cg.num_views / dt / 1e9, threads
+
+
 def time_plan(plan, proj, vol, steps, warmup, stream, dist):
     """Times `steps` full FDKs: returns (total seconds max over ranks, mean filter ms, mean BP ms)."""
     import torch
@@ -698,6 +729,24 @@ def run_batch(args, rank, world, local_rank):
     t_batch = device_timed(lambda: batch.launch(stream=stream), args.steps, args.warmup, stream, dist, device)
     clocks = sampler.stop()
     batch_vols = [v.clone() for v in vols]
+    errors, cpu = None, None
+    if rank == 0 and not args.no_error:
+        # one item of each geometry class, checked against the FP64 oracle on sampled voxels
+        errors, rates, threads = {}, [], 1
+        seen = set()
+        for i, c in enumerate(specs):
+            key = f"{c['kind']} {c['n'][0]}x{c['n'][1]}x{c['n'][2]} nv={c['nv']}"
+            if c["kind"] in seen or (c["kind"] == "parallel_1d" and c["n"][0] != 1024):
+                continue
+            seen.add(c["kind"])
+            cg_i, _ = make_geometry2(c)
+            err, rate, threads = sampled_oracle_error(cg_i, c, projs[i].cpu().numpy(), batch_vols[i].cpu().numpy(),
+                                                      args.seed + i)
+            errors[key] = err
+            rates.append(rate)
+        cpu = {"value": float(np.median(rates)), "unit": "GUPS", "cores": threads, "kind": "port",
+               "sample": "FP64 oracle FDK of 2000 sampled voxels (3D: the two central slices) of one item per "
+                         f"geometry class, all views, {threads} threads; median over the classes"}
 
     def sequential():
         for p, pr, v in zip(plans, projs, vols):
@@ -729,7 +778,7 @@ def run_batch(args, rank, world, local_rank):
         "max_rel_diff_batch_vs_sequential": diff,
         "work_entries": n_work, "batch_build_s": t_build, "tile_configs": configs,
         "clocks": clocks, "gpu_launches": (3 * len(specs) + 1) * args.steps,
-        "cpu_baseline": None, "e2e": None,
+        "error_vs_fp64_oracle": errors, "cpu_baseline": cpu, "e2e": None,
     }
     print(json.dumps(line), flush=True)
 
@@ -807,6 +856,19 @@ def run_serve(args, rank, world, local_rank):
     for j, f in enumerate(float(x) for x in args.serve_loads.split(",")):
         loads.append(dict(load=f, **run_load(f * cap, args.serve_requests, args.seed + 200 + j)))
     clocks = sampler.stop()
+    errors, cpu = None, None
+    if rank == 0 and not args.no_error:
+        errors, rates, threads = {}, [], 1
+        for i, (name, frac, c, filt, nbuf) in enumerate(kinds):
+            k = cls[i]
+            cg_i, _ = make_geometry2(c)
+            # the class's buffer 0 holds a completed reconstruction of the class's projections
+            err, rate, threads = sampled_oracle_error(cg_i, c, k["proj"], k["outs"][0], args.seed + i)
+            errors[name] = err
+            rates.append(rate)
+        cpu = {"value": float(np.median(rates)), "unit": "GUPS", "cores": threads, "kind": "port",
+               "sample": "FP64 oracle FDK of 2000 sampled voxels (3D: the two central slices) of each request "
+                         f"class, all views, {threads} threads; median over the classes"}
     st = srv.stats()
     srv.close()
     for k in cls:
@@ -824,7 +886,7 @@ def run_serve(args, rank, world, local_rank):
         "p50_ms": mid["p50_ms"], "p99_ms": mid["p99_ms"], "capacity": sat, "loads": loads,
         "server": {"rounds": st["rounds"], "peak_active": st["peak_active"], "peak_bytes": st["peak_bytes"]},
         "e2e": {"value": mid["recons_per_s"], "unit": "recons/s", "path": "host buffers in and out through the server"},
-        "clocks": clocks, "cpu_baseline": None,
+        "clocks": clocks, "error_vs_fp64_oracle": errors, "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
 
