@@ -186,19 +186,9 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
     for (double t : taps) l1 += std::fabs(t);
     p->l1 = static_cast<float>(l1);
     const auto Hd = gct::filter_spectrum(taps, p->L);
-    std::vector<float2> H(p->L), tw(p->L, make_float2(0.f, 0.f));
+    std::vector<float2> H(p->L);
     for (unsigned k = 0; k < p->L; ++k)
         H[k] = make_float2(static_cast<float>(Hd[k].real()), static_cast<float>(Hd[k].imag()));
-    // per-stage twiddles of the Stockham FFT: stage of span Ns and radix R at tw[Ns + k], k < Ns
-    auto put_stage = [&](unsigned Ns, unsigned R) {
-        for (unsigned k = 0; k < Ns; ++k) {
-            const double ang = -2.0 * 3.14159265358979323846 * k / (static_cast<double>(R) * Ns);
-            tw[Ns + k] = make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(std::sin(ang)));
-        }
-    };
-    unsigned Ns = 4;
-    for (; Ns * 4 <= p->L; Ns *= 4) put_stage(Ns, 4);
-    if (Ns * 2 == p->L) put_stage(Ns, 2);
 
     cuda_check(cudaGetDevice(&p->device), "cudaGetDevice");
     cudaDeviceProp prop{};
@@ -207,7 +197,9 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
     p->fview.upload(fview.data(), fview.size(), "plan geometry");
     p->parker.upload(parker.data(), parker.size(), "plan Parker table");
     p->H.upload(H.data(), H.size(), "plan filter spectrum");
-    p->tw.upload(tw.data(), tw.size(), "plan twiddles");
+    // status word of the plan's kernels (gct_fdk_plan_check): GEMM pipeline and FFT input waits
+    p->gemm_err.alloc(1, "kernel status");
+    cuda_check(cudaMemset(p->gemm_err.p, 0, sizeof(int)), "kernel status reset");
     p->coefs.upload(coefs.data(), coefs.size(), "plan backprojection coefficients");
     if (p->opts.filter != GCT_FILTER_FFT) {
         // B = T^T with T[k][c] = g(c - k): row n holds g(n - k); taps g(m) = taps[m + nc/2]
@@ -244,8 +236,6 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
         if (four) p->xll.alloc(rows * p->Kp, "GEMM rows (third piece)");
         if (f16) p->grinv.alloc(rows, "GEMM row scales");
         p->ybuf.alloc(rows * p->nc, "GEMM filtered rows");
-        p->gemm_err.alloc(1, "GEMM status");
-        cuda_check(cudaMemset(p->gemm_err.p, 0, sizeof(int)), "GEMM status reset");
     }
     // backprojection launch shape
     const bool vol3d = gct::is_2d_detector(kind);
@@ -393,7 +383,7 @@ void run_filter(gct_fdk_plan *p, const float *proj, void *out, const float *vsca
     fa.fview = p->fview.p + vb;
     fa.parker = p->parker.p + static_cast<long long>(vb) * p->nc;
     fa.H = p->H.p;
-    fa.twiddle = p->tw.p;
+    fa.err = p->gemm_err.p;
     fa.mode = mode;
     if (mode == gct::kOutPlainF32) {
         fa.out = static_cast<float *>(out) + vb * pix;
@@ -948,7 +938,9 @@ gct_status gct_fdk_plan_check(gct_fdk_plan *plan)
         int e = 0;
         cuda_check(cudaMemcpy(&e, plan->gemm_err.p, sizeof(int), cudaMemcpyDeviceToHost), "GEMM status read");
         if (e) {
-            cuda_check(cudaMemset(plan->gemm_err.p, 0, sizeof(int)), "GEMM status reset");
+            cuda_check(cudaMemset(plan->gemm_err.p, 0, sizeof(int)), "kernel status reset");
+            if (e & gct::kFftWaitTimeout)
+                gct::fail(GCT_ERR_TIMEOUT, "FFT filter: a projection row copy did not arrive within 2 s");
             gct::fail(GCT_ERR_TIMEOUT, "Toeplitz GEMM pipeline wait timed out (stage " + std::to_string(e) + ")");
         }
     });

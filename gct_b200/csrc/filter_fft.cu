@@ -26,13 +26,11 @@
 // Work split: one CTA per (view, segment of quad rows) (or, for one-row detectors, per pair of
 // views). A CTA walks its rows in pairs, keeps the filtered rows of the previous pair in shared
 // memory and writes each quad row whole once its two detector rows are known.
+#include <cstdint>
+
 #include "../../include/gct_fdk.h"
 #include "common.cuh"
 #include "kernels.hpp"
-
-#ifndef GCT_FFT_MINB
-#define GCT_FFT_MINB 4
-#endif
 
 namespace gct {
 namespace {
@@ -395,18 +393,15 @@ __device__ __forceinline__ void spectrum(float2 (&x)[16], const float2 *__restri
     }
 }
 
-// Filters the detector rows (ra, rb) of views (va, vb) (rows beyond the detector, or a view < 0,
-// are zero) and leaves the filtered rows in natural order: row a in x[m].x, row b in -x[m].y at
-// columns t + T m.
+// Filters the detector rows pa (real part) and pb (imaginary part) (NULL = zero row; global or
+// shared memory) of views va and vb, rows ra and rb (for the weights), and leaves the filtered rows
+// in natural order: row a in x[m].x, row b in -x[m].y at columns t + T m.
 template <int LOG2L, bool HALF>
 __device__ __forceinline__ void filter_pair(const FilterArgs &a, float2 (&x)[16], float2 *buf, int t,
-                                            const Bases<LOG2L> &bs, int va, int ra, int vb, int rb)
+                                            const Bases<LOG2L> &bs, const float *pa, const float *pb, int va, int ra,
+                                            int vb, int rb)
 {
-    const bool has_a = va >= 0 && ra >= 0 && ra < a.nr, has_b = vb >= 0 && rb >= 0 && rb < a.nr;
-    const long long pix = static_cast<long long>(a.nr) * a.nc;
-    const int ua = has_a ? va : 0, ub = has_b ? vb : ua;
-    const float *pa = has_a ? a.proj + ua * pix + static_cast<long long>(ra) * a.nc : nullptr;
-    const float *pb = has_b ? a.proj + ub * pix + static_cast<long long>(rb) * a.nc : nullptr;
+    const int ua = pa ? va : 0, ub = pb ? vb : ua;
     const float4 ga = __ldg(&a.fview[ua]), gb = __ldg(&a.fview[ub]);
     const RowWeight wa = row_weight(a.kind, ga.x, ga.y, ga.z, a.du, a.dv, ra);
     const RowWeight wb = row_weight(a.kind, gb.x, gb.y, gb.z, a.du, a.dv, rb);
@@ -438,130 +433,269 @@ __device__ __forceinline__ void stage_rows(const float2 (&x)[16], float *ya, flo
 template <int LOG2L>
 constexpr int fft_min_blocks()
 {
-    return Fft<LOG2L>::T >= 512 ? 1 : Fft<LOG2L>::T >= 256 ? 2 : Fft<LOG2L>::T >= 128 ? GCT_FFT_MINB : 8;
+    return Fft<LOG2L>::T >= 512 ? 1 : Fft<LOG2L>::T >= 256 ? 2 : Fft<LOG2L>::T >= 128 ? 4 : 8;
 }
 
-template <int LOG2L, int MODE, bool HALF, bool ONE_ROW>
+// ---- input pipeline --------------------------------------------------------------------------
+// With BULK, the two raw rows of the next pair are copied into a shared stage by the tensor memory
+// accelerator (cp.async.bulk, one thread) while the current pair is transformed; two stages, one
+// mbarrier each. Every wait is bounded (2 s of %globaltimer): on a timeout the CTA records
+// kFftWaitTimeout in a.err, waits (bounded) for its copies still in flight and returns.
+constexpr unsigned long long kFftWaitNs = 2000000000ull;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ unsigned long long now_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity)
+{
+    const unsigned long long t0 = now_ns();
+    while (true) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (now_ns() - t0 > kFftWaitNs) return false;
+    }
+}
+
+// The CTA's sequence of row pairs: items blockIdx.x, blockIdx.x + gridDim.x, ...; within an item
+// (two-row detectors) pairs (ra, ra + 1) from its first row in steps of two. One-row detectors:
+// item i is the pair of views (2 i, 2 i + 1), row 0.
+struct PairSeq {
+    int nv, nr, seg, nseg;
+    long long items;
+    bool quads, one_row;
+    __device__ __forceinline__ int first_row(long long it) const
+    {
+        const int s = static_cast<int>(it % nseg);
+        return quads ? -kQuadPad + s * seg : s * seg;
+    }
+    // end of the item's rows: quads: quad rows below it, pairs while ra <= end; plain: ra < end
+    __device__ __forceinline__ int row_end(long long it) const
+    {
+        const int r0 = first_row(it);
+        return quads ? min(r0 + seg, nr + kQuadPad) : min(r0 + seg, nr);
+    }
+    __device__ __forceinline__ bool in_item(long long it, int ra) const
+    {
+        return quads ? ra <= row_end(it) : ra < row_end(it);
+    }
+    __device__ __forceinline__ bool next(long long &it, int &ra) const
+    {
+        ra += 2;
+        if (!one_row && in_item(it, ra)) return true;
+        it += gridDim.x;
+        if (it >= items) return false;
+        ra = one_row ? 0 : first_row(it);
+        return true;
+    }
+};
+
+// Rows of pair (it, ra): views and rows of parts a and b; a view of -1 is a zero row.
+struct PairRows {
+    int va, ra, vb, rb;
+};
+__device__ __forceinline__ PairRows pair_rows(const PairSeq &q, long long it, int ra)
+{
+    PairRows p;
+    if (q.one_row) {
+        p.va = static_cast<int>(2 * it);
+        p.vb = (2 * it + 1 < q.nv) ? static_cast<int>(2 * it + 1) : -1;
+        p.ra = p.rb = 0;
+        return p;
+    }
+    const int v = static_cast<int>(it / q.nseg);
+    p.ra = ra;
+    p.rb = ra + 1;
+    p.va = (ra >= 0 && ra < q.nr) ? v : -1;
+    p.vb = (p.rb >= 0 && p.rb < q.nr && (q.quads || p.rb < q.row_end(it))) ? v : -1;
+    return p;
+}
+
+template <int LOG2L, int MODE, bool HALF, bool ONE_ROW, bool BULK>
 __global__ void __launch_bounds__(Fft<LOG2L>::T, fft_min_blocks<LOG2L>())
     filter_fft_kernel(FilterArgs a, int seg, int nseg)
 {
     using F = Fft<LOG2L>;
     constexpr int T = F::T;
-    extern __shared__ float2 smem[];
-    float2 *buf = smem;
+    constexpr bool quads = MODE != kOutPlainF32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    // layout: 2 mbarriers | exchange buffer (LP float2) | 3 padded rows | BULK: 2 stages x 2 rows
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw);
+    float2 *buf = reinterpret_cast<float2 *>(smem_raw + 16);
     const int rpitch = (a.nc + 2 * kQuadPad + 4) & ~3;  // padded shared row: 2 zeros, nc values, zeros
-    float *rows = reinterpret_cast<float *>(smem + F::LP);
+    float *rows = reinterpret_cast<float *>(buf + F::LP);
+    float *stage = rows + 3 * rpitch;                   // [2 stages][2 rows][nc] raw rows (BULK)
     const int t = threadIdx.x;
     Bases<LOG2L> bs;
     bs.init(t);
     for (int e = t; e < 3 * rpitch; e += T) rows[e] = 0.f;
+    if (BULK && t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bars)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bars + 1)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     __syncthreads();
     float2 x[16];
-    constexpr bool quads = MODE != kOutPlainF32;
 
-    if constexpr (ONE_ROW) {
-        // one-row detectors: rows of views (2 i, 2 i + 1) share a transform; each view's grid is
-        // written whole from its own row
-        const int npair = (a.nv + 1) / 2;
-        for (int pi = blockIdx.x; pi < npair; pi += gridDim.x) {
-            const int va = 2 * pi, vb = (2 * pi + 1 < a.nv) ? 2 * pi + 1 : -1;
-            filter_pair<LOG2L, HALF>(a, x, buf, t, bs, va, 0, vb, 0);
-            if constexpr (!quads) {
-#pragma unroll
-                for (int m = 0; m < 16; ++m) {
-                    const int c = t + T * m;
-                    if (c < a.nc) {
-                        static_cast<float *>(a.out)[static_cast<long long>(va) * a.nc + c] = x[m].x;
-                        if (vb >= 0) static_cast<float *>(a.out)[static_cast<long long>(vb) * a.nc + c] = -x[m].y;
-                    }
+    const long long items = ONE_ROW ? (a.nv + 1) / 2 : static_cast<long long>(a.nv) * nseg;
+    const PairSeq q{a.nv, a.nr, seg, nseg, items, quads, ONE_ROW};
+    const long long pix = static_cast<long long>(a.nr) * a.nc;
+    const uint32_t row_bytes = static_cast<uint32_t>(a.nc) * 4u;
+    int n_issued = 0, n_used = 0;  // pairs whose rows were copied into stages, and consumed
+
+    long long it = blockIdx.x;
+    int ra = (ONE_ROW || it >= items) ? 0 : q.first_row(it);
+    bool have = it < items;
+    long long cur_item = -1;
+    int prev = 0, sa = 1, sb = 2;  // shared row slots (quads): previous pair's row b, this pair's a and b
+    while (have) {
+        const PairRows pr = pair_rows(q, it, ra);
+        const bool present = pr.va >= 0 || pr.vb >= 0;
+        long long it_n = it;
+        int ra_n = ra;
+        const bool have_n = q.next(it_n, ra_n);
+        if constexpr (BULK) {
+            // thread 0 copies the rows of this pair (unless already in flight) and of the next one
+            for (int k = 0; k < 2; ++k) {
+                const PairRows pi = k == 0 ? pr : pair_rows(q, it_n, ra_n);
+                if (k == 0 ? !(present && n_issued == n_used) : !(have_n && (pi.va >= 0 || pi.vb >= 0))) continue;
+                if (t == 0) {
+                    const int st = n_issued & 1;
+                    const uint32_t bar = smem_addr(bars + st);
+                    const uint32_t bytes = row_bytes * ((pi.va >= 0) + (pi.vb >= 0));
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                                 : "memory");
+                    if (pi.va >= 0)
+                        asm volatile(
+                            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                            ::"r"(smem_addr(stage + (2 * st) * a.nc)),
+                            "l"(a.proj + pi.va * pix + static_cast<long long>(pi.ra) * a.nc), "r"(row_bytes), "r"(bar)
+                            : "memory");
+                    if (pi.vb >= 0)
+                        asm volatile(
+                            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                            ::"r"(smem_addr(stage + (2 * st + 1) * a.nc)),
+                            "l"(a.proj + pi.vb * pix + static_cast<long long>(pi.rb) * a.nc), "r"(row_bytes), "r"(bar)
+                            : "memory");
                 }
+                ++n_issued;
+            }
+        }
+        if (it != cur_item) {
+            cur_item = it;
+            prev = 0, sa = 1, sb = 2;
+        }
+        if (present) {
+            const float *pa = nullptr, *pb = nullptr;
+            if constexpr (BULK) {
+                const int st = n_used & 1;
+                const bool ok = bar_wait(smem_addr(bars + st), (n_used >> 1) & 1);
+                if (__syncthreads_or(!ok)) {
+                    // the copies did not arrive: report, wait (bounded) for those still in flight, stop
+                    if (t == 0) {
+                        if (a.err) atomicOr(a.err, kFftWaitTimeout);
+                        for (int k = n_used; k < n_issued; ++k) bar_wait(smem_addr(bars + (k & 1)), (k >> 1) & 1);
+                    }
+                    __syncthreads();
+                    return;
+                }
+                if (pr.va >= 0) pa = stage + (2 * st) * a.nc;
+                if (pr.vb >= 0) pb = stage + (2 * st + 1) * a.nc;
+                ++n_used;
             } else {
-                float *ya = rows, *yb = rows + rpitch;
-                const float sa = a.vscale ? a.vscale[va] : 1.f, sb = (a.vscale && vb >= 0) ? a.vscale[vb] : 1.f;
-                stage_rows<LOG2L>(x, ya, yb, sa, sb, a.nc, t);
-                __syncthreads();
-                for (int h = 0; h < 2; ++h) {
-                    const int v = h ? vb : va;
-                    if (v < 0) continue;
-                    const float *y = h ? yb : ya;
-                    if (a.t1d) {
-                        write_quads_t1d<MODE>(a, a.v0 + v, y, t, T);
-                    } else {
-                        write_quad_row<MODE>(a, a.v0 + v, -2, nullptr, nullptr, t, T);
-                        write_quad_row<MODE>(a, a.v0 + v, -1, nullptr, y, t, T);
-                        write_quad_row<MODE>(a, a.v0 + v, 0, y, nullptr, t, T);
-                        write_quad_row<MODE>(a, a.v0 + v, 1, nullptr, nullptr, t, T);
-                        write_quad_row<MODE>(a, a.v0 + v, 2, nullptr, nullptr, t, T);
-                    }
-                }
-                __syncthreads();  // the shared rows are rewritten by the next pair
+                if (pr.va >= 0) pa = a.proj + pr.va * pix + static_cast<long long>(pr.ra) * a.nc;
+                if (pr.vb >= 0) pb = a.proj + pr.vb * pix + static_cast<long long>(pr.rb) * a.nc;
             }
+            filter_pair<LOG2L, HALF>(a, x, buf, t, bs, pa, pb, pr.va, pr.ra, pr.vb, pr.rb);  // holds barriers
         }
-        return;
-    } else {
-    const long long items = static_cast<long long>(a.nv) * nseg;
-    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
-        const int v = static_cast<int>(it / nseg), s = static_cast<int>(it - static_cast<long long>(v) * nseg);
         if constexpr (!quads) {
-            // plain rows [r0, r1) of view v
-            const int r0 = s * seg, r1 = min(r0 + seg, a.nr);
-            for (int ra = r0; ra < r1; ra += 2) {
-                const int rb = ra + 1 < r1 ? ra + 1 : -1;
-                filter_pair<LOG2L, HALF>(a, x, buf, t, bs, v, ra, rb >= 0 ? v : -1, rb);
-                float *out = static_cast<float *>(a.out) + (static_cast<long long>(v) * a.nr + ra) * a.nc;
+            if (present) {
+                float *out = static_cast<float *>(a.out);
 #pragma unroll
                 for (int m = 0; m < 16; ++m) {
                     const int c = t + T * m;
                     if (c < a.nc) {
-                        out[c] = x[m].x;
-                        if (rb >= 0) out[a.nc + c] = -x[m].y;
+                        if (pr.va >= 0) out[pr.va * pix + static_cast<long long>(pr.ra) * a.nc + c] = x[m].x;
+                        if (pr.vb >= 0) out[pr.vb * pix + static_cast<long long>(pr.rb) * a.nc + c] = -x[m].y;
                     }
                 }
             }
-        } else {
-            // quad rows [q0, q1) of view v: quad row q needs detector rows q and q + 1
-            const int q0 = -kQuadPad + s * seg, q1 = min(q0 + seg, a.nr + kQuadPad);
-            const float sc = a.vscale ? a.vscale[v] : 1.f;
-            const int sv = a.v0 + v;
-            int prev = 0, sa = 1, sb = 2;  // shared row slots: previous pair's row b, this pair's a and b
-            for (int ra = q0; ra <= q1; ra += 2) {
-                const int rb = ra + 1;
-                float *ya = rows + sa * rpitch, *yb = rows + sb * rpitch;
-                if ((ra >= 0 && ra < a.nr) || (rb >= 0 && rb < a.nr)) {
-                    filter_pair<LOG2L, HALF>(a, x, buf, t, bs, v, ra, v, rb);  // holds barriers
-                    stage_rows<LOG2L>(x, ya, yb, sc, sc, a.nc, t);
+        } else if constexpr (ONE_ROW) {
+            // each view's grid is written whole from its own row
+            float *ya = rows, *yb = rows + rpitch;
+            const float s_a = a.vscale ? a.vscale[pr.va] : 1.f, s_b = (a.vscale && pr.vb >= 0) ? a.vscale[pr.vb] : 1.f;
+            stage_rows<LOG2L>(x, ya, yb, s_a, s_b, a.nc, t);
+            __syncthreads();
+            for (int h = 0; h < 2; ++h) {
+                const int v = h ? pr.vb : pr.va;
+                if (v < 0) continue;
+                const float *y = h ? yb : ya;
+                if (a.t1d) {
+                    write_quads_t1d<MODE>(a, a.v0 + v, y, t, T);
                 } else {
-                    __syncthreads();  // the previous pair's quad rows have been read from these slots
-                    for (int c = t; c < a.nc; c += T) ya[c + 2] = yb[c + 2] = 0.f;
+                    write_quad_row<MODE>(a, a.v0 + v, -2, nullptr, nullptr, t, T);
+                    write_quad_row<MODE>(a, a.v0 + v, -1, nullptr, y, t, T);
+                    write_quad_row<MODE>(a, a.v0 + v, 0, y, nullptr, t, T);
+                    write_quad_row<MODE>(a, a.v0 + v, 1, nullptr, nullptr, t, T);
+                    write_quad_row<MODE>(a, a.v0 + v, 2, nullptr, nullptr, t, T);
                 }
-                __syncthreads();
-                if (ra - 1 >= q0 && ra - 1 < q1) write_quad_row<MODE>(a, sv, ra - 1, rows + prev * rpitch, ya, t, T);
-                if (ra < q1) write_quad_row<MODE>(a, sv, ra, ya, yb, t, T);
-                // the next pair writes its rows into the slots of this pair's previous row and row a,
-                // after the barriers of its transforms
-                const int np = sb;
-                sb = sa;
-                sa = prev;
-                prev = np;
             }
+            __syncthreads();  // the shared rows are rewritten by the next pair
+        } else {
+            // quad rows [q0, q1) of view v: quad row r needs detector rows r and r + 1
+            const int v = static_cast<int>(it / nseg);
+            const int q0 = q.first_row(it), q1 = q.row_end(it);
+            const float sc = a.vscale ? a.vscale[v] : 1.f;
+            float *ya = rows + sa * rpitch, *yb = rows + sb * rpitch;
+            if (present) {
+                stage_rows<LOG2L>(x, ya, yb, sc, sc, a.nc, t);
+            } else {
+                __syncthreads();  // the previous pair's quad rows have been read from these slots
+                for (int c = t; c < a.nc; c += T) ya[c + 2] = yb[c + 2] = 0.f;
+            }
+            __syncthreads();
+            if (ra - 1 >= q0 && ra - 1 < q1) write_quad_row<MODE>(a, a.v0 + v, ra - 1, rows + prev * rpitch, ya, t, T);
+            if (ra < q1) write_quad_row<MODE>(a, a.v0 + v, ra, ya, yb, t, T);
+            // the next pair writes its rows into the slots of this pair's previous row and row a,
+            // after the barriers of its transforms (or the one above)
+            const int np = sb;
+            sb = sa;
+            sa = prev;
+            prev = np;
         }
-        __syncthreads();  // the next item's first pair rewrites the shared rows
-    }
+        it = it_n;
+        ra = ra_n;
+        have = have_n;
     }
 }
 
+// Shared memory of a CTA: two mbarriers, the exchange buffer, three padded rows and, with BULK,
+// two stages of two raw rows.
 template <int LOG2L>
-size_t smem_bytes_log2(int nc)
+size_t smem_bytes_log2(int nc, bool bulk)
 {
     const int rpitch = (nc + 2 * kQuadPad + 4) & ~3;
-    return static_cast<size_t>(Fft<LOG2L>::LP) * sizeof(float2) + 3 * static_cast<size_t>(rpitch) * sizeof(float);
+    return 16 + static_cast<size_t>(Fft<LOG2L>::LP) * sizeof(float2) + 3 * static_cast<size_t>(rpitch) * sizeof(float) +
+           (bulk ? 4 * static_cast<size_t>(nc) * sizeof(float) : 0);
 }
 
 template <int LOG2L, int MODE>
 void launch_mode(const FilterArgs &a, int num_sms, cudaStream_t s)
 {
     using F = Fft<LOG2L>;
-    const size_t smem = smem_bytes_log2<LOG2L>(a.nc);
+    // rows are copied by the tensor memory accelerator when they start on 16-byte boundaries and
+    // their length is a multiple of 16 bytes; otherwise each thread loads its columns directly
+    const bool bulk = a.nc % 4 == 0 && reinterpret_cast<uintptr_t>(a.proj) % 16 == 0;
+    const size_t smem = smem_bytes_log2<LOG2L>(a.nc, bulk);
     const bool half = a.nc <= F::L / 2;
     long long items;
     int seg = 0, nseg = 1;
@@ -588,11 +722,13 @@ void launch_mode(const FilterArgs &a, int num_sms, cudaStream_t s)
         kern<<<static_cast<unsigned>(grid), F::T, smem, s>>>(a, seg, nseg);
     };
     if (a.nr == 1) {
-        if (half) go(filter_fft_kernel<LOG2L, MODE, true, true>);
-        else go(filter_fft_kernel<LOG2L, MODE, false, true>);
+        if (!bulk) go(filter_fft_kernel<LOG2L, MODE, false, true, false>);
+        else if (half) go(filter_fft_kernel<LOG2L, MODE, true, true, true>);
+        else go(filter_fft_kernel<LOG2L, MODE, false, true, true>);
     } else {
-        if (half) go(filter_fft_kernel<LOG2L, MODE, true, false>);
-        else go(filter_fft_kernel<LOG2L, MODE, false, false>);
+        if (!bulk) go(filter_fft_kernel<LOG2L, MODE, false, false, false>);
+        else if (half) go(filter_fft_kernel<LOG2L, MODE, true, false, true>);
+        else go(filter_fft_kernel<LOG2L, MODE, false, false, true>);
     }
 }
 
@@ -634,25 +770,9 @@ __global__ void view_scales_kernel(const float *amax, int nv, float l1, float *v
 
 }  // namespace
 
-size_t filter_fft_smem_bytes(int L, int nc)
-{
-    switch (L) {
-        case 64: return smem_bytes_log2<6>(nc);
-        case 128: return smem_bytes_log2<7>(nc);
-        case 256: return smem_bytes_log2<8>(nc);
-        case 512: return smem_bytes_log2<9>(nc);
-        case 1024: return smem_bytes_log2<10>(nc);
-        case 2048: return smem_bytes_log2<11>(nc);
-        case 4096: return smem_bytes_log2<12>(nc);
-        default: return smem_bytes_log2<13>(nc);
-    }
-}
-
 void launch_filter_fft(const FilterArgs &a, int L, int num_sms, cudaStream_t s)
 {
     switch (L) {
-        case 64: launch_log2<6>(a, num_sms, s); break;
-        case 128: launch_log2<7>(a, num_sms, s); break;
         case 256: launch_log2<8>(a, num_sms, s); break;
         case 512: launch_log2<9>(a, num_sms, s); break;
         case 1024: launch_log2<10>(a, num_sms, s); break;

@@ -302,7 +302,7 @@ std::vector<double> parker_table(const gct_ct_geom &g, const RotationInfo &ri)
 unsigned fft_length(unsigned n)
 {
     const long need = std::max<long>(2L * n - 2 - n / 2, static_cast<long>(n) - 1 + n / 2);
-    unsigned L = 64;
+    unsigned L = 256;  // the FFT filter runs transforms of 256 to 8192 points
     while (static_cast<long>(L) <= need) L *= 2u;
     return L;
 }

@@ -19,14 +19,18 @@ struct FilterArgs {
     const float4 *fview = nullptr; // per view: (det_row_center, det_col_center, sdd, 0)
     const float *parker = nullptr; // [nv][nc]
     const float2 *H = nullptr;     // [L] filter spectrum, scaled by 1/L
-    const float2 *twiddle = nullptr; // [L] per-stage twiddles: tw[Ns + k] = exp(-2 pi i k / (R Ns))
     int mode = kOutPlainF32;
     void *out = nullptr;           // plain: rows of views [0, nv); quads: view 0 of the stack (quad_layout)
     int v0 = 0;                    // quads: stack index of the first view filtered
     int quarter = 0;               // quads: quad_layout's quarter
     const float *vscale = nullptr; // per-view output scale for quads (nullable = 1)
     int t1d = 0;                   // one-row detectors: write the transposed quad grid (t1d_quad_layout)
+    int *err = nullptr;            // plan status word: kFftWaitTimeout when an input copy timed out
 };
+
+// Status bits of the plan status word (gct_fdk_plan_check): Toeplitz GEMM pipeline stalls set
+// small codes (the stage), the FFT filter's input copies kFftWaitTimeout.
+constexpr int kFftWaitTimeout = 0x100;
 
 // Where view v's quad grid (qview entries) lives in a stack: view after view (quarter = 0), or,
 // for quarter-turn plans (quarter = nv / 4), with the four partner views v mod quarter + q quarter
@@ -51,9 +55,8 @@ __host__ __device__ inline void quad_layout(long long v, long long qview, int qu
 constexpr int kT1dPitch = 1 + 2 * kQuadPad;
 
 // Fused cosine + Parker weighting, zero padding, FFT convolution with the ramp filter and the
-// epilogue into the requested layout. L is the power-of-two FFT length.
+// epilogue into the requested layout. L is the power-of-two FFT length (256 to 8192).
 void launch_filter_fft(const FilterArgs &a, int L, int num_sms, cudaStream_t s);
-size_t filter_fft_smem_bytes(int L, int nc);
 
 // Per-view |max| of the raw projections (amax must be zeroed) and the FP16 power-of-two scale
 // that maps the bound amax * l1 (l1 = sum |taps|) below 2^14; writes vscale and 1/vscale.

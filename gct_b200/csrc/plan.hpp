@@ -108,7 +108,7 @@ struct gct_fdk_plan {
     DevBuf<int2> slice_views;
     DevBuf<float4> fview;
     DevBuf<float> parker;
-    DevBuf<float2> H, tw;
+    DevBuf<float2> H;
     DevBuf<float> coefs;
     DevBuf<unsigned char> work;
     // Toeplitz-GEMM filter: B = T^T split into 16-bit hi/lo pieces [Np][Kp] (BF16, or FP16 bit
@@ -119,7 +119,7 @@ struct gct_fdk_plan {
     DevBuf<float> grinv;             // FP16 form: per-row inverse scale of the GEMM rows
     float tap_inv = 1.f;             // FP16 form: inverse of the taps' power-of-two scale
     DevBuf<float> ybuf;
-    DevBuf<int> gemm_err;
+    DevBuf<int> gemm_err;  // kernel status word (GEMM pipeline and FFT input waits)
     // staging for gct_fdk_execute_host: projections, two device volumes (consecutive calls
     // alternate, so one call's download overlaps the next call's backprojection)
     DevBuf<float> host_proj, host_vol, host_vol2;
