@@ -358,8 +358,10 @@ __device__ __forceinline__ void write_quads_t1d(const FilterArgs &a, int v, cons
 }
 
 // Loads, weights and packs detector rows a (real part) and b (imaginary part) at columns t + T m;
-// NULL rows are zero. Columns at or past nc are zero.
-template <int LOG2L, bool HALF>
+// NULL rows are zero. Columns at or past nc are zero. SMEM: the rows are in shared memory (plain
+// loads), else in global memory (read-only loads through the non-coherent path, which accepts
+// global addresses only). The Parker rows ka, kb are always global.
+template <int LOG2L, bool HALF, bool SMEM>
 __device__ __forceinline__ void load_pair(const FilterArgs &a, float2 (&x)[16], const float *pa, const float *pb,
                                           const RowWeight &wa, const RowWeight &wb, const float *ka, const float *kb,
                                           int t)
@@ -373,8 +375,8 @@ __device__ __forceinline__ void load_pair(const FilterArgs &a, float2 (&x)[16], 
         const int c = t + T * m;
         if (c < a.nc) {
             const float k = __ldg(ka + c);
-            if (pa) x[m].x = __ldg(pa + c) * (wa.at(c) * k);
-            if (pb) x[m].y = __ldg(pb + c) * (wb.at(c) * (kb == ka ? k : __ldg(kb + c)));
+            if (pa) x[m].x = (SMEM ? pa[c] : __ldg(pa + c)) * (wa.at(c) * k);
+            if (pb) x[m].y = (SMEM ? pb[c] : __ldg(pb + c)) * (wb.at(c) * (kb == ka ? k : __ldg(kb + c)));
         }
     }
 }
@@ -393,10 +395,10 @@ __device__ __forceinline__ void spectrum(float2 (&x)[16], const float2 *__restri
     }
 }
 
-// Filters the detector rows pa (real part) and pb (imaginary part) (NULL = zero row; global or
-// shared memory) of views va and vb, rows ra and rb (for the weights), and leaves the filtered rows
+// Filters the detector rows pa (real part) and pb (imaginary part) (NULL = zero row; in shared
+// memory with SMEM, else global) of views va and vb, rows ra and rb (for the weights), and leaves the filtered rows
 // in natural order: row a in x[m].x, row b in -x[m].y at columns t + T m.
-template <int LOG2L, bool HALF>
+template <int LOG2L, bool HALF, bool SMEM>
 __device__ __forceinline__ void filter_pair(const FilterArgs &a, float2 (&x)[16], float2 *buf, int t,
                                             const Bases<LOG2L> &bs, const float *pa, const float *pb, int va, int ra,
                                             int vb, int rb)
@@ -407,7 +409,7 @@ __device__ __forceinline__ void filter_pair(const FilterArgs &a, float2 (&x)[16]
     const RowWeight wb = row_weight(a.kind, gb.x, gb.y, gb.z, a.du, a.dv, rb);
     const float *ka = a.parker + static_cast<long long>(ua) * a.nc;
     const float *kb = a.parker + static_cast<long long>(ub) * a.nc;
-    load_pair<LOG2L, HALF>(a, x, pa, pb, wa, wb, ka, kb, t);
+    load_pair<LOG2L, HALF, SMEM>(a, x, pa, pb, wa, wb, ka, kb, t);
     transform<LOG2L, HALF>(x, buf, t, bs);
     spectrum<LOG2L>(x, a.H, t);
     transform<LOG2L, false>(x, buf, t, bs);
@@ -615,7 +617,7 @@ __global__ void __launch_bounds__(Fft<LOG2L>::T, fft_min_blocks<LOG2L>())
                 if (pr.va >= 0) pa = a.proj + pr.va * pix + static_cast<long long>(pr.ra) * a.nc;
                 if (pr.vb >= 0) pb = a.proj + pr.vb * pix + static_cast<long long>(pr.rb) * a.nc;
             }
-            filter_pair<LOG2L, HALF>(a, x, buf, t, bs, pa, pb, pr.va, pr.ra, pr.vb, pr.rb);  // holds barriers
+            filter_pair<LOG2L, HALF, BULK>(a, x, buf, t, bs, pa, pb, pr.va, pr.ra, pr.vb, pr.rb);  // holds barriers
         }
         if constexpr (!quads) {
             if (present) {
