@@ -410,9 +410,13 @@ __device__ __forceinline__ void filter_pair(const FilterArgs &a, float2 (&x)[16]
     const float *ka = a.parker + static_cast<long long>(ua) * a.nc;
     const float *kb = a.parker + static_cast<long long>(ub) * a.nc;
     load_pair<LOG2L, HALF, SMEM>(a, x, pa, pb, wa, wb, ka, kb, t);
-    transform<LOG2L, HALF>(x, buf, t, bs);
-    spectrum<LOG2L>(x, a.H, t);
-    transform<LOG2L, false>(x, buf, t, bs);
+    // forward and inverse transform share one copy of the code (the fully unrolled transform is
+    // large enough that two copies miss in the instruction cache)
+#pragma unroll 1
+    for (int k = 0; k < 2; ++k) {
+        transform<LOG2L, false>(x, buf, t, bs);
+        if (k == 0) spectrum<LOG2L>(x, a.H, t);
+    }
 }
 
 // Writes the filtered rows held in x into two shared rows (padded: row[c + 2] = y[c]), scaled.
