@@ -25,8 +25,10 @@ from pathlib import Path
 import numpy as np
 
 REPO = Path(__file__).resolve().parents[1]
-sys.path.insert(0, str(REPO))
+# run as a script, this file's own directory would shadow the oracle package
+sys.path[:] = [p for p in sys.path if Path(p or ".").resolve() != Path(__file__).resolve().parent]
 sys.path.insert(0, str(REPO / "tests"))
+sys.path.insert(0, str(REPO))
 
 
 def main():
@@ -39,6 +41,9 @@ def main():
     ap.add_argument("--config", default="fan256", choices=sorted(bench.CONFIGS))
     ap.add_argument("--repeat", type=int, default=3)
     ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--split", action="store_true",
+                    help="also run the reference's stage sequence with an exact fetch (ref_fdk --bp exact) and "
+                         "report the texture's share of the engine/reference distance")
     args = ap.parse_args()
     cfg = bench.CONFIGS[args.config]
     cg, vg = bench.make_geometry(cfg)
@@ -60,12 +65,23 @@ def main():
         if res.returncode != 0:
             raise SystemExit(res.stderr[-2000:])
         ref = np.fromfile(out, dtype=np.float32).astype(np.float64).reshape(engine.shape)
+        ref_exact = None
+        if args.split:
+            r2 = subprocess.run([str(REPO / "oracle" / "_ref" / "ref_fdk"), "--bp", "exact", str(inp), str(out)],
+                                capture_output=True, text=True, timeout=3600)
+            if r2.returncode != 0:
+                raise SystemExit(r2.stderr[-2000:])
+            ref_exact = np.fromfile(out, dtype=np.float32).astype(np.float64).reshape(engine.shape)
     times = [float(m) for m in re.findall(r"reconstruct ([0-9.]+) ms", res.stderr)]
+    rel = lambda a, b: float(np.sqrt(np.mean((a - b) ** 2) / np.mean(b ** 2)))
     nx, ny, nz = cfg["n"]
     updates = nx * ny * nz * cfg["nv"]
     print(json.dumps({"workload": args.config, "reference_reconstruct_ms": times,
                       "reference_gups_best": updates / (min(times) / 1000.0) / 1e9,
-                      "rel_rms_vs_engine_fp32": float(np.sqrt(np.mean((ref - engine) ** 2) / np.mean(engine ** 2))),
+                      "rel_rms_vs_engine_fp32": rel(ref, engine),
+                      "split": None if ref_exact is None else {
+                          "lerp_part_ref_vs_ref_exact_fetch": rel(ref, ref_exact),
+                          "engine_fp32_vs_ref_exact_fetch": rel(engine, ref_exact)},
                       "note": "wall time of GCT::Recon::CUDA::reconstruct per call, host buffers in and out"}))
 
 
