@@ -14,7 +14,7 @@ replaced by a bilinear interpolation of the same filtered view in memory:
     4e-8 relative RMS, float32 rounding of the fetch);
   * ref(--bp exact) differs from ref(texture unit) by the weight quantisation alone: the lerp part
     (measured 7e-5 to 2.8e-4, larger on coarse grids);
-  * the engine differs from ref(--bp exact) by everything else: the gap north_star bounds by 1e-4
+  * the engine differs from ref(--bp exact) by everything else: the parity requirement bounds it by 1e-4
     relative RMS. Measured 0.8e-6 to 1.7e-5 (the largest on the fan-beam workload, where the
     reference's FP32 cuFFT filter of 4.6-high water-disk line integrals is itself 1.6e-5 from the
     FP64 oracle); asserted at 5e-5. The engine is within 3e-6 of the FP64 oracle throughout.
