@@ -354,6 +354,7 @@ void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float 
     qa.vscale = (mode == gct::kOutQuadF16) ? vscale : nullptr;
     qa.out = out;
     qa.quarter = quarter;
+    qa.err = p->gemm_err.p;
     gct::launch_quads_from_rows(qa, mode, p->num_sms, s);
     cuda_check(cudaGetLastError(), "quad kernel launch");
 }
@@ -506,6 +507,7 @@ void prepare_partners(gct_fdk_plan *p, const float *proj, const StackRef &st, in
     qa.vscale = f16 ? st.vscale : nullptr;
     qa.out = st.quads;
     qa.quarter = m;
+    qa.err = p->gemm_err.p;
     gct::launch_quads_partners(qa, f16 ? gct::kOutQuadF16 : gct::kOutQuadF32, p->num_sms, s);
     cuda_check(cudaGetLastError(), "partner quad kernel launch");
 }
@@ -941,6 +943,8 @@ gct_status gct_fdk_plan_check(gct_fdk_plan *plan)
             cuda_check(cudaMemset(plan->gemm_err.p, 0, sizeof(int)), "kernel status reset");
             if (e & gct::kFftWaitTimeout)
                 gct::fail(GCT_ERR_TIMEOUT, "FFT filter: a projection row copy did not arrive within 2 s");
+            if (e & gct::kQuadWaitTimeout)
+                gct::fail(GCT_ERR_TIMEOUT, "quad formation: a filtered row copy did not arrive within 2 s");
             gct::fail(GCT_ERR_TIMEOUT, "Toeplitz GEMM pipeline wait timed out (stage " + std::to_string(e) + ")");
         }
     });

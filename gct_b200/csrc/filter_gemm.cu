@@ -647,6 +647,142 @@ __global__ void quads_partners_kernel(QuadArgs a)
     }
 }
 
+// Quads from filtered FP32 rows, rolling form: a block takes (group b, segment of quad rows
+// [q0, q1)); a group is P views (P = 1: view b of the launch; P = 4: base view v0 + b and its three
+// quarter-turn partners, written as interleaved partner groups). Quad row q needs detector rows q
+// and q + 1, so the block keeps three shared rows per view and has one thread copy each new row
+// (cp.async.bulk, completion on the slot's mbarrier) while the current quad row is formed: every
+// filtered row is read once per segment instead of twice. Rows outside the detector are zeros
+// (no copy). Needs rows that start on 16-byte boundaries and hold a multiple of four floats; every
+// wait is bounded (2 s): on a timeout the block sets kQuadWaitTimeout in a.err, waits (bounded) for
+// its copies in flight and returns.
+template <int MODE, int P>
+__global__ void __launch_bounds__(256) quads_rows_kernel(QuadArgs a, int seg, int nseg)
+{
+    extern __shared__ __align__(16) unsigned char qsmem[];
+    uint64_t *qbars = reinterpret_cast<uint64_t *>(qsmem);        // one mbarrier per slot
+    const int rp = a.nc + 8;                                       // 4 zeros, nc values, 4 zeros
+    float *rows = reinterpret_cast<float *>(qsmem + 32);           // [3 slots][P][rp]
+    const int t = threadIdx.x, nt = blockDim.x;
+    for (int e = t; e < 3 * P * rp; e += nt) rows[e] = 0.f;
+    if (t == 0) {
+        for (int k = 0; k < 3; ++k) mbar_init(smem_u32(qbars + k), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const int qpitch = a.nc + 2 * kQuadPad, qrows = a.nr + 2 * kQuadPad;
+    const long long qview = static_cast<long long>(qrows) * qpitch;
+    const long long items = static_cast<long long>(a.nv) * nseg;
+    const uint32_t row_bytes = static_cast<uint32_t>(a.nc) * 4u;
+    // per slot (uniform over the block): copies completed so far (phase parity), row in the slot is zero
+    int done[3] = {0, 0, 0};
+    bool zero[3] = {true, true, true};
+    int inflight = 0, inflight_slot[3] = {0, 0, 0};
+    auto slot_of = [](int r) { return ((r % 3) + 3) % 3; };
+    // Y row of view k of group b at detector row r
+    auto yrow = [&](long long b, int k, int r) -> const float * {
+        const long long v = P == 1 ? b : a.v0 + b + static_cast<long long>(k) * a.quarter;
+        return a.Y + (v * a.nr + r) * static_cast<long long>(a.ldy);
+    };
+    auto issue = [&](long long b, int r) {
+        const int sl = slot_of(r);
+        zero[sl] = r < 0 || r >= a.nr;
+        if (zero[sl]) return;
+        if (t == 0) {
+            const uint32_t bar = smem_u32(qbars + sl);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(bar, row_bytes * P);
+#pragma unroll
+            for (int k = 0; k < P; ++k)
+                asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                             ::"r"(smem_u32(rows + (sl * P + k) * rp + 4)), "l"(yrow(b, k, r)), "r"(row_bytes),
+                             "r"(bar)
+                             : "memory");
+        }
+        inflight_slot[inflight++] = sl;
+    };
+    // waits for the copy into slot sl; false on timeout (uniform over the block)
+    auto wait_slot = [&](int sl) -> bool {
+        if (zero[sl]) return true;
+        const bool ok = mbar_wait(smem_u32(qbars + sl), static_cast<uint32_t>(done[sl] & 1));
+        if (ok) {
+            ++done[sl];
+            for (int k = 0; k < inflight; ++k)
+                if (inflight_slot[k] == sl) {
+                    inflight_slot[k] = inflight_slot[--inflight];
+                    break;
+                }
+        }
+        return !__syncthreads_or(!ok);
+    };
+    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+        const long long b = it / nseg;
+        const int q0 = -kQuadPad + static_cast<int>(it - b * nseg) * seg, q1 = min(q0 + seg, a.nr + kQuadPad);
+        float scl[P];
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            const long long v = P == 1 ? a.v0 + b : a.v0 + b + static_cast<long long>(k) * a.quarter;
+            scl[k] = a.vscale ? a.vscale[v] : 1.0f;
+        }
+        long long first;
+        int step;
+        if (P == 1) quad_layout(a.v0 + b, qview, a.quarter, first, step);
+        else first = (a.v0 + b) * qview * 4, step = 4;
+        issue(b, q0);
+        issue(b, q0 + 1);
+        for (int q = q0; q < q1; ++q) {
+            const bool ok = (q == q0 ? wait_slot(slot_of(q)) : true) && wait_slot(slot_of(q + 1));
+            if (!ok) {
+                if (t == 0) {
+                    atomicOr(a.err, kQuadWaitTimeout);
+                    for (int k = 0; k < inflight; ++k) {
+                        const int sl = inflight_slot[k];
+                        mbar_wait(smem_u32(qbars + sl), static_cast<uint32_t>(done[sl] & 1));
+                        ++done[sl];
+                    }
+                }
+                __syncthreads();
+                return;
+            }
+            if (q + 2 <= q1) issue(b, q + 2);  // into the slot of row q - 1, read by the previous quad row
+            const int st = slot_of(q), sb = slot_of(q + 1);
+            const bool zt = zero[st], zb = zero[sb];
+            const long long qbase = first + static_cast<long long>(q + kQuadPad) * qpitch * step;
+            for (int cq = t; cq < qpitch; cq += nt) {
+                const int c = cq - kQuadPad;  // shared index c + 4: columns -2 .. nc + 2 fall on zeros outside
+                float4 g[P];
+#pragma unroll
+                for (int k = 0; k < P; ++k) {
+                    const float *top = rows + (st * P + k) * rp + 4, *bot = rows + (sb * P + k) * rp + 4;
+                    const float p00 = zt ? 0.f : scl[k] * top[c], p01 = zt ? 0.f : scl[k] * top[c + 1];
+                    const float p10 = zb ? 0.f : scl[k] * bot[c], p11 = zb ? 0.f : scl[k] * bot[c + 1];
+                    g[k] = quad_f32(p00, p01, p10, p11);
+                }
+                if constexpr (P == 4) {
+                    const long long at = qbase + static_cast<long long>(cq) * 4;
+                    if (MODE == kOutQuadF32) {
+                        float4 *o = static_cast<float4 *>(a.out) + at;
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) o[k] = g[k];
+                    } else {
+                        uint2 h[4];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) h[k] = quad_f16_of(g[k]);
+                        uint4 *o = reinterpret_cast<uint4 *>(static_cast<uint2 *>(a.out) + at);
+                        o[0] = make_uint4(h[0].x, h[0].y, h[1].x, h[1].y);
+                        o[1] = make_uint4(h[2].x, h[2].y, h[3].x, h[3].y);
+                    }
+                } else {
+                    const long long at = qbase + static_cast<long long>(cq) * step;
+                    if (MODE == kOutQuadF32) static_cast<float4 *>(a.out)[at] = g[0];
+                    else static_cast<uint2 *>(a.out)[at] = quad_f16_of(g[0]);
+                }
+            }
+            __syncthreads();  // the slot of row q is rewritten by the copy issued in the next quad row
+        }
+    }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -693,6 +829,30 @@ void launch_split(const SplitArgs &a, int num_sms, cudaStream_t s)
     else split_kernel<0><<<g, 256, 0, s>>>(a);
 }
 
+namespace {
+// The rolling kernel, when every row starts on a 16-byte boundary (rows of a multiple of four floats
+// from an aligned base) and a.err is set; false when it does not apply.
+template <int P>
+bool launch_quads_rows(const QuadArgs &a, int mode, int num_sms, cudaStream_t s)
+{
+    if (a.nc % 4 != 0 || a.ldy % 4 != 0 || reinterpret_cast<uintptr_t>(a.Y) % 16 != 0 || !a.err || a.nv <= 0)
+        return false;
+    const int seg = 32;
+    const int nseg = (a.nr + 2 * kQuadPad + seg - 1) / seg;
+    const size_t smem = 32 + 3 * static_cast<size_t>(P) * (a.nc + 8) * sizeof(float);
+    if (smem > 200 * 1024) return false;
+    long long grid = static_cast<long long>(a.nv) * nseg;
+    if (grid > static_cast<long long>(num_sms) * 32) grid = static_cast<long long>(num_sms) * 32;
+    auto go = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        kern<<<static_cast<unsigned>(grid), 256, smem, s>>>(a, seg, nseg);
+    };
+    if (mode == kOutQuadF32) go(quads_rows_kernel<kOutQuadF32, P>);
+    else go(quads_rows_kernel<kOutQuadF16, P>);
+    return true;
+}
+}  // namespace
+
 void launch_quads_from_rows(const QuadArgs &a, int mode, int num_sms, cudaStream_t s)
 {
     if (a.t1d) {
@@ -705,6 +865,7 @@ void launch_quads_from_rows(const QuadArgs &a, int mode, int num_sms, cudaStream
             quads_t1d_kernel<kOutQuadF16><<<static_cast<unsigned>(grid < 1 ? 1 : grid), 256, 0, s>>>(a);
         return;
     }
+    if (launch_quads_rows<1>(a, mode, num_sms, s)) return;
     long long grid = static_cast<long long>(a.nv) * (a.nr + 2 * kQuadPad);
     if (grid > static_cast<long long>(num_sms) * 32) grid = static_cast<long long>(num_sms) * 32;
     if (mode == kOutQuadF32)
@@ -715,6 +876,7 @@ void launch_quads_from_rows(const QuadArgs &a, int mode, int num_sms, cudaStream
 
 void launch_quads_partners(const QuadArgs &a, int mode, int num_sms, cudaStream_t s)
 {
+    if (launch_quads_rows<4>(a, mode, num_sms, s)) return;
     long long grid = static_cast<long long>(a.nv) * (a.nr + 2 * kQuadPad);
     if (grid > static_cast<long long>(num_sms) * 32) grid = static_cast<long long>(num_sms) * 32;
     if (mode == kOutQuadF32)

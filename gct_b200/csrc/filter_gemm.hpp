@@ -57,7 +57,9 @@ struct QuadArgs {
     void *out = nullptr;       // quads of the full stack
     int quarter = 0;           // quad_layout (kernels.hpp)
     int t1d = 0;               // one-row detector: transposed quad grid (kernels.hpp, kT1dPitch)
+    int *err = nullptr;        // plan status word: kQuadWaitTimeout when a row copy timed out
 };
+constexpr int kQuadWaitTimeout = 0x200;
 void launch_quads_from_rows(const QuadArgs &a, int mode, int num_sms, cudaStream_t s);
 // Quarter-turn stacks: the partner groups of base views [v0, v0 + nv) (quarter = nv of the stack
 // / 4), from rows of all views at their stack positions in Y.
