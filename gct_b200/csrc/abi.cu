@@ -269,15 +269,6 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
     // its row buffer already
     if (p->sym && !p->ybuf.p)
         p->ybuf.alloc(static_cast<size_t>(p->nv) * p->nr * p->nc, "filtered rows of quarter-turn stacks");
-    if (p->sym && p->opts.filter != GCT_FILTER_FFT) {
-        cuda_check(cudaStreamCreateWithFlags(&p->filt_stream, cudaStreamNonBlocking), "filter side stream");
-        for (cudaEvent_t *e : {&p->filt_fork, &p->filt_join})
-            cuda_check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "filter events");
-        for (int c = 0; c < gct_fdk_plan::kFiltChunks; ++c) {
-            cuda_check(cudaEventCreateWithFlags(&p->filt_split[c], cudaEventDisableTiming), "filter events");
-            cuda_check(cudaEventCreateWithFlags(&p->filt_gemm[c], cudaEventDisableTiming), "filter events");
-        }
-    }
     if (p->spiral) {
         // one slice per thread along z: each slice has its own window of views
         p->sym = 0;
@@ -299,14 +290,16 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
     p->by_sym = p->opts.block_y > 0 ? p->by : (vol3d ? (f16 ? 32 : 16) : 8);
 }
 
-// Split (cosine x Parker weighting, FP16/BF16 pieces) of views [vb, vb + vc); with fused_scales
-// (amax zeroed by the caller) the split also finds the view maxima and the scales follow it.
-void run_split(gct_fdk_plan *p, const float *proj, int vb, int vc, cudaStream_t s, const StackRef *fused_scales)
+// Toeplitz-GEMM form of run_filter: split, tcgen05 GEMM into FP32 rows, then quads (or the rows
+// themselves for the plain output).
+void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float *vscale, int mode, int quarter,
+                     int vb, int vc, cudaStream_t s, const StackRef *fused_scales)
 {
+    const long long row0 = static_cast<long long>(vb) * p->nr, rows = static_cast<long long>(vc) * p->nr;
     gct::SplitArgs sa;
     sa.proj = proj;
-    sa.row0 = static_cast<long long>(vb) * p->nr;
-    sa.rows = static_cast<long long>(vc) * p->nr;
+    sa.row0 = row0;
+    sa.rows = rows;
     sa.nr = p->nr;
     sa.nc = p->nc;
     sa.Kp = p->Kp;
@@ -328,12 +321,6 @@ void run_split(gct_fdk_plan *p, const float *proj, int vb, int vc, cudaStream_t 
                                 s);
         cuda_check(cudaGetLastError(), "view scale kernel");
     }
-}
-
-// Toeplitz GEMM of the split rows of views [vb + q range_views, + vc), q < nranges, into FP32 rows
-// at Y (view v's row r at Y + ((v - vb) nr + r) ldy, i.e. Y is the address of view vb's rows).
-void run_gemm(gct_fdk_plan *p, float *Y, int vb, int vc, int nranges, int range_views, cudaStream_t s)
-{
     gct::GemmLaunch gl;
     gl.xh = p->xh.p;
     gl.xl = p->xl.p;
@@ -348,29 +335,16 @@ void run_gemm(gct_fdk_plan *p, float *Y, int vb, int vc, int nranges, int range_
     gl.tl = p->tl.p;
     gl.Np = p->Np;
     gl.Kp = p->Kp;
-    gl.m_begin = vb * p->nr;
-    gl.M = vc * p->nr;
+    gl.m_begin = static_cast<int>(row0);
+    gl.M = static_cast<int>(rows);
     gl.N = p->nc;
-    gl.Y = Y;
+    gl.Y = (mode == gct::kOutPlainF32 ? static_cast<float *>(out) : p->ybuf.p) + row0 * p->nc;
     gl.ldy = p->nc;
     gl.err = p->gemm_err.p;
-    gl.nranges = nranges;
-    gl.range_stride = static_cast<long long>(range_views) * p->nr;
     cuda_check(gct::launch_toeplitz_gemm(gl, p->num_sms, s), "Toeplitz GEMM launch");
-}
-
-// Toeplitz-GEMM form of run_filter: split, tcgen05 GEMM into FP32 rows, then quads (or the rows
-// themselves for the plain output).
-void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float *vscale, int mode, int quarter,
-                     int vb, int vc, cudaStream_t s, const StackRef *fused_scales)
-{
-    const long long row0 = static_cast<long long>(vb) * p->nr;
-    run_split(p, proj, vb, vc, s, fused_scales);
-    float *Y = (mode == gct::kOutPlainF32 ? static_cast<float *>(out) : p->ybuf.p) + row0 * p->nc;
-    run_gemm(p, Y, vb, vc, 1, 0, s);
     if (mode == gct::kOutPlainF32) return;
     gct::QuadArgs qa;
-    qa.Y = Y;
+    qa.Y = gl.Y;
     qa.ldy = p->nc;
     qa.v0 = vb;
     qa.nv = vc;
@@ -517,52 +491,6 @@ void prepare_partners(gct_fdk_plan *p, const float *proj, const StackRef &st, in
     const bool f16 = p->opts.storage == GCT_STORAGE_F16;
     const bool whole = b == 0 && n == m;
     const bool fuse = f16 && p->opts.filter != GCT_FILTER_FFT;  // the split pass finds the maxima
-    constexpr int K = gct_fdk_plan::kFiltChunks;
-    if (p->filt_stream && p->opts.filter != GCT_FILTER_FFT && n >= 2 * K) {
-        // Pipeline over K chunks of base views. The side stream splits every chunk (its four
-        // partner ranges) and forms a chunk's partner quads once the chunk's GEMM is done; the
-        // GEMM of chunk c starts on s as soon as its split is done. The split and quad passes are
-        // memory-bound and need no shared memory, so their blocks run beside the persistent
-        // tensor-core GEMM (198 KB of shared memory per SM) instead of after it.
-        cudaStream_t a = p->filt_stream;
-        cuda_check(cudaEventRecord(p->filt_fork, s), "event record");
-        cuda_check(cudaStreamWaitEvent(a, p->filt_fork, 0), "stream wait");
-        int cb[K + 1];
-        for (int c = 0; c <= K; ++c) cb[c] = b + static_cast<int>(static_cast<long long>(n) * c / K);
-        for (int c = 0; c < K; ++c) {
-            const int vc = cb[c + 1] - cb[c];
-            for (int q = 0; q < 4; ++q) {
-                const int vb = cb[c] + q * m;
-                if (fuse) cuda_check(cudaMemsetAsync(st.amax + vb, 0, sizeof(float) * vc, a), "view maxima reset");
-                run_split(p, proj, vb, vc, a, fuse ? &st : nullptr);
-            }
-            cuda_check(cudaEventRecord(p->filt_split[c], a), "event record");
-        }
-        for (int c = 0; c < K; ++c) {
-            const int vc = cb[c + 1] - cb[c];
-            cuda_check(cudaStreamWaitEvent(s, p->filt_split[c], 0), "stream wait");
-            run_gemm(p, p->ybuf.p + static_cast<long long>(cb[c]) * p->nr * p->nc, cb[c], vc, 4, m, s);
-            cuda_check(cudaEventRecord(p->filt_gemm[c], s), "event record");
-            cuda_check(cudaStreamWaitEvent(a, p->filt_gemm[c], 0), "stream wait");
-            gct::QuadArgs qa;
-            qa.Y = p->ybuf.p;
-            qa.ldy = p->nc;
-            qa.v0 = cb[c];
-            qa.nv = vc;
-            qa.nr = p->nr;
-            qa.nc = p->nc;
-            qa.vscale = f16 ? st.vscale : nullptr;
-            qa.out = st.quads;
-            qa.quarter = m;
-            qa.err = p->gemm_err.p;
-            qa.lean = 1;
-            gct::launch_quads_partners(qa, f16 ? gct::kOutQuadF16 : gct::kOutQuadF32, p->num_sms, a);
-            cuda_check(cudaGetLastError(), "partner quad kernel launch");
-        }
-        cuda_check(cudaEventRecord(p->filt_join, a), "event record");
-        cuda_check(cudaStreamWaitEvent(s, p->filt_join, 0), "stream wait");
-        return;
-    }
     for (int q = 0; q < (whole ? 1 : 4); ++q) {
         const int vb = whole ? 0 : b + q * m, vc = whole ? p->nv : n;
         if (fuse) cuda_check(cudaMemsetAsync(st.amax + vb, 0, sizeof(float) * vc, s), "view maxima reset");

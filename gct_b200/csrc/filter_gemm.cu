@@ -146,16 +146,7 @@ struct GemmParams {
     int form;       // GemmForm
     const float *rinv;  // FP16 form: per-row inverse scale, indexed like the A rows
     int *err;       // set non-zero on a timed-out wait
-    int nranges;    // row ranges: range q is rows m_begin + q * range_stride + [0, M)
-    long long range_stride;
 };
-
-// Rows of M tile mt_all (over all ranges): the range and the tile's first row relative to m_begin.
-__device__ __forceinline__ long long tile_row0(const GemmParams &p, int mt_all)
-{
-    const int rq = mt_all / p.m_tiles, mt = mt_all - rq * p.m_tiles;
-    return static_cast<long long>(rq) * p.range_stride + static_cast<long long>(mt) * BM;
-}
 
 // K blocks of the band segments for the output tile starting at column n0: the rows k with
 // |c - k| <= kBand for some c in [n0, n0 + BN).
@@ -241,7 +232,7 @@ __global__ void __launch_bounds__(192, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
-    const int total = p.nranges * p.m_tiles * p.n_tiles;
+    const int total = p.m_tiles * p.n_tiles;
     const int kfull = full_segments(p.form) * p.num_kb, nbseg = band_segments(p.form);
     const uint32_t idesc = p.form == kGemmF16x2 ? kIdescF16 : kIdescBF16;
 
@@ -250,7 +241,7 @@ __global__ void __launch_bounds__(192, 1)
             int stage = 0;
             uint32_t phase = 0;
             for (int t = blockIdx.x; t < total && !*fail_flag; t += gridDim.x) {
-                const int m0 = p.m_begin + static_cast<int>(tile_row0(p, t / p.n_tiles)), n0 = (t % p.n_tiles) * BN;
+                const int m0 = p.m_begin + (t / p.n_tiles) * BM, n0 = (t % p.n_tiles) * BN;
                 int kb0, kb1;
                 band_blocks(p, n0, kb0, kb1);
                 const int nband = kb1 - kb0;
@@ -325,12 +316,10 @@ __global__ void __launch_bounds__(192, 1)
                 break;
             }
             tc_fence_after();
-            const int mt_l = mt % p.m_tiles;                 // tile within its range
-            const int rl = mt_l * BM + q * 32 + lane;        // row within the range
-            const long long row = tile_row0(p, mt) + q * 32 + lane;  // relative to m_begin
-            float *yrow = p.Y + row * p.ldy;
+            const int row = mt * BM + q * 32 + lane;  // relative to m_begin
+            float *yrow = p.Y + static_cast<long long>(row) * p.ldy;
             // FP16 form: undo the row and tap scales (powers of two, exact); 1 otherwise
-            const float rs = (p.rinv && rl < p.M) ? __ldg(p.rinv + p.m_begin + row) : 1.0f;
+            const float rs = (p.rinv && row < p.M) ? __ldg(p.rinv + p.m_begin + row) : 1.0f;
 #pragma unroll 1
             for (int ch = 0; ch < BN / 32; ++ch) {
                 uint32_t r[32];
@@ -338,7 +327,7 @@ __global__ void __launch_bounds__(192, 1)
                 GCT_LD32(r, taddr);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 const int c0 = n0 + ch * 32;
-                if (rl < p.M) {
+                if (row < p.M) {
                     if (c0 + 32 <= p.N && (p.ldy & 3) == 0) {
                         float4 *dst = reinterpret_cast<float4 *>(yrow + c0);
 #pragma unroll
@@ -887,7 +876,7 @@ void launch_quads_from_rows(const QuadArgs &a, int mode, int num_sms, cudaStream
 
 void launch_quads_partners(const QuadArgs &a, int mode, int num_sms, cudaStream_t s)
 {
-    if (!a.lean && launch_quads_rows<4>(a, mode, num_sms, s)) return;
+    if (launch_quads_rows<4>(a, mode, num_sms, s)) return;
     long long grid = static_cast<long long>(a.nv) * (a.nr + 2 * kQuadPad);
     if (grid > static_cast<long long>(num_sms) * 32) grid = static_cast<long long>(num_sms) * 32;
     if (mode == kOutQuadF32)
@@ -915,14 +904,12 @@ cudaError_t launch_toeplitz_gemm(const GemmLaunch &g, int num_sms, cudaStream_t 
     p.num_kb = g.Kp / BK;
     p.m_tiles = (g.M + BM - 1) / BM;
     p.n_tiles = g.Np / BN;
-    p.nranges = g.nranges < 1 ? 1 : g.nranges;
-    p.range_stride = g.range_stride;
     p.Y = g.Y;
     p.ldy = g.ldy;
     p.form = g.form;
     p.rinv = f16 ? g.rinv : nullptr;
     p.err = g.err;
-    const int tiles = p.nranges * p.m_tiles * p.n_tiles;
+    const int tiles = p.m_tiles * p.n_tiles;
     const int grid = tiles < num_sms ? tiles : num_sms;
     const size_t smem = toeplitz_gemm_smem_bytes();
     cudaError_t e = cudaFuncSetAttribute(toeplitz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -46,9 +46,6 @@ struct GemmLaunch {
     float *Y = nullptr;  // row m_begin + i at Y + i * ldy
     int ldy = 0;
     int *err = nullptr;
-    // several row ranges in one launch: range q is rows m_begin + q * range_stride + [0, M)
-    int nranges = 1;
-    long long range_stride = 0;
 };
 cudaError_t launch_toeplitz_gemm(const GemmLaunch &g, int num_sms, cudaStream_t s);
 
@@ -61,7 +58,6 @@ struct QuadArgs {
     int quarter = 0;           // quad_layout (kernels.hpp)
     int t1d = 0;               // one-row detector: transposed quad grid (kernels.hpp, kT1dPitch)
     int *err = nullptr;        // plan status word: kQuadWaitTimeout when a row copy timed out
-    int lean = 0;              // use the variant without shared memory (to run beside the GEMM)
 };
 constexpr int kQuadWaitTimeout = 0x200;
 void launch_quads_from_rows(const QuadArgs &a, int mode, int num_sms, cudaStream_t s);

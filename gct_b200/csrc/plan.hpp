@@ -120,13 +120,6 @@ struct gct_fdk_plan {
     float tap_inv = 1.f;             // FP16 form: inverse of the taps' power-of-two scale
     DevBuf<float> ybuf;
     DevBuf<int> gemm_err;  // kernel status word (GEMM pipeline and FFT input waits)
-    // quarter-turn stacks with the Toeplitz filter: a side stream that runs the split and quad
-    // passes of chunks of base views beside the GEMM of the neighbouring chunk, and its events
-    // (fork, per chunk: split done and GEMM done, join)
-    static constexpr int kFiltChunks = 4;
-    cudaStream_t filt_stream = nullptr;
-    cudaEvent_t filt_fork = nullptr, filt_join = nullptr;
-    cudaEvent_t filt_split[kFiltChunks] = {}, filt_gemm[kFiltChunks] = {};
     // staging for gct_fdk_execute_host: projections, two device volumes (consecutive calls
     // alternate, so one call's download overlaps the next call's backprojection)
     DevBuf<float> host_proj, host_vol, host_vol2;
@@ -151,13 +144,6 @@ struct gct_fdk_plan {
         for (cudaEvent_t e : stream_events)
             if (e) cudaEventDestroy(e);
         if (copy_stream) cudaStreamDestroy(copy_stream);
-        for (cudaEvent_t e : {filt_fork, filt_join})
-            if (e) cudaEventDestroy(e);
-        for (int c = 0; c < kFiltChunks; ++c) {
-            if (filt_split[c]) cudaEventDestroy(filt_split[c]);
-            if (filt_gemm[c]) cudaEventDestroy(filt_gemm[c]);
-        }
-        if (filt_stream) cudaStreamDestroy(filt_stream);
     }
 
     size_t quad_bytes() const { return opts.storage == GCT_STORAGE_F16 ? 8 : 16; }
