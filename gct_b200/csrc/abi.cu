@@ -290,16 +290,16 @@ void build_plan(gct_fdk_plan *p, const gct_ct_geom *g, const gct_vol_geom *vol,
     p->by_sym = p->opts.block_y > 0 ? p->by : (vol3d ? (f16 ? 32 : 16) : 8);
 }
 
-// Toeplitz-GEMM form of run_filter: split, tcgen05 GEMM into FP32 rows, then quads (or the rows
-// themselves for the plain output).
-void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float *vscale, int mode, int quarter,
-                     int vb, int vc, cudaStream_t s, const StackRef *fused_scales)
+// Weighting and split of the rows of views [vb, vb + vc) into the plan's A pieces (row order:
+// view-major, or partner-interleaved for `quarter` > 0). `fused_scales` (FP16 storage): the split
+// also finds the view maxima, and the view scales follow it.
+void split_rows(gct_fdk_plan *p, const float *proj, int vb, int vc, int quarter, cudaStream_t s,
+                const StackRef *fused_scales)
 {
-    const long long row0 = static_cast<long long>(vb) * p->nr, rows = static_cast<long long>(vc) * p->nr;
     gct::SplitArgs sa;
     sa.proj = proj;
-    sa.row0 = row0;
-    sa.rows = rows;
+    sa.row0 = static_cast<long long>(vb) * p->nr;
+    sa.rows = static_cast<long long>(vc) * p->nr;
     sa.nr = p->nr;
     sa.nc = p->nc;
     sa.Kp = p->Kp;
@@ -314,6 +314,7 @@ void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float 
     sa.amax = fused_scales ? fused_scales->amax : nullptr;
     sa.rinv = p->grinv.p;
     sa.tap_inv = p->tap_inv;
+    sa.quarter = quarter;
     gct::launch_split(sa, p->num_sms, s);
     cuda_check(cudaGetLastError(), "split kernel launch");
     if (fused_scales) {  // the split found the view maxima: scales before the quads are written
@@ -321,6 +322,11 @@ void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float 
                                 s);
         cuda_check(cudaGetLastError(), "view scale kernel");
     }
+}
+
+// The GEMM launch fields every form shares.
+gct::GemmLaunch gemm_launch(const gct_fdk_plan *p)
+{
     gct::GemmLaunch gl;
     gl.xh = p->xh.p;
     gl.xl = p->xl.p;
@@ -335,12 +341,23 @@ void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float 
     gl.tl = p->tl.p;
     gl.Np = p->Np;
     gl.Kp = p->Kp;
+    gl.N = p->nc;
+    gl.err = p->gemm_err.p;
+    return gl;
+}
+
+// Toeplitz-GEMM form of run_filter: split, tcgen05 GEMM into FP32 rows, then quads (or the rows
+// themselves for the plain output).
+void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float *vscale, int mode, int quarter,
+                     int vb, int vc, cudaStream_t s, const StackRef *fused_scales)
+{
+    const long long row0 = static_cast<long long>(vb) * p->nr, rows = static_cast<long long>(vc) * p->nr;
+    split_rows(p, proj, vb, vc, 0, s, fused_scales);
+    gct::GemmLaunch gl = gemm_launch(p);
     gl.m_begin = static_cast<int>(row0);
     gl.M = static_cast<int>(rows);
-    gl.N = p->nc;
     gl.Y = (mode == gct::kOutPlainF32 ? static_cast<float *>(out) : p->ybuf.p) + row0 * p->nc;
     gl.ldy = p->nc;
-    gl.err = p->gemm_err.p;
     cuda_check(gct::launch_toeplitz_gemm(gl, p->num_sms, s), "Toeplitz GEMM launch");
     if (mode == gct::kOutPlainF32) return;
     gct::QuadArgs qa;
@@ -491,6 +508,24 @@ void prepare_partners(gct_fdk_plan *p, const float *proj, const StackRef &st, in
     const bool f16 = p->opts.storage == GCT_STORAGE_F16;
     const bool whole = b == 0 && n == m;
     const bool fuse = f16 && p->opts.filter != GCT_FILTER_FFT;  // the split pass finds the maxima
+    if (fuse) {
+        // FP16 quads from the Toeplitz GEMM: rows split in partner-interleaved order (with the view
+        // maxima and scales), then one GEMM whose epilogue writes the partner groups
+        for (int q = 0; q < (whole ? 1 : 4); ++q) {
+            const int vb = whole ? 0 : b + q * m, vc = whole ? p->nv : n;
+            cuda_check(cudaMemsetAsync(st.amax + vb, 0, sizeof(float) * vc, s), "view maxima reset");
+            split_rows(p, proj, vb, vc, m, s, &st);
+        }
+        gct::GemmLaunch gl = gemm_launch(p);
+        gl.quads = st.quads;
+        gl.vscale = st.vscale;
+        gl.quarter = m;
+        gl.nr = p->nr;
+        gl.b_begin = b;
+        gl.b_count = n;
+        cuda_check(gct::launch_toeplitz_gemm(gl, p->num_sms, s), "Toeplitz GEMM launch (partner quads)");
+        return;
+    }
     for (int q = 0; q < (whole ? 1 : 4); ++q) {
         const int vb = whole ? 0 : b + q * m, vc = whole ? p->nv : n;
         if (fuse) cuda_check(cudaMemsetAsync(st.amax + vb, 0, sizeof(float) * vc, s), "view maxima reset");

@@ -146,7 +146,41 @@ struct GemmParams {
     int form;       // GemmForm
     const float *rinv;  // FP16 form: per-row inverse scale, indexed like the A rows
     int *err;       // set non-zero on a timed-out wait
+    // partner-quad epilogue (pq != 0): A rows partner-interleaved from row m_begin; M tile mb
+    // starts at A row m_begin + kPqStride mb and covers kPqRows + 1 detector-row positions (four
+    // partner rows each) of base views from b_begin, the last one only as the lower neighbour of
+    // the one before; `positions` = base views x nr
+    int pq;
+    uint2 *quads;          // FP16 quads of the stack (view 0), quad_layout with `quarter`
+    const float *vscale;   // per-view power-of-two scale of the stored values
+    int quarter, nr, qpitch, b_begin;
+    long long qview, positions;
 };
+
+// Partner-quad tiles: 32 positions x 4 partners = BM A rows, consecutive tiles overlapping by one
+// position, so every quad row's lower detector row lies in the same tile as its upper one.
+constexpr int kPqRows = BM / 4 - 1;
+constexpr int kPqStride = 4 * kPqRows;
+
+// Tile i of this CTA: (A row of its first row, first output column, N tile index); false past the
+// last. Row tiles: every tile of the grid in turn. Partner-quad tiles: whole M blocks per CTA with
+// their N tiles in order, so that one epilogue thread sees a row's columns left to right.
+__device__ __forceinline__ bool tile_at(const GemmParams &p, int i, int &m0, int &n0, int &mb)
+{
+    if (p.pq) {
+        mb = blockIdx.x + (i / p.n_tiles) * gridDim.x;
+        if (mb >= p.m_tiles) return false;
+        m0 = p.m_begin + mb * kPqStride;
+        n0 = (i % p.n_tiles) * BN;
+        return true;
+    }
+    const long long t = blockIdx.x + static_cast<long long>(i) * gridDim.x;
+    if (t >= static_cast<long long>(p.m_tiles) * p.n_tiles) return false;
+    mb = static_cast<int>(t / p.n_tiles);
+    m0 = p.m_begin + mb * BM;
+    n0 = static_cast<int>(t % p.n_tiles) * BN;
+    return true;
+}
 
 // K blocks of the band segments for the output tile starting at column n0: the rows k with
 // |c - k| <= kBand for some c in [n0, n0 + BN).
@@ -191,6 +225,139 @@ __device__ __forceinline__ void step_operands(const GemmParams &p, int ks, int k
     }
 }
 
+__device__ __forceinline__ void epilogue_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+// Quad column cq of quad row r of one partner (group index base + 4 cq) from its corner values,
+// with the zero rows around a view: row -1 (lower row = detector row 0) and -2 above the first
+// detector row, rows nr and nr + 1 below the last.
+__device__ __forceinline__ void pq_store(const GemmParams &p, long long base, int cq, float lt, float rt, float lb,
+                                         float rb, bool first_row, bool last_row)
+{
+    uint2 *o = p.quads + base + 4LL * cq;
+    const long long row = 4LL * p.qpitch;
+    *o = quad_f16(lt, rt, lb, rb);
+    if (first_row) {
+        o[-row] = quad_f16(0.f, 0.f, lt, rt);
+        o[-2 * row] = make_uint2(0u, 0u);
+    }
+    if (last_row) {
+        o[row] = make_uint2(0u, 0u);
+        o[2 * row] = make_uint2(0u, 0u);
+    }
+}
+
+// Partner-quad epilogue of the four epilogue warps (TMEM lane quadrant q). TMEM lane t of a tile
+// holds position t / 4 (partner t % 4) of the tile's kPqRows + 1 positions. Per 32-column chunk
+// each thread scales its row (FP16 row scale x view scale, both powers of two), takes the next
+// detector row of its partner from lane + 4 (a shuffle, or for lanes 28..31 the next quadrant's
+// first four lanes through shared memory), and writes the quads of its position: lanes 4i..4i+3
+// store one 32-byte partner group. The quad left of each chunk takes its left corners from the
+// previous chunk (the previous N tile of the same M block, same thread). Every decision to stop is
+// voted by all four warps, so the named barriers stay matched. Returns false on a timed-out wait.
+__device__ bool pq_epilogue(const GemmParams &p, uint32_t tmem_base, int q, int lane, uint32_t tfull0,
+                            uint32_t tempty0, float4 (*s_x)[4][4][9], int (*s_stop)[4], const volatile int *fail_flag)
+{
+    const int trow = q * 32 + lane, pl = trow >> 2, k = trow & 3;
+    int acc = 0, tile_i = 0;
+    uint32_t aphase = 0;
+    for (int mb = blockIdx.x; mb < p.m_tiles; mb += gridDim.x) {
+        const long long pos = static_cast<long long>(kPqRows) * mb + pl;
+        const bool have = pos < p.positions;
+        const int bl = have ? static_cast<int>(pos / p.nr) : 0;
+        const int r = have ? static_cast<int>(pos - static_cast<long long>(bl) * p.nr) : 0;
+        const bool writer = have && pl < kPqRows;
+        const bool first_row = r == 0, last_row = r == p.nr - 1;
+        const long long b = static_cast<long long>(p.b_begin) + bl;
+        float rs = 0.f;
+        if (have) {
+            const long long arow = static_cast<long long>(p.m_begin) + static_cast<long long>(kPqStride) * mb + trow;
+            rs = (p.rinv ? __ldg(p.rinv + arow) : 1.0f) * __ldg(p.vscale + b + static_cast<long long>(k) * p.quarter);
+        }
+        const long long base = (b * p.qview + static_cast<long long>(r + kQuadPad) * p.qpitch) * 4 + k;
+        float ct = 0.f, cb = 0.f;  // column c0 - 1 of this row and of the next one
+        for (int nt = 0; nt < p.n_tiles; ++nt, ++tile_i) {
+            const bool ok = mbar_wait(tfull0 + 8u * acc, aphase);
+            if (lane == 0) s_stop[tile_i & 1][q] = (!ok || *fail_flag) ? 1 : 0;
+            epilogue_bar();
+            const int *vote = s_stop[tile_i & 1];
+            if (vote[0] | vote[1] | vote[2] | vote[3]) return ok;
+            tc_fence_after();
+#pragma unroll 1
+            for (int ch = 0; ch < BN / 32; ++ch) {
+                uint32_t rr[32];
+                const uint32_t taddr =
+                    tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * BN + ch * 32);
+                GCT_LD32(rr, taddr);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                const int c0 = nt * BN + ch * 32;
+                float v[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) v[j] = c0 + j < p.N ? rs * __uint_as_float(rr[j]) : 0.f;
+                float4(*xb)[9] = s_x[ch & 1][q];
+                if (lane < 4) {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) xb[lane][j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+                }
+                epilogue_bar();
+                float bt[32];
+                if (lane >= 28) {
+                    const float4(*nb)[9] = s_x[ch & 1][(q + 1) & 3];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const float4 t4 = nb[lane - 28][j];
+                        bt[4 * j] = t4.x, bt[4 * j + 1] = t4.y, bt[4 * j + 2] = t4.z, bt[4 * j + 3] = t4.w;
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const float d = __shfl_down_sync(0xffffffffu, v[j], 4);
+                    if (lane < 28) bt[j] = d;
+                    if (last_row) bt[j] = 0.f;
+                }
+                if (writer) {
+                    const int lim = p.N + 3;  // last quad column
+                    if (c0 == 0) pq_store(p, base, 0, 0.f, 0.f, 0.f, 0.f, first_row, last_row);
+                    if (c0 + 32 <= lim && !first_row && !last_row) {
+                        // interior rows, whole chunk: quads of columns c0 - 1 .. c0 + 30, each sharing
+                        // its left sums with the quad before (the quad_f32 operations, unchanged)
+                        uint2 *o = p.quads + base + 4LL * (c0 + 1);
+                        float lp = ct + cb, cp = cb - ct;
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const float l = v[j] + bt[j], cc = bt[j] - v[j];
+                            o[4 * j] = quad_f16_of(make_float4(0.5f * lp, 0.5f * (l - lp), cp, cc - cp));
+                            lp = l;
+                            cp = cc;
+                        }
+                    } else {
+                        if (c0 + 1 <= lim) pq_store(p, base, c0 + 1, ct, v[0], cb, bt[0], first_row, last_row);
+#pragma unroll
+                        for (int j = 0; j < 31; ++j)
+                            if (c0 + 2 + j <= lim)
+                                pq_store(p, base, c0 + 2 + j, v[j], v[j + 1], bt[j], bt[j + 1], first_row, last_row);
+                    }
+                }
+                ct = v[31];
+                cb = bt[31];
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(tempty0 + 8u * acc);
+            if (++acc == 2) {
+                acc = 0;
+                aphase ^= 1;
+            }
+        }
+        // quad columns past the last tile (detector column n_tiles BN - 1 and the zero padding)
+        if (writer)
+            for (int cq = p.n_tiles * BN + 1; cq <= p.N + 3; ++cq) {
+                const bool edge = cq == p.n_tiles * BN + 1;
+                pq_store(p, base, cq, edge ? ct : 0.f, 0.f, edge ? cb : 0.f, 0.f, first_row, last_row);
+            }
+    }
+    return true;
+}
+
 __global__ void __launch_bounds__(192, 1)
     toeplitz_gemm_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                          const __grid_constant__ CUtensorMap mAll, const __grid_constant__ CUtensorMap mBh,
@@ -204,6 +371,10 @@ __global__ void __launch_bounds__(192, 1)
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 4);
     __shared__ int s_fail;
     const volatile int *fail_flag = &s_fail;  // re-read on every loop test
+    // partner-quad epilogue: first four rows' values of each TMEM lane quadrant (two buffers) and
+    // the per-tile stop votes of the four epilogue warps (two buffers)
+    __shared__ float4 s_x[2][4][4][9];
+    __shared__ int s_stop[2][4];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     auto full = [&](int s) { return smem_u32(bars + s); };
     auto empty = [&](int s) { return smem_u32(bars + STAGES + s); };
@@ -232,7 +403,6 @@ __global__ void __launch_bounds__(192, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
-    const int total = p.m_tiles * p.n_tiles;
     const int kfull = full_segments(p.form) * p.num_kb, nbseg = band_segments(p.form);
     const uint32_t idesc = p.form == kGemmF16x2 ? kIdescF16 : kIdescBF16;
 
@@ -240,8 +410,8 @@ __global__ void __launch_bounds__(192, 1)
         if (lane == 0) {  // TMA producer
             int stage = 0;
             uint32_t phase = 0;
-            for (int t = blockIdx.x; t < total && !*fail_flag; t += gridDim.x) {
-                const int m0 = p.m_begin + (t / p.n_tiles) * BM, n0 = (t % p.n_tiles) * BN;
+            int m0, n0, mb;
+            for (int i = 0; tile_at(p, i, m0, n0, mb) && !*fail_flag; ++i) {
                 int kb0, kb1;
                 band_blocks(p, n0, kb0, kb1);
                 const int nband = kb1 - kb0;
@@ -268,7 +438,8 @@ __global__ void __launch_bounds__(192, 1)
         if (lane == 0) {  // MMA issuer
             int stage = 0, acc = 0;
             uint32_t phase = 0, aphase = 0;
-            for (int t = blockIdx.x; t < total && !*fail_flag; t += gridDim.x) {
+            int m0, n0, mb;
+            for (int i = 0; tile_at(p, i, m0, n0, mb) && !*fail_flag; ++i) {
                 if (!mbar_wait(tempty(acc), aphase ^ 1)) {
                     atomicExch(&s_fail, 2);
                     break;
@@ -276,7 +447,7 @@ __global__ void __launch_bounds__(192, 1)
                 tc_fence_after();
                 const uint32_t d = tmem_base + static_cast<uint32_t>(acc * BN);
                 int kb0, kb1;
-                band_blocks(p, (t % p.n_tiles) * BN, kb0, kb1);
+                band_blocks(p, n0, kb0, kb1);
                 const int ksteps = kfull + nbseg * (kb1 - kb0);
                 bool ok = true;
                 for (int ks = 0; ks < ksteps; ++ks) {
@@ -305,12 +476,16 @@ __global__ void __launch_bounds__(192, 1)
                 }
             }
         }
+    } else if (p.pq) {  // epilogue warps 2..5, partner quads
+        const int q = warp & 3;
+        if (!pq_epilogue(p, tmem_base, q, lane, tfull(0), tempty(0), s_x, s_stop, fail_flag))
+            atomicExch(&s_fail, 4);
     } else {  // epilogue warps 2..5: TMEM lane quadrant (warp % 4)
         const int q = warp & 3;
         int acc = 0;
         uint32_t aphase = 0;
-        for (int t = blockIdx.x; t < total && !*fail_flag; t += gridDim.x) {
-            const int mt = t / p.n_tiles, n0 = (t % p.n_tiles) * BN;
+        int m0, n0, mt;
+        for (int i = 0; tile_at(p, i, m0, n0, mt) && !*fail_flag; ++i) {
             if (!mbar_wait(tfull(acc), aphase)) {
                 atomicExch(&s_fail, 4);
                 break;
@@ -505,16 +680,17 @@ __global__ void split_kernel(SplitArgs a)
     for (long long rl = warp0; rl < a.rows; rl += nwarps) {
         const long long row = a.row0 + rl;
         const int v = static_cast<int>(row / a.nr), r = static_cast<int>(row - static_cast<long long>(v) * a.nr);
+        const long long arow = a.quarter ? gemm_partner_row(v, r, a.nr, a.quarter) : row;  // A row
         const float4 gv = __ldg(&a.fview[v]);
         const RowWeight rw = row_weight(a.kind, gv.x, gv.y, gv.z, a.du, a.dv, r);
         const float *src = a.proj + row * a.nc;
         const float *pk = a.parker + static_cast<long long>(v) * a.nc;
-        uint2 *dh = reinterpret_cast<uint2 *>(a.xh + row * a.Kp);
-        uint2 *dl = reinterpret_cast<uint2 *>(a.xl + row * a.Kp);
-        uint2 *dll = a.xll ? reinterpret_cast<uint2 *>(a.xll + row * a.Kp) : nullptr;
+        uint2 *dh = reinterpret_cast<uint2 *>(a.xh + arow * a.Kp);
+        uint2 *dl = reinterpret_cast<uint2 *>(a.xl + arow * a.Kp);
+        uint2 *dll = a.xll ? reinterpret_cast<uint2 *>(a.xll + arow * a.Kp) : nullptr;
         float m = 0.f;
         if (NCH >= 0) {
-            split_f16_row<(NCH > 0 ? NCH : 0)>(a, row, src, pk, rw, vec, dh, dl, lane, m);
+            split_f16_row<(NCH > 0 ? NCH : 0)>(a, arow, src, pk, rw, vec, dh, dl, lane, m);
         } else {
             for (int k4 = lane; k4 < a.Kp / 4; k4 += 32) {
                 float x[4];
@@ -909,8 +1085,25 @@ cudaError_t launch_toeplitz_gemm(const GemmLaunch &g, int num_sms, cudaStream_t 
     p.form = g.form;
     p.rinv = f16 ? g.rinv : nullptr;
     p.err = g.err;
-    const int tiles = p.m_tiles * p.n_tiles;
-    const int grid = tiles < num_sms ? tiles : num_sms;
+    p.pq = g.quads ? 1 : 0;
+    p.quads = static_cast<uint2 *>(g.quads);
+    p.vscale = g.vscale;
+    p.quarter = g.quarter;
+    p.nr = g.nr;
+    p.qpitch = g.N + 2 * kQuadPad;
+    p.qview = static_cast<long long>(g.nr + 2 * kQuadPad) * p.qpitch;
+    p.b_begin = g.b_begin;
+    p.positions = static_cast<long long>(g.b_count) * g.nr;
+    if (p.pq) {
+        if (!g.vscale || g.quarter <= 0 || g.nr <= 0 || g.b_count <= 0 || g.b_begin < 0 ||
+            g.b_begin + g.b_count > g.quarter || static_cast<long long>(g.quarter) * 4 * g.nr != g.a_rows)
+            return cudaErrorInvalidValue;
+        p.m_begin = g.b_begin * g.nr * 4;
+        p.M = static_cast<int>(p.positions * 4);
+        p.m_tiles = static_cast<int>((p.positions + kPqRows - 1) / kPqRows);
+    }
+    const long long tiles = p.pq ? p.m_tiles : static_cast<long long>(p.m_tiles) * p.n_tiles;
+    const int grid = tiles < num_sms ? static_cast<int>(tiles) : num_sms;
     const size_t smem = toeplitz_gemm_smem_bytes();
     cudaError_t e = cudaFuncSetAttribute(toeplitz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));

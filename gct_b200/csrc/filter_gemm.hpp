@@ -30,6 +30,9 @@ struct SplitArgs {
     float *amax = nullptr;                       // per-view max |raw value| (zeroed by the caller), or NULL
     float *rinv = nullptr;                       // FP16 form: per-row 1 / (row scale x tap scale), [all rows]
     float tap_inv = 1.f;                         // FP16 form: 1 / tap scale (a power of two)
+    // quarter-turn stacks (quad_layout's quarter > 0): the pieces and rinv of view v's row r go to
+    // the partner-interleaved A row ((v mod quarter) nr + r) 4 + v div quarter (gemm_partner_row)
+    int quarter = 0;
 };
 void launch_split(const SplitArgs &a, int num_sms, cudaStream_t s);
 
@@ -46,7 +49,19 @@ struct GemmLaunch {
     float *Y = nullptr;  // row m_begin + i at Y + i * ldy
     int ldy = 0;
     int *err = nullptr;
+    // Partner-quad output (quarter > 0, A rows partner-interleaved): instead of FP32 rows the
+    // epilogue writes the FP16 quads of base views [b_begin, b_begin + b_count) and their three
+    // partners, in quad_layout order, into the stack `quads` (view 0 address) with the per-view
+    // scales vscale; m_begin / M are then ignored (taken from the base views).
+    void *quads = nullptr;
+    const float *vscale = nullptr;
+    int quarter = 0, nr = 0, b_begin = 0, b_count = 0;
 };
+// A row of view v's detector row r in a partner-interleaved GEMM (quarter > 0).
+__host__ __device__ inline long long gemm_partner_row(long long v, int r, int nr, int quarter)
+{
+    return ((v % quarter) * nr + r) * 4 + v / quarter;
+}
 cudaError_t launch_toeplitz_gemm(const GemmLaunch &g, int num_sms, cudaStream_t s);
 
 struct QuadArgs {

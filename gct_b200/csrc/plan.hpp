@@ -188,8 +188,9 @@ inline StackRef stack_of(const gct_fdk_plan *p, void *workspace, bool view_major
 void run_filter(gct_fdk_plan *p, const float *proj, void *out, const float *vscale, int mode, int quarter, int vb,
                 int vc, cudaStream_t s, const StackRef *fused_scales = nullptr);
 void prepare(gct_fdk_plan *p, const float *proj, const StackRef &st, int vb, int vc, cudaStream_t s);
-// Quarter-turn stacks (st.quarter > 0): base views [b, b + n) and their partners, through the
-// plan's FP32 row buffer and one coalesced pass that writes the partner groups.
+// Quarter-turn stacks (st.quarter > 0): base views [b, b + n) and their partners. FP16 storage
+// with a Toeplitz filter: one GEMM whose epilogue writes the partner groups; otherwise through the
+// plan's FP32 row buffer and one coalesced pass that writes them.
 void prepare_partners(gct_fdk_plan *p, const float *proj, const StackRef &st, int b, int n, cudaStream_t s);
 gct::BpArgs bp_args(const gct_fdk_plan *p, const StackRef &st, float *vol, int v_begin, int v_count);
 void run_backproject_sym(gct_fdk_plan *p, const StackRef &st, float *vol, int b_begin, int b_count,

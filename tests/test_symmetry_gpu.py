@@ -151,3 +151,71 @@ def test_toeplitz_filter_with_quarter_turns():
         p.check()
     ref = orc.fdk(case.og, case.ov, proj).reshape(got.shape)
     assert rel_rms(got, ref) <= 1e-3
+
+
+TOEPLITZ_FORMS = [g.FILTER_TOEPLITZ_F16X2, g.FILTER_TOEPLITZ_BF16X3, g.FILTER_TOEPLITZ_BF16X4]
+
+
+def _quads_from_rows(y, vscale, quarter):
+    """FP16 partner groups of a quarter-turn stack from FP32 filtered rows y [nv][nr][nc]: the
+    quad formula of the engine (quad (R, cq) from rows R - 2, R - 1 and columns cq - 2, cq - 1 of
+    the zero-padded view, values times the view's power-of-two scale, A C B D in FP16), arranged
+    [base view][quad row][quad column][partner][A, C, B, D] as the stack stores them."""
+    nv, nr, nc = y.shape
+    out = np.empty((quarter, nr + 4, nc + 4, 4, 4), np.float16)
+    for v in range(nv):
+        yp = np.zeros((nr + 5, nc + 5), np.float32)
+        yp[2:nr + 2, 2:nc + 2] = np.float32(vscale[v]) * y[v]
+        p00, p01 = yp[:nr + 4, :nc + 4], yp[:nr + 4, 1:nc + 5]
+        p10, p11 = yp[1:nr + 5, :nc + 4], yp[1:nr + 5, 1:nc + 5]
+        left, right = p00 + p10, p01 + p11
+        half = np.float32(0.5)
+        quad = np.stack([half * left, p10 - p00, half * (right - left), (p11 - p01) - (p10 - p00)], axis=-1)
+        out[v % quarter, :, :, v // quarter, :] = quad.astype(np.float16)
+    return out
+
+
+@pytest.mark.parametrize("filt", TOEPLITZ_FORMS)
+@pytest.mark.parametrize("kind,nc,nr", [("cone_flat", 96, 24), ("cone_flat", 254, 9), ("cone_cyl", 256, 5),
+                                        ("cone_flat", 300, 33), ("fan_line", 130, 1)])
+def test_gemm_partner_quads_are_the_quads_of_the_filtered_rows(kind, nc, nr, filt):
+    """FP16 quarter-turn stacks with a Toeplitz filter take their partner groups straight from the
+    GEMM's epilogue (TMEM -> quads). The stack must hold, bit for bit, the quads formed from the
+    same GEMM's plain filtered rows (gct_fdk_filter) with the view scales of the stack: the row and
+    view scales are powers of two, so the two orders of scaling round identically. Every entry of
+    the stack is written (the workspace starts as 0xFF bytes)."""
+    import torch
+    case = make_case(kind, nc=nc, nr=nr, n=32)
+    proj = oracle_projections(case)
+    with _plan(case, g.STORAGE_F16, filt=filt) as p:
+        assert p.quarter_turn != 0
+        nv = case.cg.num_views
+        dproj = torch.from_numpy(proj).cuda()
+        ws = torch.full((p.workspace_bytes,), 0xFF, dtype=torch.uint8, device="cuda")
+        p.prepare(dproj, workspace=ws)
+        rows = torch.empty((nv, case.cg.num_rows, case.cg.num_cols), dtype=torch.float32, device="cuda")
+        p.filter(dproj, rows)
+        p.check()
+        torch.cuda.synchronize()
+        wsb = ws.cpu().numpy()
+        quad_bytes = nv * (nr + 4) * (nc + 4) * 8
+        region = (quad_bytes + 255) // 256 * 256
+        vscale = wsb[region + 4 * nv:region + 8 * nv].view(np.float32)
+        got = wsb[:quad_bytes].view(np.uint16).reshape(nv // 4, nr + 4, nc + 4, 4, 4)
+        want = _quads_from_rows(rows.cpu().numpy(), vscale, nv // 4).view(np.uint16)
+        bad = np.argwhere(got != want)
+        assert bad.size == 0, f"{len(bad)} differing halves, first at {bad[:4].tolist()}"
+
+
+@pytest.mark.parametrize("filt", TOEPLITZ_FORMS)
+def test_gemm_partner_quads_in_chunks_match_whole(filt):
+    """The host-buffer path prepares base views in chunks (each with its partners, one GEMM each);
+    the volume equals the one-launch execute to the chunked sums' rounding."""
+    case = make_case("cone_flat", nv=240)
+    proj = oracle_projections(case)
+    with _plan(case, g.STORAGE_F16, filt=filt) as p:
+        dev = _execute(p, case, proj)
+        host = np.empty(case.vg.shape, np.float32)
+        p.execute_host(proj, host)
+        p.check()
+    assert rel_rms(host, dev) <= 1e-5
