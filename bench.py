@@ -601,9 +601,10 @@ def run_gct(args, cfg, rank, world, local_rank):
         "cpu_baseline": cpu,
         "e2e": e2e,
         "clocks": clocks,
-        # per mixed step: GEMM forms split (with the view maxima), view scales, GEMM, quads,
-        # backprojection; FFT: view maxima, view scales, FFT filter, (partner quads), backprojection
-        "gpu_launches": (5 if args.mixed_filter != "fft" or mixed_quarter_turn else 4) * args.steps,
+        # per mixed step: GEMM forms split (with the view maxima), view scales, GEMM (writing the
+        # partner quads of quarter-turn stacks itself), quads (view-major stacks), backprojection;
+        # FFT: view maxima, view scales, FFT filter, (partner quads), backprojection
+        "gpu_launches": (5 if (args.mixed_filter != "fft") != bool(mixed_quarter_turn) else 4) * args.steps,
         "mixed_filter": {"gemm16": "split-FP16 Toeplitz GEMM on tcgen05, 1 full term + 3 banded (rows scaled per row "
                                    "in two FP16 pieces, central taps in three, far taps' dropped parts folded into "
                                    "the central tap)",
