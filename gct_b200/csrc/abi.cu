@@ -354,6 +354,17 @@ void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float 
     const long long row0 = static_cast<long long>(vb) * p->nr, rows = static_cast<long long>(vc) * p->nr;
     split_rows(p, proj, vb, vc, 0, s, fused_scales);
     gct::GemmLaunch gl = gemm_launch(p);
+    if (mode == gct::kOutQuadF16 && quarter == 0 && !p->t1d && p->nc % 2 == 0 &&
+        reinterpret_cast<uintptr_t>(out) % 16 == 0) {
+        // view-major FP16 quads straight from the GEMM's epilogue
+        gl.quads = out;
+        gl.vscale = vscale;
+        gl.nr = p->nr;
+        gl.v_begin = vb;
+        gl.v_count = vc;
+        cuda_check(gct::launch_toeplitz_gemm(gl, p->num_sms, s), "Toeplitz GEMM launch (quads)");
+        return;
+    }
     gl.m_begin = static_cast<int>(row0);
     gl.M = static_cast<int>(rows);
     gl.Y = (mode == gct::kOutPlainF32 ? static_cast<float *>(out) : p->ybuf.p) + row0 * p->nc;
@@ -521,8 +532,8 @@ void prepare_partners(gct_fdk_plan *p, const float *proj, const StackRef &st, in
         gl.vscale = st.vscale;
         gl.quarter = m;
         gl.nr = p->nr;
-        gl.b_begin = b;
-        gl.b_count = n;
+        gl.v_begin = b;
+        gl.v_count = n;
         cuda_check(gct::launch_toeplitz_gemm(gl, p->num_sms, s), "Toeplitz GEMM launch (partner quads)");
         return;
     }

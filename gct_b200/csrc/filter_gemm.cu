@@ -146,31 +146,32 @@ struct GemmParams {
     int form;       // GemmForm
     const float *rinv;  // FP16 form: per-row inverse scale, indexed like the A rows
     int *err;       // set non-zero on a timed-out wait
-    // partner-quad epilogue (pq != 0): A rows partner-interleaved from row m_begin; M tile mb
-    // starts at A row m_begin + kPqStride mb and covers kPqRows + 1 detector-row positions (four
-    // partner rows each) of base views from b_begin, the last one only as the lower neighbour of
-    // the one before; `positions` = base views x nr
+    // quad epilogue (pq = P, the partner views per position: 4 for quarter-turn stacks with
+    // partner-interleaved A rows, 1 for view-major stacks): M tile mb starts at A row
+    // m_begin + pq_stride(P) mb and covers pq_rows(P) + 1 detector-row positions (P rows each) of
+    // views from v_begin (base views for P = 4), the last one only as the lower neighbour of the
+    // one before; `positions` = (base) views x nr
     int pq;
-    uint2 *quads;          // FP16 quads of the stack (view 0), quad_layout with `quarter`
+    uint2 *quads;          // FP16 quads of the stack (view 0), quad_layout with `quarter` (P = 4) or 0
     const float *vscale;   // per-view power-of-two scale of the stored values
-    int quarter, nr, qpitch, b_begin;
+    int quarter, nr, qpitch, v_begin;
     long long qview, positions;
 };
 
-// Partner-quad tiles: 32 positions x 4 partners = BM A rows, consecutive tiles overlapping by one
-// position, so every quad row's lower detector row lies in the same tile as its upper one.
-constexpr int kPqRows = BM / 4 - 1;
-constexpr int kPqStride = 4 * kPqRows;
+// Quad tiles: BM / P positions x P partner rows, consecutive tiles overlapping by one position, so
+// every quad row's lower detector row lies in the same tile as its upper one.
+__host__ __device__ constexpr int pq_rows(int P) { return BM / P - 1; }
+__host__ __device__ constexpr int pq_stride(int P) { return P * pq_rows(P); }
 
 // Tile i of this CTA: (A row of its first row, first output column, N tile index); false past the
-// last. Row tiles: every tile of the grid in turn. Partner-quad tiles: whole M blocks per CTA with
-// their N tiles in order, so that one epilogue thread sees a row's columns left to right.
+// last. Row tiles: every tile of the grid in turn. Quad tiles: whole M blocks per CTA with their N
+// tiles in order, so that one epilogue thread sees a row's columns left to right.
 __device__ __forceinline__ bool tile_at(const GemmParams &p, int i, int &m0, int &n0, int &mb)
 {
     if (p.pq) {
         mb = blockIdx.x + (i / p.n_tiles) * gridDim.x;
         if (mb >= p.m_tiles) return false;
-        m0 = p.m_begin + mb * kPqStride;
+        m0 = p.m_begin + mb * pq_stride(p.pq);
         n0 = (i % p.n_tiles) * BN;
         return true;
     }
@@ -227,14 +228,15 @@ __device__ __forceinline__ void step_operands(const GemmParams &p, int ks, int k
 
 __device__ __forceinline__ void epilogue_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
-// Quad column cq of quad row r of one partner (group index base + 4 cq) from its corner values,
-// with the zero rows around a view: row -1 (lower row = detector row 0) and -2 above the first
-// detector row, rows nr and nr + 1 below the last.
+// Quad column cq of quad row r of one partner (entry base + P cq) from its corner values, with
+// the zero rows around a view: row -1 (lower row = detector row 0) and -2 above the first detector
+// row, rows nr and nr + 1 below the last.
+template <int P>
 __device__ __forceinline__ void pq_store(const GemmParams &p, long long base, int cq, float lt, float rt, float lb,
                                          float rb, bool first_row, bool last_row)
 {
-    uint2 *o = p.quads + base + 4LL * cq;
-    const long long row = 4LL * p.qpitch;
+    uint2 *o = p.quads + base + static_cast<long long>(P) * cq;
+    const long long row = static_cast<long long>(P) * p.qpitch;
     *o = quad_f16(lt, rt, lb, rb);
     if (first_row) {
         o[-row] = quad_f16(0.f, 0.f, lt, rt);
@@ -246,35 +248,40 @@ __device__ __forceinline__ void pq_store(const GemmParams &p, long long base, in
     }
 }
 
-// Partner-quad epilogue of the four epilogue warps (TMEM lane quadrant q). TMEM lane t of a tile
-// holds position t / 4 (partner t % 4) of the tile's kPqRows + 1 positions. Per 32-column chunk
-// each thread scales its row (FP16 row scale x view scale, both powers of two), takes the next
-// detector row of its partner from lane + 4 (a shuffle, or for lanes 28..31 the next quadrant's
-// first four lanes through shared memory), and writes the quads of its position: lanes 4i..4i+3
-// store one 32-byte partner group. The quad left of each chunk takes its left corners from the
+// Quad epilogue of the four epilogue warps (TMEM lane quadrant q). TMEM lane t of a tile holds
+// position t / P (partner t % P) of the tile's pq_rows(P) + 1 positions. Per 32-column chunk each
+// thread scales its row (FP16 row scale x view scale, both powers of two), takes the next detector
+// row of its partner from lane + P (a shuffle, or for the last P lanes the next quadrant's first
+// P lanes through shared memory), and writes the quads of its position. P = 4: lanes 4i..4i+3
+// store one 32-byte partner group per quad column; P = 1: each thread stores its own quad row,
+// two quads per 16-byte store. Quads at a chunk's left edge take their left corners from the
 // previous chunk (the previous N tile of the same M block, same thread). Every decision to stop is
 // voted by all four warps, so the named barriers stay matched. Returns false on a timed-out wait.
+template <int P>
 __device__ bool pq_epilogue(const GemmParams &p, uint32_t tmem_base, int q, int lane, uint32_t tfull0,
                             uint32_t tempty0, float4 (*s_x)[4][4][9], int (*s_stop)[4], const volatile int *fail_flag)
 {
-    const int trow = q * 32 + lane, pl = trow >> 2, k = trow & 3;
+    constexpr int kRows = pq_rows(P);
+    const int trow = q * 32 + lane, pl = trow / P, k = trow % P;
     int acc = 0, tile_i = 0;
     uint32_t aphase = 0;
     for (int mb = blockIdx.x; mb < p.m_tiles; mb += gridDim.x) {
-        const long long pos = static_cast<long long>(kPqRows) * mb + pl;
+        const long long pos = static_cast<long long>(kRows) * mb + pl;
         const bool have = pos < p.positions;
-        const int bl = have ? static_cast<int>(pos / p.nr) : 0;
-        const int r = have ? static_cast<int>(pos - static_cast<long long>(bl) * p.nr) : 0;
-        const bool writer = have && pl < kPqRows;
+        const int vl = have ? static_cast<int>(pos / p.nr) : 0;
+        const int r = have ? static_cast<int>(pos - static_cast<long long>(vl) * p.nr) : 0;
+        const bool writer = have && pl < kRows;
         const bool first_row = r == 0, last_row = r == p.nr - 1;
-        const long long b = static_cast<long long>(p.b_begin) + bl;
+        const long long b = static_cast<long long>(p.v_begin) + vl;  // base view (P = 4) or view
         float rs = 0.f;
         if (have) {
-            const long long arow = static_cast<long long>(p.m_begin) + static_cast<long long>(kPqStride) * mb + trow;
+            const long long arow =
+                static_cast<long long>(p.m_begin) + static_cast<long long>(pq_stride(P)) * mb + trow;
             rs = (p.rinv ? __ldg(p.rinv + arow) : 1.0f) * __ldg(p.vscale + b + static_cast<long long>(k) * p.quarter);
         }
-        const long long base = (b * p.qview + static_cast<long long>(r + kQuadPad) * p.qpitch) * 4 + k;
-        float ct = 0.f, cb = 0.f;  // column c0 - 1 of this row and of the next one
+        const long long base = (b * p.qview + static_cast<long long>(r + kQuadPad) * p.qpitch) * P + k;
+        float ct = 0.f, cb = 0.f;    // column c0 - 1 of this row and of the next one
+        float ct2 = 0.f, cb2 = 0.f;  // column c0 - 2 (P = 1)
         for (int nt = 0; nt < p.n_tiles; ++nt, ++tile_i) {
             const bool ok = mbar_wait(tfull0 + 8u * acc, aphase);
             if (lane == 0) s_stop[tile_i & 1][q] = (!ok || *fail_flag) ? 1 : 0;
@@ -294,29 +301,29 @@ __device__ bool pq_epilogue(const GemmParams &p, uint32_t tmem_base, int q, int 
 #pragma unroll
                 for (int j = 0; j < 32; ++j) v[j] = c0 + j < p.N ? rs * __uint_as_float(rr[j]) : 0.f;
                 float4(*xb)[9] = s_x[ch & 1][q];
-                if (lane < 4) {
+                if (lane < P) {
 #pragma unroll
                     for (int j = 0; j < 8; ++j) xb[lane][j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
                 }
                 epilogue_bar();
                 float bt[32];
-                if (lane >= 28) {
+                if (lane >= 32 - P) {
                     const float4(*nb)[9] = s_x[ch & 1][(q + 1) & 3];
 #pragma unroll
                     for (int j = 0; j < 8; ++j) {
-                        const float4 t4 = nb[lane - 28][j];
+                        const float4 t4 = nb[lane - (32 - P)][j];
                         bt[4 * j] = t4.x, bt[4 * j + 1] = t4.y, bt[4 * j + 2] = t4.z, bt[4 * j + 3] = t4.w;
                     }
                 }
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
-                    const float d = __shfl_down_sync(0xffffffffu, v[j], 4);
-                    if (lane < 28) bt[j] = d;
+                    const float d = __shfl_down_sync(0xffffffffu, v[j], P);
+                    if (lane < 32 - P) bt[j] = d;
                     if (last_row) bt[j] = 0.f;
                 }
-                if (writer) {
-                    const int lim = p.N + 3;  // last quad column
-                    if (c0 == 0) pq_store(p, base, 0, 0.f, 0.f, 0.f, 0.f, first_row, last_row);
+                const int lim = p.N + 3;  // last quad column
+                if (writer && P == 4) {
+                    if (c0 == 0) pq_store<P>(p, base, 0, 0.f, 0.f, 0.f, 0.f, first_row, last_row);
                     if (c0 + 32 <= lim && !first_row && !last_row) {
                         // interior rows, whole chunk: quads of columns c0 - 1 .. c0 + 30, each sharing
                         // its left sums with the quad before (the quad_f32 operations, unchanged)
@@ -330,13 +337,48 @@ __device__ bool pq_epilogue(const GemmParams &p, uint32_t tmem_base, int q, int 
                             cp = cc;
                         }
                     } else {
-                        if (c0 + 1 <= lim) pq_store(p, base, c0 + 1, ct, v[0], cb, bt[0], first_row, last_row);
+                        if (c0 + 1 <= lim) pq_store<P>(p, base, c0 + 1, ct, v[0], cb, bt[0], first_row, last_row);
 #pragma unroll
                         for (int j = 0; j < 31; ++j)
                             if (c0 + 2 + j <= lim)
-                                pq_store(p, base, c0 + 2 + j, v[j], v[j + 1], bt[j], bt[j + 1], first_row, last_row);
+                                pq_store<P>(p, base, c0 + 2 + j, v[j], v[j + 1], bt[j], bt[j + 1], first_row, last_row);
+                    }
+                } else if (writer) {
+                    // P = 1: quad columns c0 .. c0 + 31 (detector columns c0 - 2 .. c0 + 30), so that a
+                    // pair of quads starts on a 16-byte boundary
+                    if (c0 + 31 <= lim && !first_row && !last_row) {
+                        uint4 *o = reinterpret_cast<uint4 *>(p.quads + base + c0);
+                        float lp = ct2 + cb2, cp = cb2 - ct2;  // column c0 - 2
+                        float l1 = ct + cb, c1 = cb - ct;      // column c0 - 1
+                        const uint2 q0 = quad_f16_of(make_float4(0.5f * lp, 0.5f * (l1 - lp), cp, c1 - cp));
+                        const float l2 = v[0] + bt[0], c2 = bt[0] - v[0];
+                        const uint2 q1 = quad_f16_of(make_float4(0.5f * l1, 0.5f * (l2 - l1), c1, c2 - c1));
+                        o[0] = make_uint4(q0.x, q0.y, q1.x, q1.y);
+                        lp = l2;
+                        cp = c2;
+#pragma unroll
+                        for (int j = 1; j < 16; ++j) {
+                            const float la = v[2 * j - 1] + bt[2 * j - 1], ca = bt[2 * j - 1] - v[2 * j - 1];
+                            const float lb = v[2 * j] + bt[2 * j], cb_ = bt[2 * j] - v[2 * j];
+                            const uint2 qa = quad_f16_of(make_float4(0.5f * lp, 0.5f * (la - lp), cp, ca - cp));
+                            const uint2 qb = quad_f16_of(make_float4(0.5f * la, 0.5f * (lb - la), ca, cb_ - ca));
+                            o[j] = make_uint4(qa.x, qa.y, qb.x, qb.y);
+                            lp = lb;
+                            cp = cb_;
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            if (c0 + j > lim) continue;
+                            const float lt = j == 0 ? ct2 : j == 1 ? ct : v[j - 2];
+                            const float lb = j == 0 ? cb2 : j == 1 ? cb : bt[j - 2];
+                            const float rt = j == 0 ? ct : v[j - 1], rb = j == 0 ? cb : bt[j - 1];
+                            pq_store<P>(p, base, c0 + j, lt, rt, lb, rb, first_row, last_row);
+                        }
                     }
                 }
+                ct2 = v[30];
+                cb2 = bt[30];
                 ct = v[31];
                 cb = bt[31];
             }
@@ -348,12 +390,17 @@ __device__ bool pq_epilogue(const GemmParams &p, uint32_t tmem_base, int q, int 
                 aphase ^= 1;
             }
         }
-        // quad columns past the last tile (detector column n_tiles BN - 1 and the zero padding)
-        if (writer)
-            for (int cq = p.n_tiles * BN + 1; cq <= p.N + 3; ++cq) {
-                const bool edge = cq == p.n_tiles * BN + 1;
-                pq_store(p, base, cq, edge ? ct : 0.f, 0.f, edge ? cb : 0.f, 0.f, first_row, last_row);
+        // quad columns past the last tile (the tile's last detector columns and the zero padding)
+        if (writer) {
+            const int np = p.n_tiles * BN;
+            for (int cq = P == 4 ? np + 1 : np; cq <= p.N + 3; ++cq) {
+                const int c = cq - 2;  // left detector column of the quad
+                const float lt = c == np - 2 ? ct2 : c == np - 1 ? ct : 0.f;
+                const float lb = c == np - 2 ? cb2 : c == np - 1 ? cb : 0.f;
+                const float rt = c == np - 2 ? ct : 0.f, rb = c == np - 2 ? cb : 0.f;
+                pq_store<P>(p, base, cq, lt, rt, lb, rb, first_row, last_row);
             }
+        }
     }
     return true;
 }
@@ -478,8 +525,9 @@ __global__ void __launch_bounds__(192, 1)
         }
     } else if (p.pq) {  // epilogue warps 2..5, partner quads
         const int q = warp & 3;
-        if (!pq_epilogue(p, tmem_base, q, lane, tfull(0), tempty(0), s_x, s_stop, fail_flag))
-            atomicExch(&s_fail, 4);
+        const bool ok = p.pq == 4 ? pq_epilogue<4>(p, tmem_base, q, lane, tfull(0), tempty(0), s_x, s_stop, fail_flag)
+                                  : pq_epilogue<1>(p, tmem_base, q, lane, tfull(0), tempty(0), s_x, s_stop, fail_flag);
+        if (!ok) atomicExch(&s_fail, 4);
     } else {  // epilogue warps 2..5: TMEM lane quadrant (warp % 4)
         const int q = warp & 3;
         int acc = 0;
@@ -1085,22 +1133,26 @@ cudaError_t launch_toeplitz_gemm(const GemmLaunch &g, int num_sms, cudaStream_t 
     p.form = g.form;
     p.rinv = f16 ? g.rinv : nullptr;
     p.err = g.err;
-    p.pq = g.quads ? 1 : 0;
+    p.pq = g.quads ? (g.quarter > 0 ? 4 : 1) : 0;
     p.quads = static_cast<uint2 *>(g.quads);
     p.vscale = g.vscale;
     p.quarter = g.quarter;
     p.nr = g.nr;
     p.qpitch = g.N + 2 * kQuadPad;
     p.qview = static_cast<long long>(g.nr + 2 * kQuadPad) * p.qpitch;
-    p.b_begin = g.b_begin;
-    p.positions = static_cast<long long>(g.b_count) * g.nr;
+    p.v_begin = g.v_begin;
+    p.positions = static_cast<long long>(g.v_count) * g.nr;
     if (p.pq) {
-        if (!g.vscale || g.quarter <= 0 || g.nr <= 0 || g.b_count <= 0 || g.b_begin < 0 ||
-            g.b_begin + g.b_count > g.quarter || static_cast<long long>(g.quarter) * 4 * g.nr != g.a_rows)
+        // partner stacks: base views of the quarter, A rows partner-interleaved; view-major
+        // stacks: views of the stack, an even quad pitch (pairs of quads on 16-byte boundaries)
+        const long long views = p.pq == 4 ? g.quarter : g.a_rows / (g.nr > 0 ? g.nr : 1);
+        if (!g.vscale || g.nr <= 0 || g.v_count <= 0 || g.v_begin < 0 || g.v_begin + g.v_count > views ||
+            (p.pq == 4 && static_cast<long long>(g.quarter) * 4 * g.nr != g.a_rows) ||
+            (p.pq == 1 && (p.qpitch % 2 != 0 || reinterpret_cast<uintptr_t>(g.quads) % 16 != 0)))
             return cudaErrorInvalidValue;
-        p.m_begin = g.b_begin * g.nr * 4;
-        p.M = static_cast<int>(p.positions * 4);
-        p.m_tiles = static_cast<int>((p.positions + kPqRows - 1) / kPqRows);
+        p.m_begin = g.v_begin * g.nr * p.pq;
+        p.M = static_cast<int>(p.positions * p.pq);
+        p.m_tiles = static_cast<int>((p.positions + pq_rows(p.pq) - 1) / pq_rows(p.pq));
     }
     const long long tiles = p.pq ? p.m_tiles : static_cast<long long>(p.m_tiles) * p.n_tiles;
     const int grid = tiles < num_sms ? static_cast<int>(tiles) : num_sms;

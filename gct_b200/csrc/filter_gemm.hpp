@@ -49,13 +49,14 @@ struct GemmLaunch {
     float *Y = nullptr;  // row m_begin + i at Y + i * ldy
     int ldy = 0;
     int *err = nullptr;
-    // Partner-quad output (quarter > 0, A rows partner-interleaved): instead of FP32 rows the
-    // epilogue writes the FP16 quads of base views [b_begin, b_begin + b_count) and their three
-    // partners, in quad_layout order, into the stack `quads` (view 0 address) with the per-view
-    // scales vscale; m_begin / M are then ignored (taken from the base views).
+    // Quad output (quads set): instead of FP32 rows the epilogue writes FP16 quads, in
+    // quad_layout order, into the stack `quads` (view 0 address) with the per-view scales vscale:
+    // quarter > 0 (A rows partner-interleaved): base views [v_begin, v_begin + v_count) and their
+    // three partners; quarter = 0: views [v_begin, v_begin + v_count) of a view-major stack (quad
+    // pitch nc + 4 even). m_begin / M are then ignored (taken from the views).
     void *quads = nullptr;
     const float *vscale = nullptr;
-    int quarter = 0, nr = 0, b_begin = 0, b_count = 0;
+    int quarter = 0, nr = 0, v_begin = 0, v_count = 0;
 };
 // A row of view v's detector row r in a partner-interleaved GEMM (quarter > 0).
 __host__ __device__ inline long long gemm_partner_row(long long v, int r, int nr, int quarter)

@@ -219,3 +219,35 @@ def test_gemm_partner_quads_in_chunks_match_whole(filt):
         p.execute_host(proj, host)
         p.check()
     assert rel_rms(host, dev) <= 1e-5
+
+
+@pytest.mark.parametrize("filt", TOEPLITZ_FORMS)
+@pytest.mark.parametrize("kind,nc,nr", [("cone_flat", 96, 24), ("cone_flat", 254, 9), ("cone_cyl", 300, 33),
+                                        ("fan_line", 130, 1), ("cone_flat", 97, 7)])
+def test_gemm_view_major_quads_are_the_quads_of_the_filtered_rows(kind, nc, nr, filt):
+    """FP16 stacks without quarter turns (view after view) take their quads straight from the GEMM's
+    epilogue too when the quad pitch nc + 4 is even (one thread per detector row, two quads per
+    16-byte store); an odd pitch (nc = 97) goes through FP32 rows and the quad pass. Either way the
+    stack holds, bit for bit, the quads of the plain filtered rows with the view scales."""
+    import torch
+    case = make_case(kind, nc=nc, nr=nr, n=32)
+    proj = oracle_projections(case)
+    with _plan(case, g.STORAGE_F16, sym=g.SYMMETRY_OFF, filt=filt) as p:
+        assert p.quarter_turn == 0
+        nv = case.cg.num_views
+        dproj = torch.from_numpy(proj).cuda()
+        ws = torch.full((p.workspace_bytes,), 0xFF, dtype=torch.uint8, device="cuda")
+        p.prepare(dproj, workspace=ws)
+        rows = torch.empty((nv, case.cg.num_rows, case.cg.num_cols), dtype=torch.float32, device="cuda")
+        p.filter(dproj, rows)
+        p.check()
+        torch.cuda.synchronize()
+        wsb = ws.cpu().numpy()
+        quad_bytes = nv * (nr + 4) * (nc + 4) * 8
+        region = (quad_bytes + 255) // 256 * 256
+        vscale = wsb[region + 4 * nv:region + 8 * nv].view(np.float32)
+        got = wsb[:quad_bytes].view(np.uint16).reshape(nv, nr + 4, nc + 4, 4)
+        # one partner group per view: the view-major stack is the partner layout with quarter = nv
+        want = _quads_from_rows(rows.cpu().numpy(), vscale, nv)[:, :, :, 0, :].view(np.uint16)
+        bad = np.argwhere(got != want)
+        assert bad.size == 0, f"{len(bad)} differing halves, first at {bad[:4].tolist()}"
