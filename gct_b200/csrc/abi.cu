@@ -355,7 +355,7 @@ void run_filter_gemm(gct_fdk_plan *p, const float *proj, void *out, const float 
     split_rows(p, proj, vb, vc, 0, s, fused_scales);
     gct::GemmLaunch gl = gemm_launch(p);
     if (mode == gct::kOutQuadF16 && quarter == 0 && !p->t1d && p->nc % 2 == 0 &&
-        reinterpret_cast<uintptr_t>(out) % 16 == 0) {
+        reinterpret_cast<uintptr_t>(out) % 16 == 0 && gct::gemm_quad_tiles(rows, 1) >= p->num_sms) {
         // view-major FP16 quads straight from the GEMM's epilogue
         gl.quads = out;
         gl.vscale = vscale;
@@ -449,29 +449,87 @@ gct::BpArgs bp_args(const gct_fdk_plan *p, const StackRef &st, float *vol, int v
     return ba;
 }
 
+namespace {
+// View chunk of a split backprojection of `views` views (0: no split): a one-voxel-deep image
+// whose launch of `blocks` blocks (`per_sm` resident per SM) fills less than one wave is split
+// into the most parts (chunks of at least 8 views) whose blocks fit two whole waves.
+int split_chunk(const gct_fdk_plan *p, long long blocks, int per_sm, int views)
+{
+    if (p->kz != 1 || p->spiral || p->t1d || blocks <= 0 || per_sm <= 0 || views < 16) return 0;
+    const long long wave = static_cast<long long>(p->num_sms) * per_sm;
+    if (blocks >= wave) return 0;
+    const long long parts = std::min<long long>(2 * wave / blocks, views / 8);
+    if (parts < 2) return 0;
+    return static_cast<int>((views + parts - 1) / parts);
+}
+
+// Launches ba (vol, accumulate) through partial images when `chunk` > 0.
+template <class Launch>
+void launch_split(gct_fdk_plan *p, gct::BpArgs ba, int chunk, cudaStream_t s, Launch go)
+{
+    if (chunk <= 0) {
+        go(ba);
+        return;
+    }
+    const int parts = (ba.v_count + chunk - 1) / chunk;
+    const long long n = static_cast<long long>(p->kx) * p->ky * p->kz;
+    if (p->bp_part.n < static_cast<size_t>(parts) * n)
+        p->bp_part.alloc(static_cast<size_t>(parts) * n, "partial images of a view-split backprojection");
+    float *vol = ba.vol;
+    const bool accumulate = ba.accumulate != 0;
+    ba.vol = p->bp_part.p;
+    ba.vchunk = chunk;
+    ba.vol_stride = n;
+    ba.accumulate = 0;
+    go(ba);
+    gct::launch_reduce_partials(p->bp_part.p, parts, n, vol, accumulate, s);
+    cuda_check(cudaGetLastError(), "partial image reduction");
+}
+}  // namespace
+
 void run_backproject(gct_fdk_plan *p, const StackRef &st, float *vol, int v_begin, int v_count,
-                     bool accumulate, cudaStream_t s)
+                     bool accumulate, cudaStream_t s, bool split)
 {
     if (st.quarter && v_begin == 0 && v_count == p->nv) {
-        run_backproject_sym(p, st, vol, 0, p->nv / 4, accumulate, s);
+        run_backproject_sym(p, st, vol, 0, p->nv / 4, accumulate, s, split);
         return;
     }
     gct::BpArgs ba = bp_args(p, st, vol, v_begin, v_count);
     ba.accumulate = accumulate ? 1 : 0;
-    gct::launch_backproject(ba, static_cast<int>(p->family), p->opts.storage, p->z_affine, p->zpt, p->bx,
-                            p->by, s);
-    cuda_check(cudaGetLastError(), "backprojection kernel launch");
+    const long long blocks = static_cast<long long>((p->kx + p->bx - 1) / p->bx) * ((p->ky + p->by - 1) / p->by);
+    const int chunk =
+        split ? split_chunk(p, blocks,
+                            gct::backproject_blocks_per_sm(ba, static_cast<int>(p->family), p->opts.storage,
+                                                           p->z_affine, false, p->zpt, p->bx * p->by),
+                            v_count)
+              : 0;
+    launch_split(p, ba, chunk, s, [&](const gct::BpArgs &b) {
+        gct::launch_backproject(b, static_cast<int>(p->family), p->opts.storage, p->z_affine, p->zpt, p->bx, p->by,
+                                s);
+        cuda_check(cudaGetLastError(), "backprojection kernel launch");
+    });
 }
 
 void run_backproject_sym(gct_fdk_plan *p, const StackRef &st, float *vol, int b_begin, int b_count,
-                         bool accumulate, cudaStream_t s)
+                         bool accumulate, cudaStream_t s, bool split)
 {
     gct::BpArgs ba = bp_args(p, st, vol, b_begin, b_count);
     ba.accumulate = accumulate ? 1 : 0;
     ba.sym = p->sym;
-    gct::launch_backproject_sym(ba, static_cast<int>(p->family), p->opts.storage, p->zpt_sym, p->bx_sym, p->by_sym,
-                                s);
-    cuda_check(cudaGetLastError(), "backprojection kernel launch");
+    const int h = p->kx / 2;
+    const long long blocks =
+        static_cast<long long>((h + p->bx_sym - 1) / p->bx_sym) * ((h + p->by_sym - 1) / p->by_sym);
+    const int chunk =
+        split ? split_chunk(p, blocks,
+                            gct::backproject_blocks_per_sm(ba, static_cast<int>(p->family), p->opts.storage, true,
+                                                           true, p->zpt_sym, p->bx_sym * p->by_sym),
+                            b_count)
+              : 0;
+    launch_split(p, ba, chunk, s, [&](const gct::BpArgs &b) {
+        gct::launch_backproject_sym(b, static_cast<int>(p->family), p->opts.storage, p->zpt_sym, p->bx_sym,
+                                    p->by_sym, s);
+        cuda_check(cudaGetLastError(), "backprojection kernel launch");
+    });
 }
 
 void check_range(const gct_fdk_plan *p, uint32_t vb, uint32_t vc)
@@ -519,7 +577,7 @@ void prepare_partners(gct_fdk_plan *p, const float *proj, const StackRef &st, in
     const bool f16 = p->opts.storage == GCT_STORAGE_F16;
     const bool whole = b == 0 && n == m;
     const bool fuse = f16 && p->opts.filter != GCT_FILTER_FFT;  // the split pass finds the maxima
-    if (fuse) {
+    if (fuse && gct::gemm_quad_tiles(static_cast<long long>(n) * p->nr, 4) >= p->num_sms) {
         // FP16 quads from the Toeplitz GEMM: rows split in partner-interleaved order (with the view
         // maxima and scales), then one GEMM whose epilogue writes the partner groups
         for (int q = 0; q < (whole ? 1 : 4); ++q) {
@@ -692,7 +750,7 @@ void execute_host_budget(gct_fdk_plan *p, const float *proj_host, float *vol_hos
                                                              static_cast<uintptr_t>(vb) * pix * sizeof(float));
         prepare(p, proj0, st, vb, vc, s);
         cuda_check(cudaEventRecord(freed[slot], s), "event record");
-        run_backproject(p, st, p->host_vol.p, vb, vc, c > 0, s);
+        run_backproject(p, st, p->host_vol.p, vb, vc, c > 0, s, false);  // within the byte budget
     }
     cuda_check(cudaMemcpyAsync(vol_host, p->host_vol.p, sizeof(float) * vol_n, cudaMemcpyDeviceToHost, s),
                "volume download");
@@ -1121,7 +1179,7 @@ void execute_noalloc(gct_fdk_plan *p, const float *proj, float *vol, cudaStream_
             st.vinv = scales + 2 * chunk - vb;
         }
         prepare(p, proj, st, vb, vc, s);
-        run_backproject(p, st, vol, vb, vc, vb > 0, s);
+        run_backproject(p, st, vol, vb, vc, vb > 0, s, false);  // allocates nothing
     }
 }
 }  // namespace

@@ -336,6 +336,19 @@ __device__ __forceinline__ BlockBox block_box(const BpArgs &a, int i0, int j0, i
                     static_cast<float>(k0 + zpt - 1)};
 }
 
+// View-split launch (a.vchunk > 0): grid slice blockIdx.z takes its chunk of the view range and
+// its own partial image; true when the launch is split.
+__device__ __forceinline__ bool split_views(BpArgs &a)
+{
+    if (a.vchunk <= 0) return false;
+    const int z = blockIdx.z, b = z * a.vchunk;
+    a.v_begin += b;
+    a.v_count = max(0, min(a.vchunk, a.v_count - b));
+    a.vol += z * a.vol_stride;
+    a.accumulate = 0;
+    return true;
+}
+
 template <int FAMILY, class Q, int ZPT, bool ZAFFINE, int ES>
 __global__ void __launch_bounds__(256) bp_kernel(BpArgs a)
 {
@@ -344,10 +357,10 @@ __global__ void __launch_bounds__(256) bp_kernel(BpArgs a)
     __shared__ BlockBox s_box;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k0 = blockIdx.z * ZPT;
+    BpArgs la = a;
+    const int k0 = split_views(la) ? 0 : blockIdx.z * ZPT;
     if (threadIdx.x == 0 && threadIdx.y == 0)
         s_box = block_box(a, blockIdx.x * blockDim.x, blockIdx.y * blockDim.y, blockDim.x, blockDim.y, k0, ZPT);
-    BpArgs la = a;
     if (a.slice_views) {  // spiral scans: this slice's rotation of views (ZPT == 1, uniform per block)
         const int2 w = a.slice_views[k0 < a.nz ? k0 : a.nz - 1];
         const int b = max(w.x, a.v_begin), e = min(w.x + w.y, a.v_begin + a.v_count);
@@ -375,7 +388,8 @@ template <int FAMILY, class Q>
 void launch_q(const BpArgs &a, bool z_affine, int zpt, int bx, int by, cudaStream_t s)
 {
     const dim3 block(bx, by);
-    const dim3 grid((a.nx + bx - 1) / bx, (a.ny + by - 1) / by, (a.nz + zpt - 1) / zpt);
+    const unsigned gz = a.vchunk > 0 ? (a.v_count + a.vchunk - 1) / a.vchunk : (a.nz + zpt - 1) / zpt;
+    const dim3 grid((a.nx + bx - 1) / bx, (a.ny + by - 1) / by, gz);
     switch (zpt) {
         case 1: launch_zpt<FAMILY, Q, 1>(a, z_affine, grid, block, s); break;
         case 2: launch_zpt<FAMILY, Q, 2>(a, z_affine, grid, block, s); break;
@@ -658,9 +672,11 @@ __global__ void __launch_bounds__(256) bp_sym_kernel(BpArgs a)
     __shared__ float4 s_coef[kViewsPerChunk * kC / 4];
     __shared__ float4 s_w[kViewsPerChunk];  // weight scales of the four partners of each base view
     __shared__ int s_cls[kViewsPerChunk];   // box class of each of the block's four turned boxes, 2 bits each
-    sym_tile<FAMILY, Q, ZPT>(a, blockIdx.x * blockDim.x, blockIdx.y * blockDim.y, blockIdx.z * ZPT, blockDim.x,
-                             blockDim.y, threadIdx.y * blockDim.x + threadIdx.x, blockDim.x * blockDim.y,
-                             a.accumulate ? kBpAccumulate : kBpStore, s_coef, s_w, s_cls);
+    BpArgs la = a;
+    const int k0 = split_views(la) ? 0 : blockIdx.z * ZPT;
+    sym_tile<FAMILY, Q, ZPT>(la, blockIdx.x * blockDim.x, blockIdx.y * blockDim.y, k0, blockDim.x, blockDim.y,
+                             threadIdx.y * blockDim.x + threadIdx.x, blockDim.x * blockDim.y,
+                             la.accumulate ? kBpAccumulate : kBpStore, s_coef, s_w, s_cls);
 }
 
 template <int FAMILY, class Q>
@@ -668,7 +684,8 @@ void launch_sym_q(const BpArgs &a, int zpt, int bx, int by, cudaStream_t s)
 {
     const int h = a.nx / 2;
     const dim3 block(bx, by);
-    const dim3 grid((h + bx - 1) / bx, (h + by - 1) / by, (a.nz + zpt - 1) / zpt);
+    const unsigned gz = a.vchunk > 0 ? (a.v_count + a.vchunk - 1) / a.vchunk : (a.nz + zpt - 1) / zpt;
+    const dim3 grid((h + bx - 1) / bx, (h + by - 1) / by, gz);
     switch (zpt) {
         case 1: bp_sym_kernel<FAMILY, Q, 1><<<grid, block, 0, s>>>(a); break;
         case 2: bp_sym_kernel<FAMILY, Q, 2><<<grid, block, 0, s>>>(a); break;
@@ -800,7 +817,66 @@ __global__ void __launch_bounds__(kQueueThreads, 2)
     }
 }
 
+__global__ void reduce_partials_kernel(const float *__restrict__ part, int nparts, long long n, float *vol,
+                                       int accumulate)
+{
+    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        float t = accumulate ? vol[i] : 0.f;
+        for (int c = 0; c < nparts; ++c) t += __ldg(part + c * n + i);
+        vol[i] = t;
+    }
+}
+
 }  // namespace
+
+namespace {
+template <class K>
+int occupancy(K kern, int threads)
+{
+    int n = 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, 0) == cudaSuccess ? n : 0;
+}
+template <int FAMILY, class Q, int ZPT>
+int occupancy_zpt(const BpArgs &a, bool z_affine, bool sym, int threads)
+{
+    if (sym) return occupancy(bp_sym_kernel<FAMILY, Q, ZPT>, threads);
+    if (a.quarter) return occupancy(bp_kernel<FAMILY, Q, ZPT, true, 4>, threads);
+    if (z_affine || FAMILY == 0) return occupancy(bp_kernel<FAMILY, Q, ZPT, true, 1>, threads);
+    return occupancy(bp_kernel<FAMILY, Q, ZPT, false, 1>, threads);
+}
+template <int FAMILY, class Q>
+int occupancy_q(const BpArgs &a, bool z_affine, bool sym, int zpt, int threads)
+{
+    switch (zpt) {
+        case 1: return occupancy_zpt<FAMILY, Q, 1>(a, z_affine, sym, threads);
+        case 2: return occupancy_zpt<FAMILY, Q, 2>(a, z_affine, sym, threads);
+        case 4: return occupancy_zpt<FAMILY, Q, 4>(a, z_affine, sym, threads);
+        case 8: return occupancy_zpt<FAMILY, Q, 8>(a, z_affine, sym, threads);
+        default: return sym ? 0 : occupancy_zpt<FAMILY, Q, 16>(a, z_affine, sym, threads);
+    }
+}
+}  // namespace
+
+int backproject_blocks_per_sm(const BpArgs &a, int family, int storage, bool z_affine, bool sym, int zpt, int threads)
+{
+    if (storage == 0) {
+        if (family == 0) return occupancy_q<0, QuadF32>(a, z_affine, sym, zpt, threads);
+        if (family == 1) return occupancy_q<1, QuadF32>(a, z_affine, sym, zpt, threads);
+        return occupancy_q<2, QuadF32>(a, z_affine, sym, zpt, threads);
+    }
+    if (family == 0) return occupancy_q<0, QuadF16>(a, z_affine, sym, zpt, threads);
+    if (family == 1) return occupancy_q<1, QuadF16>(a, z_affine, sym, zpt, threads);
+    return occupancy_q<2, QuadF16>(a, z_affine, sym, zpt, threads);
+}
+
+void launch_reduce_partials(const float *part, int nparts, long long n, float *vol, bool accumulate, cudaStream_t s)
+{
+    long long grid = (n + 255) / 256;
+    if (grid > 148LL * 16) grid = 148LL * 16;
+    reduce_partials_kernel<<<static_cast<unsigned>(grid < 1 ? 1 : grid), 256, 0, s>>>(part, nparts, n, vol,
+                                                                                      accumulate ? 1 : 0);
+}
 
 void launch_backproject_sym(const BpArgs &a, int family, int storage, int zpt, int bx, int by, cudaStream_t s)
 {

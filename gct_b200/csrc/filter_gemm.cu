@@ -1037,6 +1037,7 @@ bool make_map(CUtensorMap *m, CUtensorMapDataType dt, const void *base, unsigned
 
 }  // namespace
 
+long long gemm_quad_tiles(long long positions, int P) { return (positions + pq_rows(P) - 1) / pq_rows(P); }
 int gemm_pad_k(int n) { return (n + BK - 1) / BK * BK; }
 int gemm_pad_n(int n) { return (n + BN - 1) / BN * BN; }
 size_t toeplitz_gemm_smem_bytes() { return STAGES * STAGE_BYTES + 1024 + 256; }

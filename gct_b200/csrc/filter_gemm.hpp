@@ -64,6 +64,9 @@ __host__ __device__ inline long long gemm_partner_row(long long v, int r, int nr
     return ((v % quarter) * nr + r) * 4 + v / quarter;
 }
 cudaError_t launch_toeplitz_gemm(const GemmLaunch &g, int num_sms, cudaStream_t s);
+// M tiles of a quad-epilogue GEMM over `positions` detector-row positions of P partner rows each
+// (one CTA takes whole M tiles, so fewer tiles than SMs leave SMs idle).
+long long gemm_quad_tiles(long long positions, int P);
 
 struct QuadArgs {
     const float *Y = nullptr;  // filtered rows of views [v0, v0 + nv), row stride ldy

@@ -83,7 +83,17 @@ struct BpArgs {
     // quarter-turn launches (quarter > 0): v_begin / v_count count base views, whose partners are
     // v + q * quarter (q = 1..3); sym (+1 / -1) is the turn that maps their voxel columns
     int sym = 0;
+    // view-split launches of one-voxel-deep images (vchunk > 0, nz == 1): grid slice z takes views
+    // [v_begin + z vchunk, + vchunk) and stores its sums at vol + z vol_stride (reduce_partials)
+    int vchunk = 0;
+    long long vol_stride = 0;
 };
+
+// Resident blocks per SM of the backprojection kernel a launch of these options would use
+// (sym: the quarter-turn kernel), for blocks of `threads` threads.
+int backproject_blocks_per_sm(const BpArgs &a, int family, int storage, bool z_affine, bool sym, int zpt, int threads);
+// vol[i] (+)= sum over c < nparts of part[c * n + i], in order of c (accumulate: add to vol).
+void launch_reduce_partials(const float *part, int nparts, long long n, float *vol, bool accumulate, cudaStream_t s);
 
 // Voxel-driven backprojection. family: 0 affine, 1 projective, 2 arc. storage: 0 f32, 1 f16.
 // z_affine selects the column kernel (u and the denominator constant along z).

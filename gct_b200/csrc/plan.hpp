@@ -109,6 +109,7 @@ struct gct_fdk_plan {
     DevBuf<float4> fview;
     DevBuf<float> parker;
     DevBuf<float2> H;
+    DevBuf<float> bp_part;  // partial images of view-split backprojections (run_backproject)
     DevBuf<float> coefs;
     DevBuf<unsigned char> work;
     // Toeplitz-GEMM filter: B = T^T split into 16-bit hi/lo pieces [Np][Kp] (BF16, or FP16 bit
@@ -193,9 +194,12 @@ void prepare(gct_fdk_plan *p, const float *proj, const StackRef &st, int vb, int
 // plan's FP32 row buffer and one coalesced pass that writes them.
 void prepare_partners(gct_fdk_plan *p, const float *proj, const StackRef &st, int b, int n, cudaStream_t s);
 gct::BpArgs bp_args(const gct_fdk_plan *p, const StackRef &st, float *vol, int v_begin, int v_count);
+// `split`: a one-voxel-deep image whose launch would leave most of the GPU idle is backprojected
+// in view chunks into partial images (plan-owned, allocated on first use) and summed in chunk
+// order; callers that must not allocate pass false.
 void run_backproject_sym(gct_fdk_plan *p, const StackRef &st, float *vol, int b_begin, int b_count,
-                         bool accumulate, cudaStream_t s);
+                         bool accumulate, cudaStream_t s, bool split = true);
 void run_backproject(gct_fdk_plan *p, const StackRef &st, float *vol, int v_begin, int v_count, bool accumulate,
-                     cudaStream_t s);
+                     cudaStream_t s, bool split = true);
 void check_range(const gct_fdk_plan *p, uint32_t vb, uint32_t vc);
 void *plan_workspace(gct_fdk_plan *p, void *workspace);

@@ -255,3 +255,39 @@ def test_async_host_calls_overlap_and_match(storage):
         plan.host_sync()
     for o, r in zip(outs, ref):
         assert np.array_equal(o, r)
+
+
+@pytest.mark.parametrize("storage,sym,tol", [(g.STORAGE_F32, g.SYMMETRY_OFF, 1e-6), (g.STORAGE_F16, g.SYMMETRY_OFF, 1e-6),
+                                             (g.STORAGE_F16, g.SYMMETRY_ON, 1e-5)])
+@pytest.mark.parametrize("kind", ["fan_line", "fan_arc"])
+def test_view_split_images_match_unsplit(kind, storage, sym, tol):
+    """One-voxel-deep images small enough to leave most of the GPU idle are backprojected in view
+    chunks into partial images that are summed in chunk order (execute, backproject). The
+    allocation-free entry point launches the plain kernel unsplit: with the same kernel the two
+    differ only by the grouping of the sum over views (relative RMS <= 1e-6); against the
+    quarter-turn kernel (symmetry on) by its FP32 coordinate rounding as well (<= 1e-5, the
+    tolerance of the quarter-turn tests). A split backproject with accumulate adds onto the image
+    already there (the split image itself, giving twice it)."""
+    import ctypes as C
+    import torch
+    from gct_b200 import _lib
+    case = make_case(kind, nv=360, n=64)
+    proj = torch.from_numpy(oracle_projections(case)).cuda()
+    with g.FdkPlan(case.cg, case.vg, opts=g.FdkOptions(storage=storage, symmetry=sym)) as plan:
+        assert (plan.quarter_turn != 0) == (sym == g.SYMMETRY_ON)
+        split = torch.full(case.vg.shape, float("nan"), dtype=torch.float32, device="cuda")
+        plan.execute(proj, split)
+        whole = torch.full(case.vg.shape, float("nan"), dtype=torch.float32, device="cuda")
+        lib = _lib.load()
+        _lib.check(lib.gct_fdk_execute_noalloc(plan._handle, C.c_void_p(proj.data_ptr()),
+                                               C.c_void_p(whole.data_ptr()),
+                                               C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        acc = split.clone()
+        plan.prepare(proj)
+        plan.backproject(acc, accumulate=True)
+        plan.check()
+        torch.cuda.synchronize()
+    s, w, a = split.cpu().numpy(), whole.cpu().numpy(), acc.cpu().numpy()
+    assert np.isfinite(s).all()
+    assert rel_rms(s, w) <= tol
+    assert rel_rms(a, 2.0 * s) <= 1e-6

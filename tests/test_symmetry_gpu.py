@@ -175,21 +175,28 @@ def _quads_from_rows(y, vscale, quarter):
     return out
 
 
+# Sizes: the quads come from the GEMM's epilogue when the launch has at least one M tile per SM
+# (148 on a B200): 31 positions per tile for partner stacks, 127 rows for view-major ones, so the
+# stacks below hold 120 views x 160 rows (or 18400 one-row views); the small cases take the
+# FP32-row path and must give the same stack.
+QUAD_CASES = [("cone_flat", 96, 160, 120), ("cone_flat", 254, 160, 120), ("cone_cyl", 256, 161, 120),
+              ("cone_flat", 300, 160, 120), ("fan_line", 130, 1, 18400), ("cone_flat", 96, 24, 120),
+              ("fan_line", 130, 1, 120)]
+
+
 @pytest.mark.parametrize("filt", TOEPLITZ_FORMS)
-@pytest.mark.parametrize("kind,nc,nr", [("cone_flat", 96, 24), ("cone_flat", 254, 9), ("cone_cyl", 256, 5),
-                                        ("cone_flat", 300, 33), ("fan_line", 130, 1)])
-def test_gemm_partner_quads_are_the_quads_of_the_filtered_rows(kind, nc, nr, filt):
+@pytest.mark.parametrize("kind,nc,nr,nv", QUAD_CASES)
+def test_gemm_partner_quads_are_the_quads_of_the_filtered_rows(kind, nc, nr, nv, filt):
     """FP16 quarter-turn stacks with a Toeplitz filter take their partner groups straight from the
     GEMM's epilogue (TMEM -> quads). The stack must hold, bit for bit, the quads formed from the
     same GEMM's plain filtered rows (gct_fdk_filter) with the view scales of the stack: the row and
     view scales are powers of two, so the two orders of scaling round identically. Every entry of
     the stack is written (the workspace starts as 0xFF bytes)."""
     import torch
-    case = make_case(kind, nc=nc, nr=nr, n=32)
+    case = make_case(kind, nc=nc, nr=nr, n=32, nv=nv)
     proj = oracle_projections(case)
     with _plan(case, g.STORAGE_F16, filt=filt) as p:
         assert p.quarter_turn != 0
-        nv = case.cg.num_views
         dproj = torch.from_numpy(proj).cuda()
         ws = torch.full((p.workspace_bytes,), 0xFF, dtype=torch.uint8, device="cuda")
         p.prepare(dproj, workspace=ws)
@@ -222,19 +229,18 @@ def test_gemm_partner_quads_in_chunks_match_whole(filt):
 
 
 @pytest.mark.parametrize("filt", TOEPLITZ_FORMS)
-@pytest.mark.parametrize("kind,nc,nr", [("cone_flat", 96, 24), ("cone_flat", 254, 9), ("cone_cyl", 300, 33),
-                                        ("fan_line", 130, 1), ("cone_flat", 97, 7)])
-def test_gemm_view_major_quads_are_the_quads_of_the_filtered_rows(kind, nc, nr, filt):
+@pytest.mark.parametrize("kind,nc,nr,nv", QUAD_CASES[:4] + [("fan_line", 130, 1, 18800), ("cone_flat", 97, 160, 120),
+                                                          ("cone_flat", 96, 24, 120)])
+def test_gemm_view_major_quads_are_the_quads_of_the_filtered_rows(kind, nc, nr, nv, filt):
     """FP16 stacks without quarter turns (view after view) take their quads straight from the GEMM's
-    epilogue too when the quad pitch nc + 4 is even (one thread per detector row, two quads per
+    epilogue too when the quad pitch nc + 4 is even and the launch is large enough (one thread per detector row, two quads per
     16-byte store); an odd pitch (nc = 97) goes through FP32 rows and the quad pass. Either way the
     stack holds, bit for bit, the quads of the plain filtered rows with the view scales."""
     import torch
-    case = make_case(kind, nc=nc, nr=nr, n=32)
+    case = make_case(kind, nc=nc, nr=nr, n=32, nv=nv)
     proj = oracle_projections(case)
     with _plan(case, g.STORAGE_F16, sym=g.SYMMETRY_OFF, filt=filt) as p:
         assert p.quarter_turn == 0
-        nv = case.cg.num_views
         dproj = torch.from_numpy(proj).cuda()
         ws = torch.full((p.workspace_bytes,), 0xFF, dtype=torch.uint8, device="cuda")
         p.prepare(dproj, workspace=ws)
