@@ -672,11 +672,25 @@ __global__ void __launch_bounds__(256) bp_sym_kernel(BpArgs a)
     __shared__ float4 s_coef[kViewsPerChunk * kC / 4];
     __shared__ float4 s_w[kViewsPerChunk];  // weight scales of the four partners of each base view
     __shared__ int s_cls[kViewsPerChunk];   // box class of each of the block's four turned boxes, 2 bits each
+    sym_tile<FAMILY, Q, ZPT>(a, blockIdx.x * blockDim.x, blockIdx.y * blockDim.y, blockIdx.z * ZPT, blockDim.x,
+                             blockDim.y, threadIdx.y * blockDim.x + threadIdx.x, blockDim.x * blockDim.y,
+                             a.accumulate ? kBpAccumulate : kBpStore, s_coef, s_w, s_cls);
+}
+
+// The view-split launch of bp_sym_kernel (a.vchunk > 0, one-voxel-deep images): its own kernel, so
+// that the whole-volume kernel keeps its register allocation (the local copy of the arguments
+// here took it from 128 to 102 registers, and 34.8 to 42.5 ms at 512^3 / 720 views).
+template <int FAMILY, class Q, int ZPT>
+__global__ void __launch_bounds__(256) bp_sym_split_kernel(BpArgs a)
+{
+    __shared__ float4 s_coef[kViewsPerChunk * kC / 4];
+    __shared__ float4 s_w[kViewsPerChunk];
+    __shared__ int s_cls[kViewsPerChunk];
     BpArgs la = a;
-    const int k0 = split_views(la) ? 0 : blockIdx.z * ZPT;
-    sym_tile<FAMILY, Q, ZPT>(la, blockIdx.x * blockDim.x, blockIdx.y * blockDim.y, k0, blockDim.x, blockDim.y,
-                             threadIdx.y * blockDim.x + threadIdx.x, blockDim.x * blockDim.y,
-                             la.accumulate ? kBpAccumulate : kBpStore, s_coef, s_w, s_cls);
+    split_views(la);
+    sym_tile<FAMILY, Q, ZPT>(la, blockIdx.x * blockDim.x, blockIdx.y * blockDim.y, 0, blockDim.x, blockDim.y,
+                             threadIdx.y * blockDim.x + threadIdx.x, blockDim.x * blockDim.y, kBpStore, s_coef, s_w,
+                             s_cls);
 }
 
 template <int FAMILY, class Q>
@@ -686,6 +700,15 @@ void launch_sym_q(const BpArgs &a, int zpt, int bx, int by, cudaStream_t s)
     const dim3 block(bx, by);
     const unsigned gz = a.vchunk > 0 ? (a.v_count + a.vchunk - 1) / a.vchunk : (a.nz + zpt - 1) / zpt;
     const dim3 grid((h + bx - 1) / bx, (h + by - 1) / by, gz);
+    if (a.vchunk > 0) {
+        switch (zpt) {
+            case 1: bp_sym_split_kernel<FAMILY, Q, 1><<<grid, block, 0, s>>>(a); break;
+            case 2: bp_sym_split_kernel<FAMILY, Q, 2><<<grid, block, 0, s>>>(a); break;
+            case 4: bp_sym_split_kernel<FAMILY, Q, 4><<<grid, block, 0, s>>>(a); break;
+            default: bp_sym_split_kernel<FAMILY, Q, 8><<<grid, block, 0, s>>>(a); break;
+        }
+        return;
+    }
     switch (zpt) {
         case 1: bp_sym_kernel<FAMILY, Q, 1><<<grid, block, 0, s>>>(a); break;
         case 2: bp_sym_kernel<FAMILY, Q, 2><<<grid, block, 0, s>>>(a); break;
@@ -840,7 +863,7 @@ int occupancy(K kern, int threads)
 template <int FAMILY, class Q, int ZPT>
 int occupancy_zpt(const BpArgs &a, bool z_affine, bool sym, int threads)
 {
-    if (sym) return occupancy(bp_sym_kernel<FAMILY, Q, ZPT>, threads);
+    if (sym) return occupancy(bp_sym_split_kernel<FAMILY, Q, ZPT>, threads);  // asked for view-split launches
     if (a.quarter) return occupancy(bp_kernel<FAMILY, Q, ZPT, true, 4>, threads);
     if (z_affine || FAMILY == 0) return occupancy(bp_kernel<FAMILY, Q, ZPT, true, 1>, threads);
     return occupancy(bp_kernel<FAMILY, Q, ZPT, false, 1>, threads);
