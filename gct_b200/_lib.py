@@ -142,6 +142,7 @@ SIGNATURES = {
     "gct_fdk_plan_check": [VP],
     "gct_fdk_plan_workspace_bytes": [VP, P(C.c_uint64)],
     "gct_fdk_plan_symmetry": [VP, P(C.c_int32)],
+    "gct_fdk_plan_z_mirror": [VP, P(C.c_int32)],
     "gct_fdk_execute": [VP, VP, VP, VP, VP],
     "gct_fdk_filter": [VP, VP, VP, VP],
     "gct_fdk_prepare": [VP, VP, VP, C.c_uint32, C.c_uint32, VP],

@@ -89,10 +89,16 @@ struct ArcWeight {  // wscale / (rho^2 + T(z)^2), T(z) = T0 + z tk
 // floor of v, or v - 1 at integers) and leaves the centred fraction vm - iv in [-0.5, 0.5].
 // `base` is arranged so that base + bits(t) * stride addresses quad row iv + kQuadPad, where
 // bits(t) is the float bit pattern of the shifted coordinate.
-template <class L, int ZPT, bool CLAMP, class W>
+// MIRROR (z-mirror plans, ZPT even): the column's mirror voxels nz - 1 - k sample row position
+// nr - 1 - v, i.e. vm' = (nr - 2) - vm: quad row nr - 2 - iv with the centred fraction negated,
+// addressed as mbase - bits(t) * stride; their sums go to accm. In clamped (mixed) columns the
+// mirror coordinate is clamped and split on its own.
+template <class L, int ZPT, bool CLAMP, bool MIRROR = false, class W>
 __device__ __forceinline__ void column(unsigned long long base, int stride, typename L::U fu, float vm0, float vs,
-                                       float vmax, const W &wt, float (&acc)[ZPT])
+                                       float vmax, const W &wt, float (&acc)[ZPT], unsigned long long mbase = 0,
+                                       float (*accm)[ZPT] = nullptr)
 {
+    static_assert(!MIRROR || ZPT % 2 == 0, "mirror columns take voxel pairs");
     if constexpr (ZPT % 2 == 0) {
         // voxel pairs (z, z + 1): the row split and the accumulate run as packed FP32x2
         // operations (sm_100 FFMA2 / FADD2), element for element the same roundings as below
@@ -101,6 +107,11 @@ __device__ __forceinline__ void column(unsigned long long base, int stride, type
 #pragma unroll
         for (int z = 0; z < ZPT; z += 2) {
             float2 vm = __ffma2_rn(vs2, make_float2(static_cast<float>(z), static_cast<float>(z + 1)), vm02);
+            float2 vmm = make_float2(0.f, 0.f);
+            if (MIRROR && CLAMP) {
+                vmm = make_float2(fminf(fmaxf((vmax - 2.0f) - vm.x, -1.5f), vmax - 0.5f),
+                                  fminf(fmaxf((vmax - 2.0f) - vm.y, -1.5f), vmax - 0.5f));
+            }
             if (CLAMP) {
                 vm.x = fminf(fmaxf(vm.x, -1.5f), vmax - 0.5f);
                 vm.y = fminf(fmaxf(vm.y, -1.5f), vmax - 0.5f);
@@ -116,6 +127,29 @@ __device__ __forceinline__ void column(unsigned long long base, int stride, type
             const float2 r = __ffma2_rn(make_float2(wt.at(z), wt.at(z + 1)), val, make_float2(acc[z], acc[z + 1]));
             acc[z] = r.x;
             acc[z + 1] = r.y;
+            if constexpr (MIRROR) {
+                float2 valm;
+                if constexpr (CLAMP) {
+                    const float2 tm = __fadd2_rn(vmm, shift);
+                    const float2 flm = __fadd2_rn(tm, mshift);
+                    const float2 fvm = __ffma2_rn(flm, make_float2(-1.0f, -1.0f), vmm);
+                    const auto *q0 = reinterpret_cast<const typename L::S *>(
+                        base + static_cast<unsigned long long>(static_cast<long long>(__float_as_int(tm.x)) * stride));
+                    const auto *q1 = reinterpret_cast<const typename L::S *>(
+                        base + static_cast<unsigned long long>(static_cast<long long>(__float_as_int(tm.y)) * stride));
+                    valm = make_float2(L::lerp(__ldg(q0), fu, fvm.x), L::lerp(__ldg(q1), fu, fvm.y));
+                } else {
+                    const auto *q0 = reinterpret_cast<const typename L::S *>(
+                        mbase - static_cast<unsigned long long>(static_cast<long long>(__float_as_int(t.x)) * stride));
+                    const auto *q1 = reinterpret_cast<const typename L::S *>(
+                        mbase - static_cast<unsigned long long>(static_cast<long long>(__float_as_int(t.y)) * stride));
+                    valm = make_float2(L::lerp(__ldg(q0), fu, -fvc.x), L::lerp(__ldg(q1), fu, -fvc.y));
+                }
+                float(&dm)[ZPT] = *accm;
+                const float2 rm = __ffma2_rn(make_float2(wt.at(z), wt.at(z + 1)), valm, make_float2(dm[z], dm[z + 1]));
+                dm[z] = rm.x;
+                dm[z + 1] = rm.y;
+            }
         }
     } else {
 #pragma unroll
@@ -137,10 +171,12 @@ constexpr int kBoxOff = 0, kBoxInside = 1, kBoxMixed = 2;
 
 // cls == kBoxInside skips the per-column range tests: box_class has shown, with a margin, that
 // every column of the block passes them, so the result is the same as with the tests.
-template <class L, int ZPT, class W>
+// MIRROR: the column's mirror voxels as well (column(); accm), whose row segment is the mirror of
+// this one's, so the same range decisions hold for both.
+template <class L, int ZPT, bool MIRROR = false, class W>
 __device__ __forceinline__ void column_dispatch(const typename L::S *view, int es, int qpitch, float u, float v0,
                                                 float vs, float umax, float vmax, const W &wt, float (&acc)[ZPT],
-                                                int cls = kBoxMixed)
+                                                int cls = kBoxMixed, float (*accm)[ZPT] = nullptr)
 {
     if (cls != kBoxInside && !(u >= -1.0f && u <= umax)) return;  // the column's rays miss the detector: zero
     int iu;
@@ -154,10 +190,15 @@ __device__ __forceinline__ void column_dispatch(const typename L::S *view, int e
         reinterpret_cast<unsigned long long>(view + (iu + kQuadPad) * es) -
         static_cast<unsigned long long>(static_cast<long long>(kShiftBits - kQuadPad) * stride);
     const typename L::U fuc = L::ucol(fu);
+    // mirror rows: base + bits' stride with bits' = (nr - 2 + 2 kShiftBits) - bits
+    const unsigned long long mbase =
+        MIRROR ? base + static_cast<unsigned long long>(
+                            (static_cast<long long>(vmax) - 2 + 2LL * kShiftBits) * static_cast<long long>(stride))
+               : 0ull;
     if (cls == kBoxInside || (lo >= -1.0f && hi <= vmax))
-        column<L, ZPT, false>(base, stride, fuc, v0 - 0.5f, vs, vmax, wt, acc);
+        column<L, ZPT, false, MIRROR>(base, stride, fuc, v0 - 0.5f, vs, vmax, wt, acc, mbase, accm);
     else
-        column<L, ZPT, true>(base, stride, fuc, v0 - 0.5f, vs, vmax, wt, acc);
+        column<L, ZPT, true, MIRROR>(base, stride, fuc, v0 - 0.5f, vs, vmax, wt, acc, mbase, accm);
 }
 
 // Classifies the block's voxel box [i0, i1] x [j0, j1] x [k0, k1] for one view of the affine or
@@ -227,20 +268,23 @@ struct BlockBox {
 };
 
 // ES is the entry step of the stack's quad_layout: 1 view-major, 4 interleaved partner views.
-template <int FAMILY, class Q, int ZPT, bool ZAFFINE, int ES = 1>
+// MIRROR (z-mirror plans: affine or projective family, z-affine, ZPT even): the segment lies in
+// the lower half of the grid and the thread also sums its mirror voxels nz - 1 - k.
+template <int FAMILY, class Q, int ZPT, bool ZAFFINE, int ES = 1, bool MIRROR = false>
 __device__ __forceinline__ void bp_column(const BpArgs &a, int i, int j, int k0, bool active, int vps,
                                           float4 *s_coef, int *s_cls, const BlockBox *s_box, int tid, int nthr,
                                           int mode)
 {
+    static_assert(!MIRROR || (ZAFFINE && FAMILY != 2 && ES == 1), "mirror columns: z-affine view-major stacks");
     constexpr bool kClassify = ZAFFINE && FAMILY != 2;
     using L = typename LerpOf<Q>::type;
     using S = typename L::S;
     const float fi = static_cast<float>(i), fj = static_cast<float>(j), fk0 = static_cast<float>(k0);
     const S *quads = static_cast<const S *>(a.quads);
 
-    float acc[ZPT];
+    float acc[ZPT], accm[ZPT];
 #pragma unroll
-    for (int z = 0; z < ZPT; ++z) acc[z] = 0.f;
+    for (int z = 0; z < ZPT; ++z) acc[z] = accm[z] = 0.f;
 
     for (int vc = 0; vc < a.v_count; vc += vps) {
         const int nvc = min(vps, a.v_count - vc);
@@ -270,15 +314,17 @@ __device__ __forceinline__ void bp_column(const BpArgs &a, int i, int j, int k0,
                 // parallel kinds: u = u0 + ui i + uj j, v = v0 + vi i + vj j + vk k, constant weight
                 const float u = fmaf(c[2], fj, fmaf(c[1], fi, c[0]));
                 const float v0 = fmaf(c[4], fk0, fmaf(c[7], fj, fmaf(c[6], fi, c[3])));
-                column_dispatch<L, ZPT>(view, es, a.qpitch, u, v0, c[4], a.umax, a.vmax, ConstWeight{c[5]}, acc, cls);
+                column_dispatch<L, ZPT, MIRROR>(view, es, a.qpitch, u, v0, c[4], a.umax, a.vmax, ConstWeight{c[5]},
+                                                acc, cls, MIRROR ? &accm : nullptr);
             } else if (FAMILY == 1) {
                 if (ZAFFINE) {
                     const float D = fmaf(c[10], fj, fmaf(c[9], fi, c[8]));
                     const float inv = rcp_approx(D);
                     const float u = fmaf(c[2], fj, fmaf(c[1], fi, c[0])) * inv;
                     const float v0 = fmaf(c[7], fk0, fmaf(c[6], fj, fmaf(c[5], fi, c[4]))) * inv;
-                    column_dispatch<L, ZPT>(view, es, a.qpitch, u, v0, c[7] * inv, a.umax, a.vmax,
-                                            ConstWeight{c[12] * inv * inv}, acc, cls);
+                    column_dispatch<L, ZPT, MIRROR>(view, es, a.qpitch, u, v0, c[7] * inv, a.umax, a.vmax,
+                                                    ConstWeight{c[12] * inv * inv}, acc, cls,
+                                                    MIRROR ? &accm : nullptr);
                 } else {
 #pragma unroll
                     for (int z = 0; z < ZPT; ++z) {
@@ -318,13 +364,19 @@ __device__ __forceinline__ void bp_column(const BpArgs &a, int i, int j, int k0,
         }
     }
     if (!active) return;
+    const int kend = MIRROR ? a.nz / 2 : a.nz;
 #pragma unroll
     for (int z = 0; z < ZPT; ++z) {
         const int k = k0 + z;
-        if (k < a.nz) {
+        if (k < kend) {
             float *dst = a.vol + (static_cast<long long>(k) * a.ny + j) * a.nx + i;
             if (mode == kBpAtomic) atomicAdd(dst, acc[z]);
             else *dst = mode == kBpAccumulate ? *dst + acc[z] : acc[z];
+            if constexpr (MIRROR) {
+                float *dm = a.vol + (static_cast<long long>(a.nz - 1 - k) * a.ny + j) * a.nx + i;
+                if (mode == kBpAtomic) atomicAdd(dm, accm[z]);
+                else *dm = mode == kBpAccumulate ? *dm + accm[z] : accm[z];
+            }
         }
     }
 }
@@ -373,9 +425,35 @@ __global__ void __launch_bounds__(256) bp_kernel(BpArgs a)
                                            a.accumulate ? kBpAccumulate : kBpStore);
 }
 
+// z-mirror plans (a.mirror): the grid covers the lower half of the volume along z; each thread's
+// segment also serves its mirror voxels (bp_column MIRROR). Affine and projective z-affine
+// families, view-major stacks, an even number of voxels per thread.
+template <int FAMILY, class Q, int ZPT>
+__global__ void __launch_bounds__(256) bp_mirror_kernel(BpArgs a)
+{
+    __shared__ float4 s_coef[kViewsPerChunk * kC / 4];
+    __shared__ int s_cls[kViewsPerChunk];
+    __shared__ BlockBox s_box;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k0 = blockIdx.z * ZPT;
+    if (threadIdx.x == 0 && threadIdx.y == 0)
+        s_box = block_box(a, blockIdx.x * blockDim.x, blockIdx.y * blockDim.y, blockDim.x, blockDim.y, k0, ZPT);
+    // the first barrier of bp_column orders the s_box store before any read
+    bp_column<FAMILY, Q, ZPT, true, 1, true>(a, i, j, k0, i < a.nx && j < a.ny, kViewsPerChunk, s_coef, s_cls, &s_box,
+                                             threadIdx.y * blockDim.x + threadIdx.x, blockDim.x * blockDim.y,
+                                             a.accumulate ? kBpAccumulate : kBpStore);
+}
+
 template <int FAMILY, class Q, int ZPT>
 void launch_zpt(const BpArgs &a, bool z_affine, dim3 grid, dim3 block, cudaStream_t s)
 {
+    if constexpr (FAMILY != 2 && ZPT % 2 == 0) {
+        if (a.mirror) {
+            bp_mirror_kernel<FAMILY, Q, ZPT><<<grid, block, 0, s>>>(a);
+            return;
+        }
+    }
     if (a.quarter)  // interleaved partner views: quarter-turn plans, which are z-affine
         bp_kernel<FAMILY, Q, ZPT, true, 4><<<grid, block, 0, s>>>(a);
     else if (z_affine || FAMILY == 0)
@@ -388,7 +466,8 @@ template <int FAMILY, class Q>
 void launch_q(const BpArgs &a, bool z_affine, int zpt, int bx, int by, cudaStream_t s)
 {
     const dim3 block(bx, by);
-    const unsigned gz = a.vchunk > 0 ? (a.v_count + a.vchunk - 1) / a.vchunk : (a.nz + zpt - 1) / zpt;
+    const int nz = a.mirror ? a.nz / 2 : a.nz;  // mirror launches cover the lower half
+    const unsigned gz = a.vchunk > 0 ? (a.v_count + a.vchunk - 1) / a.vchunk : (nz + zpt - 1) / zpt;
     const dim3 grid((a.nx + bx - 1) / bx, (a.ny + by - 1) / by, gz);
     switch (zpt) {
         case 1: launch_zpt<FAMILY, Q, 1>(a, z_affine, grid, block, s); break;

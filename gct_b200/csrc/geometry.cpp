@@ -528,6 +528,36 @@ int quarter_turn_symmetry(gct_geom_kind kind, const std::vector<double> &c64, un
     return 0;
 }
 
+bool z_mirror_symmetry(gct_geom_kind kind, const std::vector<double> &c64, unsigned nv, unsigned nr, unsigned nx,
+                       unsigned ny, unsigned nz)
+{
+    if (nz < 2 || nz % 2 != 0 || nv == 0 || c64.size() != static_cast<size_t>(nv) * kCoefPerView) return false;
+    const Family fam = family_of(kind);
+    if (fam == Family::Arc) return false;
+    const double K = nz - 1.0, m = nr - 1.0, kRel = 1e-9;
+    for (unsigned v = 0; v < nv; ++v) {
+        const double *c = &c64[static_cast<size_t>(v) * kCoefPerView];
+        // v(i, j, k) + v(i, j, K - k) = m for every (i, j): the row form's constant, i and j parts
+        double d0, di, dj, scale;
+        if (fam == Family::Affine) {  // v = c3 + c6 i + c7 j + c4 k
+            d0 = 2.0 * c[3] + c[4] * K - m;
+            di = 2.0 * c[6];
+            dj = 2.0 * c[7];
+            scale = std::max({std::fabs(c[3]), std::fabs(c[4]) * nz, m});
+        } else {  // v = (c4 + c5 i + c6 j + c7 k) / D, D = c8 + c9 i + c10 j (z-affine: c3 = c11 = 0)
+            if (c[3] != 0.0 || c[11] != 0.0) return false;
+            d0 = 2.0 * c[4] + c[7] * K - m * c[8];
+            di = 2.0 * c[5] - m * c[9];
+            dj = 2.0 * c[6] - m * c[10];
+            scale = std::max({std::fabs(c[4]), std::fabs(c[7]) * nz, m * std::fabs(c[8]), std::fabs(c[5]) * nx,
+                              std::fabs(c[6]) * ny, m * std::fabs(c[9]) * nx, m * std::fabs(c[10]) * ny});
+        }
+        const double tol = kRel * scale;
+        if (std::fabs(d0) > tol || std::fabs(di) * nx > tol || std::fabs(dj) * ny > tol) return false;
+    }
+    return true;
+}
+
 // ---- projection matrices -----------------------------------------------------------------------
 
 namespace {

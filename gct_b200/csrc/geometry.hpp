@@ -110,4 +110,12 @@ std::vector<float> bp_coefficients(const gct_ct_geom &g, const gct_vol_geom &vol
 int quarter_turn_symmetry(gct_geom_kind kind, const std::vector<double> &c64, unsigned nv, unsigned nx,
                           unsigned ny, unsigned nz);
 
+// Mirror symmetry in z of a z-affine axial scan (affine or projective family): true when, for
+// every view, voxel (i, j, nz - 1 - k) projects onto the same column and weight as (i, j, k) and
+// onto the detector row position mirrored about the detector's middle row, v' = nr - 1 - v (the
+// source in the grid's middle plane, the detector's row centre on that plane), to 1e-9 of the
+// form's range. c64 are the FP64 coefficients of bp_coefficients.
+bool z_mirror_symmetry(gct_geom_kind kind, const std::vector<double> &c64, unsigned nv, unsigned nr, unsigned nx,
+                       unsigned ny, unsigned nz);
+
 }  // namespace gct

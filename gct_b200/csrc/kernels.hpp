@@ -87,6 +87,9 @@ struct BpArgs {
     // [v_begin + z vchunk, + vchunk) and stores its sums at vol + z vol_stride (reduce_partials)
     int vchunk = 0;
     long long vol_stride = 0;
+    // z-mirror launches (plans whose views map voxel (i, j, nz - 1 - k) to the mirror of (i, j, k)
+    // about the detector's middle row, z_mirror_symmetry): column kernels over the lower half
+    int mirror = 0;
 };
 
 // Resident blocks per SM of the backprojection kernel a launch of these options would use

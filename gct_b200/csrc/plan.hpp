@@ -103,6 +103,9 @@ struct gct_fdk_plan {
     // run over the first quarter of the views and of the (x, y) columns, each thread serving the
     // four rotated columns from the four partner views, with zpt_sym voxels along z.
     int sym = 0, zpt_sym = 8, bx_sym = 8, by_sym = 16;
+    // z-mirror symmetry (z_mirror_symmetry): column kernels over the lower half of the grid, each
+    // thread also summing its mirror voxels
+    bool mirror = false;
     // spiral scans: per-slice view windows (first, count); count 0 leaves the slice zero
     bool spiral = false;
     DevBuf<int2> slice_views;

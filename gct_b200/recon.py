@@ -143,6 +143,13 @@ class FdkPlan:
         _lib.check(self._lib.gct_fdk_plan_symmetry(self._handle, C.byref(t)))
         return int(t.value)
 
+    @property
+    def z_mirror(self) -> int:
+        """1 when whole-volume backprojections pair each voxel with its mirror in z, else 0."""
+        t = C.c_int32(0)
+        _lib.check(self._lib.gct_fdk_plan_z_mirror(self._handle, C.byref(t)))
+        return int(t.value)
+
     def execute(self, proj, vol, workspace=None, stream=None) -> None:
         _lib.check(self._lib.gct_fdk_execute(self._handle, C.c_void_p(_ptr(proj)), C.c_void_p(_ptr(vol)),
                                              _ws(workspace), C.c_void_p(_stream(stream))))

@@ -303,6 +303,14 @@ gct_status gct_fdk_plan_workspace_bytes(const gct_fdk_plan *plan, uint64_t *byte
  * or the option is off. No reference counterpart (an execution property of this engine). */
 gct_status gct_fdk_plan_symmetry(const gct_fdk_plan *plan, int32_t *quarter_turn);
 
+/* Mirror symmetry in z the plan found (GCT_SYMMETRY_AUTO with FP16 storage, or _ON): 1 when every
+ * view maps voxel (x, y, nz-1-z) onto the same detector column and weight as (x, y, z) and onto
+ * the row mirrored about the detector's middle row (source on the grid's middle plane, detector
+ * centred on it, nz even), so that whole-volume backprojections without the quarter-turn form
+ * evaluate each view once per voxel pair; 0 otherwise. No reference counterpart (an execution
+ * property of this engine). */
+gct_status gct_fdk_plan_z_mirror(const gct_fdk_plan *plan, int32_t *mirror);
+
 /* Full FDK on device buffers, asynchronous on `stream`: fused cosine + Parker weighting and
  * ramp filtering, then backprojection and the angular-increment scale. proj_dev is
  * [view][row][col] float32, vol_dev receives [z][y][x] float32 (overwritten). workspace may be

@@ -257,3 +257,74 @@ def test_gemm_view_major_quads_are_the_quads_of_the_filtered_rows(kind, nc, nr, 
         want = _quads_from_rows(rows.cpu().numpy(), vscale, nv)[:, :, :, 0, :].view(np.uint16)
         bad = np.argwhere(got != want)
         assert bad.size == 0, f"{len(bad)} differing halves, first at {bad[:4].tolist()}"
+
+
+# ---- z-mirror form -----------------------------------------------------------------------------
+# A short scan has no quarter-turn partners, but with the source on the grid's middle plane and the
+# detector centred on it every view maps voxel (x, y, nz - 1 - z) to the same column and weight as
+# (x, y, z) and to the mirrored detector row: the column kernels then run over the lower half of
+# the grid and each evaluation of a view serves a voxel pair. Results differ from the plain kernel
+# by FP32 coordinate rounding only (the mirror sample takes its row split from its partner's).
+
+def _short(kind="cone_flat", **kw):
+    return make_case(kind, nv=100, range_rad=math.pi + 0.5, **kw)
+
+
+@pytest.mark.parametrize("kind", ["cone_flat", "parallel_2d", "cone_parallel"])
+def test_z_mirror_detected(kind):
+    case = _short(kind)
+    with _plan(case, g.STORAGE_F16, sym=g.SYMMETRY_AUTO) as a, _plan(case, g.STORAGE_F32, sym=g.SYMMETRY_AUTO) as b, \
+            _plan(case, g.STORAGE_F32, sym=g.SYMMETRY_ON) as c, _plan(case, g.STORAGE_F16, sym=g.SYMMETRY_OFF) as d:
+        assert a.quarter_turn == 0 and a.z_mirror == 1
+        assert b.z_mirror == 0 and c.z_mirror == 1 and d.z_mirror == 0
+
+
+@pytest.mark.parametrize("case_kw", [dict(nz=7), dict(mid=(0.0, 0.0, 1.5)), dict(kind="cone_cyl")])
+def test_z_mirror_not_detected(case_kw):
+    kw = dict(case_kw)
+    kind = kw.pop("kind", "cone_flat")
+    case = _short(kind, **kw)
+    with _plan(case, g.STORAGE_F16, sym=g.SYMMETRY_AUTO) as p:
+        assert p.z_mirror == 0
+
+
+def test_quarter_turn_takes_precedence_over_z_mirror():
+    case = make_case("cone_flat")
+    with _plan(case, g.STORAGE_F16, sym=g.SYMMETRY_AUTO) as p:
+        assert p.quarter_turn != 0 and p.z_mirror == 0
+
+
+@pytest.mark.parametrize("storage", [g.STORAGE_F32, g.STORAGE_F16])
+@pytest.mark.parametrize("case_kw", [dict(kind="cone_flat"), dict(kind="parallel_2d"),
+                                     dict(kind="cone_parallel"), dict(kind="cone_flat", nz=48)])
+def test_z_mirror_matches_plain_kernel_and_oracle(case_kw, storage):
+    """nz = 48 reaches past the detector's rows (clamped, mixed and off blocks)."""
+    kw = dict(case_kw)
+    case = _short(kw.pop("kind"), **kw)
+    proj = oracle_projections(case)
+    with _plan(case, storage, sym=g.SYMMETRY_ON) as pm, _plan(case, storage, sym=g.SYMMETRY_OFF) as pp:
+        assert pm.z_mirror == 1
+        got = _execute(pm, case, proj)
+        plain = _execute(pp, case, proj)
+    assert np.isfinite(got).all()
+    assert rel_rms(got, plain) <= 1e-5
+    ref = orc.fdk(case.og, case.ov, proj).reshape(got.shape)
+    assert rel_rms(got, ref) <= (1e-4 if storage == g.STORAGE_F32 else 1e-3)
+
+
+def test_z_mirror_accumulate_and_host_chunks():
+    import torch
+    case = _short()
+    proj = oracle_projections(case)
+    with _plan(case, g.STORAGE_F16, sym=g.SYMMETRY_AUTO) as p:
+        assert p.z_mirror == 1
+        dev = _execute(p, case, proj)
+        host = np.empty(case.vg.shape, np.float32)
+        p.execute_host(proj, host)
+        acc = torch.from_numpy(dev).cuda()
+        p.prepare(torch.from_numpy(proj).cuda())
+        p.backproject(acc, accumulate=True)
+        torch.cuda.synchronize()
+        twice = acc.cpu().numpy()
+    assert rel_rms(host, dev) <= 1e-5
+    assert rel_rms(twice, 2.0 * dev) <= 1e-6
