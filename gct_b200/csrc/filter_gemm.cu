@@ -28,10 +28,12 @@
 //      128 x 64 A tiles and 256 x 64 B tiles (128B swizzle) into a 4-stage shared-memory ring;
 //      one thread of warp 1 issues tcgen05.mma (M 128, N 256, K 16) into one of two TMEM
 //      accumulators of 256 FP32 columns; warps 2-5 drain the other accumulator with tcgen05.ld and
-//      store FP32 rows (FP16 form: times the row's inverse scale). An output tile's K loop is the
-//      full-K segments of its form followed by its band segments.
-//   3. quads_from_rows_kernel: the filtered rows become the backprojector's bilinear-coefficient
-//      quads (FP32 or FP16 with the per-view scale).
+//      store FP32 rows (FP16 form: times the row's inverse scale) or, for FP16 stacks, the
+//      backprojector's bilinear-coefficient quads themselves (pq_epilogue: partner groups of
+//      quarter-turn stacks from partner-interleaved A rows, or view-major quads). An output
+//      tile's K loop is the full-K segments of its form followed by its band segments.
+//   3. otherwise quads_rows_kernel / quads_from_rows_kernel: the filtered rows become the quads
+//      (FP32, or FP16 with the per-view scale).
 // Every mbarrier wait is bounded (2 s of %globaltimer); on timeout the kernel records an error
 // code, stops issuing work, frees its TMEM and returns.
 #include <cuda.h>
@@ -418,8 +420,8 @@ __global__ void __launch_bounds__(192, 1)
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 4);
     __shared__ int s_fail;
     const volatile int *fail_flag = &s_fail;  // re-read on every loop test
-    // partner-quad epilogue: first four rows' values of each TMEM lane quadrant (two buffers) and
-    // the per-tile stop votes of the four epilogue warps (two buffers)
+    // quad epilogue: the first P rows' values of each TMEM lane quadrant (two buffers) and the
+    // per-tile stop votes of the four epilogue warps (two buffers)
     __shared__ float4 s_x[2][4][4][9];
     __shared__ int s_stop[2][4];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
