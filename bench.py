@@ -94,7 +94,8 @@ def parse_args():
                          "pieces (one full term + three over the diagonal band), split-BF16 in the four-term "
                          "form (three pieces of rows and central taps) or three terms, or the FFT")
     ap.add_argument("--symmetry", choices=["auto", "off", "on"], default="auto",
-                    help="quarter-turn backprojection: auto (FP16 storage, when the scan has it), off, on")
+                    help="quarter-turn and z-mirror backprojection forms: auto (FP16 storage, when the scan has "
+                         "them), off, on")
     ap.add_argument("--no-error", action="store_true", help="skip the FP64 oracle error check")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -468,6 +469,41 @@ def time_plan(plan, proj, vol, steps, warmup, stream, dist):
     return total, filt, bp
 
 
+def time_plans_interleaved(plans, proj, vols, steps, warmup, stream, dist):
+    """Times `steps` full FDKs of each plan with the plans' steps interleaved (plan a step, plan b
+    step, ...), so that every path runs under the same clocks and power state; each step is
+    device-timed with CUDA events on the launching stream. Returns {name: (seconds of that plan's
+    steps, max over ranks; mean filter ms; mean BP ms)}."""
+    import torch
+    for _ in range(warmup):
+        for name, plan in plans.items():
+            plan.prepare(proj, stream=stream)
+            plan.backproject(vols[name], stream=stream)
+    ev = {name: [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)] for name in plans}
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    for s in range(steps):
+        for name, plan in plans.items():
+            e = ev[name][s]
+            e[0].record(stream)
+            plan.prepare(proj, stream=stream)
+            e[1].record(stream)
+            plan.backproject(vols[name], stream=stream)
+            e[2].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    out = {}
+    for name in plans:  # every rank takes the same reductions in the same order
+        total = sum(e[0].elapsed_time(e[2]) for e in ev[name]) / 1000.0
+        if dist:
+            total = max_over_ranks(total, "cuda")
+        out[name] = (total, float(np.mean([e[0].elapsed_time(e[1]) for e in ev[name]])),
+                     float(np.mean([e[1].elapsed_time(e[2]) for e in ev[name]])))
+    return out
+
+
 def max_over_ranks(value: float, device) -> float:
     """The job's time for a per-rank time: the maximum over all ranks (every rank calls this)."""
     import torch
@@ -523,13 +559,14 @@ def run_gct(args, cfg, rank, world, local_rank):
     if rank == 0 and not args.no_error:
         errors, nsamp = oracle_errors(cg, cfg, proj, vols, args.seed)
 
+    # the two paths' steps alternate, so that the comparison sees one set of clocks (timed one
+    # after the other, the second path ran under the first one's power cap)
+    sampler = ClockSampler(local_rank)
+    timed = time_plans_interleaved({"fp32": plans["fp32"], "mixed": plans["mixed"]}, proj, vols, args.steps,
+                                   args.warmup, stream, dist)
+    clocks = sampler.stop()
     results = {}
-    clocks = None
-    for name in ("fp32", "mixed"):
-        sampler = ClockSampler(local_rank) if name == "mixed" else None
-        total, filt_ms, bp_ms = time_plan(plans[name], proj, vols[name], args.steps, args.warmup, stream, dist)
-        if sampler:
-            clocks = sampler.stop()
+    for name, (total, filt_ms, bp_ms) in timed.items():
         results[name] = dict(total=total, filt_ms=filt_ms, bp_ms=bp_ms,
                              gups=replica_rate(updates, world, args.steps, total) / 1e9)
 
@@ -587,6 +624,7 @@ def run_gct(args, cfg, rank, world, local_rank):
                    "views": cfg["nv"], "detector": [cfg["nc"], cfg["nr"]], "phantom": (f"{cfg['n_ell']} seeded ellipses in a {WATER_DISK_RADIUS_MM:g} mm radius water disk"
                                if cfg.get("phantom") == "water_disk" else f"{cfg['n_ell']} seeded ellipsoids"),
                    "noise": f"Poisson I0={cfg['i0']:g}" if cfg["i0"] else "none", "l2": "inputs larger than L2, no flush",
+                   "timing": "mixed and FP32 steps interleaved, each device-timed with CUDA events",
                    "parallelism": f"replicas x{world}"},
         "recons_per_s": world * args.steps / mixed["total"],
         "stages_ms": {"filter": mixed["filt_ms"], "backproject": mixed["bp_ms"]},
