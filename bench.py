@@ -49,6 +49,10 @@ CONFIGS = {
                      n=(512, 512, 384), vox=0.5, range=None, n_ell=16, i0=None,
                      label="flat-panel cone-beam short scan (pi + fan), 512x512x384, 496 views, 1240x960 at 0.3 mm, "
                            "SOD 785, SDD 1200"),
+    "short256": dict(kind="cone_flat", nv=248, nc=620, nr=480, du=0.6, dv=0.6, sod=785.0, sdd=1200.0,
+                     n=(256, 256, 192), vox=1.0, range=None, n_ell=16, i0=None,
+                     label="flat-panel cone-beam short scan (pi + fan), 256x256x192, 248 views, 620x480 at 0.6 mm, "
+                           "SOD 785, SDD 1200 (profiling-size case of short384)"),
     "fan256": dict(kind="fan_line", nv=360, nc=512, nr=1, du=1.2, dv=1.0, sod=570.0, sdd=1040.0,
                    n=(256, 256, 1), vox=1.0, range=2 * math.pi, n_ell=10, i0=None, phantom="water_disk",
                    label="fan-beam line detector full scan, 256^2 at 1 mm, 360 views, 512 cells at 1.2 mm, "
